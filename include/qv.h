@@ -1,0 +1,160 @@
+/*
+ * qv.h -- C ABI of the B200 velocity-and-timestep path for Qvort filaments.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (QV_OK = 0, negative = error; nothing throws across the ABI) and
+ * is synchronous at return unless its name ends in _async.  A context owns the
+ * device buffers of one filament system; calls on one context must not
+ * overlap (it is not re-entrant).  Work is issued on the context's stream.
+ *
+ * Data conventions follow the reference's point array f(:) (src/cdata.f90:20-39):
+ *   n slots; positions and velocities are interleaved x[3*i+c] (the column-major
+ *   layout of a Fortran real(c_double) :: x(3,n)); infront/behind hold 1-based
+ *   slot indices and infront==0 marks an empty slot that every loop skips
+ *   (src/timestep.f90:43).
+ *
+ * Each entry point cites the reference routine (file:line, within abag/qvort)
+ * whose call it replaces.
+ */
+#ifndef QV_H
+#define QV_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QV_OK 0
+#define QV_ERR_ARG (-1)        /* bad argument or size */
+#define QV_ERR_CUDA (-2)       /* a CUDA call failed; see qv_last_error */
+#define QV_ERR_SINGULAR (-3)   /* tree singularity (src/tree.f90:372-376) */
+#define QV_ERR_TREE_DEPTH (-4) /* octree deeper than QV_MAX_DEPTH (coincident points) */
+#define QV_ERR_STATE (-5)      /* call out of order (no points, no tree, ...) */
+#define QV_ERR_NOMEM (-6)      /* device allocation failed */
+#define QV_ERR_UNSUPPORTED (-7)/* a run.in option outside this path (mirror, forcing, ...) */
+#define QV_ERR_NAN (-8)        /* NaN in positions (NAN_finder, src/general.f90:253-280) */
+
+#define QV_MAX_DEPTH 64
+
+/* boundary (src/initial.f90:106-136) */
+#define QV_BC_OPEN 0
+#define QV_BC_PERIODIC 1
+#define QV_BC_OPENX 2  /* periodic in y,z */
+#define QV_BC_OPENXY 3 /* periodic in z */
+/* velocity (src/cdata.f90:489-491) */
+#define QV_VEL_OFF 0
+#define QV_VEL_LIA 1
+#define QV_VEL_BS 2
+#define QV_VEL_TREE 3
+/* arithmetic of the non-local sums */
+#define QV_PREC_FP64 0  /* FP64 throughout (the reference's arithmetic) */
+#define QV_PREC_MIXED 1 /* FP32 pair terms, FP64 recentring, compensated sums */
+
+/* run.in parameters used by the path (src/cdata.f90:196-416) */
+typedef struct qv_params {
+  double quant_circ;          /* quant_circ, default 9.97e-4 */
+  double corea;               /* corea, default 8.244023e-9 */
+  double box_size;            /* box_size */
+  double delta;               /* delta */
+  double dt;                  /* dt */
+  double tree_theta;          /* tree_theta (0: direct sum, pclose) */
+  int boundary;               /* QV_BC_* */
+  int velocity;               /* QV_VEL_* */
+  int deriv_order;            /* 2 ('second') or 4 ('fourth') */
+  int tree_extra_correction;  /* tree_extra_correction, default 1 */
+  int fixed_lia_beta;         /* fixed_LIA_beta */
+  int precision;              /* QV_PREC_* */
+  int runge_kutta;            /* runge_kutta */
+  int recon_shots;            /* recon_shots, default 1 */
+} qv_params;
+
+typedef struct qv_ctx qv_ctx;
+
+/* Fill *p with the reference's run.in defaults (src/cdata.f90:196-416). */
+int qv_default_params(qv_params *p);
+
+/* Create / destroy a context.  Replaces nothing: the reference keeps state in
+ * module variables (src/cdata.f90).  stream may be NULL (a private stream). */
+int qv_create(const qv_params *p, void *stream, qv_ctx **out);
+int qv_destroy(qv_ctx *ctx);
+int qv_set_params(qv_ctx *ctx, const qv_params *p);
+const char *qv_last_error(const qv_ctx *ctx);
+
+/* Gather of f(:)%x, f(:)%infront, f(:)%behind into the context (host
+ * pointers).  Resets the AB history and closest to zero. */
+int qv_set_points(qv_ctx *ctx, int n, const double *x, const int *infront, const int *behind);
+/* The same from device pointers (the torch harness). */
+int qv_set_points_device(qv_ctx *ctx, int n, const double *x, const int *infront,
+                         const int *behind);
+/* f(:)%u1..u3 in/out (host; NULL means zero on set, skip on get). */
+int qv_set_history(qv_ctx *ctx, const double *u1, const double *u2, const double *u3);
+int qv_get_history(qv_ctx *ctx, double *u1, double *u2, double *u3);
+/* f(:)%closest in/out; pclose_tree never resets it (src/tree.f90:225). */
+int qv_set_closest(qv_ctx *ctx, const int *closest);
+/* Scatter back f(:)%x and f(:)%u (host; NULL skips). */
+int qv_get_points(qv_ctx *ctx, double *x, double *u);
+/* Device pointers of the context's arrays (valid until the next set_points). */
+int qv_device_arrays(qv_ctx *ctx, double **x, double **u, int **infront, int **behind);
+
+/* ghostp (src/periodic.f90:8-17): ghosts from positions and links. */
+int qv_ghosts(qv_ctx *ctx);
+int qv_get_ghosts(qv_ctx *ctx, double *gi, double *gb, double *gii, double *gbb);
+
+/* construct_tree (src/tree.f90:44-80): the octree, bit-exact. */
+int qv_build_tree(qv_ctx *ctx);
+/* Number of nodes and depth of the last tree. */
+int qv_tree_info(qv_ctx *ctx, int *nnodes, int *depth);
+/* Non-empty nodes of the last tree in breadth-first order, children in the
+ * fixed fbl..btr order (src/tree.f90:92-114); the same layout the oracle
+ * exports.  Returns the node count, or -count when cap is too small. */
+int qv_tree_export(qv_ctx *ctx, int cap, int *parent, int *digit, int *depth, double *pos,
+                   double *width, int *pcount, double *cent, double *circ, double *Cij,
+                   int *first);
+
+/* The first loop of pmotion (src/timestep.f90:41-47) = calc_velocity
+ * (src/timestep.f90:180-309) for every active point, LIA + Biot-Savart direct
+ * sum or tree walk + periodic images.  Host outputs may be NULL; eval_count
+ * receives the reference's eval_counter (src/tree.f90:63-79,393,413). */
+int qv_velocity(qv_ctx *ctx, double *u, double *u_li, double *u_bs, long long *eval_count);
+
+/* The second loop of pmotion (src/timestep.f90:48-71): the AB ladder on the
+ * context's velocities, then the u3<-u2<-u1<-u shift. */
+int qv_step_ab(qv_ctx *ctx);
+/* pmotion_RK3 (src/timestep.f90:95-176): 3 velocity stages with ghost and
+ * tree rebuilds between them. */
+int qv_step_rk3(qv_ctx *ctx);
+/* enforce_periodic and the yz / z variants (src/periodic.f90:188-214). */
+int qv_enforce_periodic(qv_ctx *ctx);
+
+/* pclose_tree (src/tree.f90:219-278) on the tree of the last build and the
+ * current positions and links, or pclose (src/line.f90:205-234) when
+ * tree_theta == 0.  closest/closestd are host outputs (NULL skips). */
+int qv_closest(qv_ctx *ctx, int *closest, double *closestd);
+
+/* energy_info (src/diagnostic.f90:259-280) with the context's velocities. */
+int qv_energy(qv_ctx *ctx, double *energy);
+
+/* One pass of the loop body of src/run.f90:41-107 restricted to the path:
+ * ghostp, construct_tree, pmotion/pmotion_RK3, the candidate search when
+ * itime % recon_shots == 0, ghostp, boundary wrap.  Device-resident. */
+int qv_step(qv_ctx *ctx, int itime);
+
+/* Block until the context's stream is idle. */
+int qv_sync(qv_ctx *ctx);
+
+/* Instrumentation (no reference counterpart beyond the seg_fault trace flags,
+ * src/run.f90:31-166, and eval_counter, src/tree.f90:40).  With profiling on,
+ * the phases below are bracketed by CUDA events on the context's stream and
+ * their device times accumulate into ms[QV_NPHASES]. */
+#define QV_NPHASES 7 /* ghosts, tree build, local term, non-local sum, update, search, wrap */
+int qv_profile(qv_ctx *ctx, int enable);
+int qv_phase_times(qv_ctx *ctx, double *ms, int reset);
+/* Kernel launches issued by this context so far, and the leaf / far-field
+ * evaluations of the last tree walk. */
+int qv_counters(qv_ctx *ctx, long long *launches, long long *leaf_evals, long long *far_evals);
+/* Measured FP32 FMA throughput of the current device (TFLOP/s), the
+ * denominator of the FP32-pipe roofline. */
+int qv_probe_fp32(void *stream, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,216 @@
+"""ctypes binding of the CPU oracle (oracle/qv_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, never by the qvort_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "libqv_oracle.so"
+
+
+def build() -> Path:
+    src = HERE / "qv_oracle.c"
+    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-C", str(HERE), "-s"], check=True)
+    return LIB
+
+
+class QoParams(C.Structure):
+    _fields_ = [
+        ("quant_circ", C.c_double), ("corea", C.c_double), ("box_size", C.c_double),
+        ("delta", C.c_double), ("dt", C.c_double), ("tree_theta", C.c_double),
+        ("boundary", C.c_int), ("velocity", C.c_int), ("deriv_order", C.c_int),
+        ("tree_extra_correction", C.c_int), ("fixed_lia_beta", C.c_int),
+    ]
+
+
+_BC = {"open": 0, "periodic": 1, "openx": 2, "openxy": 3}
+_VEL = {"Off": 0, "LIA": 1, "BS": 2, "Tree": 3}
+
+
+def params(**kw) -> QoParams:
+    p = QoParams()
+    p.quant_circ = kw.get("quant_circ", 9.97e-4)
+    p.corea = kw.get("corea", 8.244023e-9)
+    p.box_size = kw.get("box_size", 0.1)
+    p.delta = kw.get("delta", 5e-4)
+    p.dt = kw.get("dt", 1e-7)
+    p.tree_theta = kw.get("tree_theta", 0.0)
+    b = kw.get("boundary", "open")
+    p.boundary = _BC[b] if isinstance(b, str) else b
+    v = kw.get("velocity", "BS")
+    p.velocity = _VEL[v] if isinstance(v, str) else v
+    p.deriv_order = kw.get("deriv_order", 2)
+    p.tree_extra_correction = kw.get("tree_extra_correction", 1)
+    p.fixed_lia_beta = kw.get("fixed_lia_beta", 0)
+    return p
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB))
+        P = C.POINTER(QoParams)
+        v = C.c_void_p
+        _lib.qo_ghosts.argtypes = [P, C.c_int, v, v, v, v, v, v, v]
+        _lib.qo_enforce_periodic.argtypes = [P, C.c_int, v, v]
+        _lib.qo_tree_build.argtypes = [P, C.c_int, v, v, v]
+        _lib.qo_tree_build.restype = C.c_void_p
+        _lib.qo_tree_free.argtypes = [v]
+        _lib.qo_tree_status.argtypes = [v]
+        _lib.qo_tree_maxdepth.argtypes = [v]
+        _lib.qo_tree_count.argtypes = [v]
+        _lib.qo_tree_export.argtypes = [v, C.c_int] + [v] * 10
+        _lib.qo_velocity.argtypes = [P, C.c_int, v, v, v, v, v, v, v, v, C.c_int, v, v, v, v,
+                                     C.POINTER(C.c_longlong), C.c_int]
+        _lib.qo_pmotion_ab.argtypes = [C.c_double, C.c_int, v, v, v, v, v, v]
+        _lib.qo_pclose_tree.argtypes = [v, C.c_int, v, v, v, v, v, C.c_int]
+        _lib.qo_pclose.argtypes = [C.c_int, v, v, v, v, v]
+        _lib.qo_energy.argtypes = [P, C.c_int, v, v, v, v, v, v, v]
+        _lib.qo_energy.restype = C.c_double
+        _lib.qo_step.argtypes = [P, C.c_int, v, v, v, v, v, v, v, v, v, v, v, C.c_int, v, v,
+                                 C.POINTER(C.c_longlong), C.c_int]
+        _lib.qo_dt_max.argtypes = [P]
+        _lib.qo_dt_max.restype = C.c_double
+        _lib.qo_set_depth_cap.argtypes = [C.c_int]
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def ghosts(p: QoParams, x, inf, beh):
+    x, inf, beh = _f(x), _i(inf), _i(beh)
+    n = x.shape[0]
+    g = [np.zeros((n, 3)) for _ in range(4)]
+    lib().qo_ghosts(C.byref(p), n, _p(x), _p(inf), _p(beh), *[_p(a) for a in g])
+    return g
+
+
+class Tree:
+    def __init__(self, p: QoParams, x, gi, inf):
+        self.x, self.gi, self.inf = _f(x), _f(gi), _i(inf)
+        self.h = lib().qo_tree_build(C.byref(p), self.x.shape[0], _p(self.x), _p(self.gi),
+                                     _p(self.inf))
+
+    @property
+    def status(self) -> int:
+        return lib().qo_tree_status(self.h)
+
+    def export(self) -> dict:
+        m = lib().qo_tree_count(self.h)
+        out = dict(parent=np.empty(m, np.int32), digit=np.empty(m, np.int32),
+                   depth=np.empty(m, np.int32), pos=np.empty((m, 3)), width=np.empty(m),
+                   pcount=np.empty(m, np.int32), cent=np.empty((m, 3)), circ=np.empty((m, 3)),
+                   Cij=np.empty((m, 9)), first=np.empty(m, np.int32))
+        keys = ["parent", "digit", "depth", "pos", "width", "pcount", "cent", "circ", "Cij",
+                "first"]
+        lib().qo_tree_export(self.h, m, *[_p(out[k]) for k in keys])
+        return out
+
+    def close(self):
+        if self.h:
+            lib().qo_tree_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def velocity(p: QoParams, x, inf, beh, g, tree: Tree | None = None, targets=None,
+             nthreads: int = 1):
+    x, inf, beh = _f(x), _i(inf), _i(beh)
+    g = [_f(a) for a in g]
+    n = x.shape[0]
+    tg = None if targets is None else _i(targets)
+    nt = n if tg is None else tg.shape[0]
+    u = np.zeros((nt, 3))
+    uli = np.zeros((nt, 3))
+    ubs = np.zeros((nt, 3))
+    ev = C.c_longlong()
+    st = lib().qo_velocity(C.byref(p), n, _p(x), _p(inf), _p(beh), *[_p(a) for a in g],
+                           tree.h if tree is not None else None, nt, _p(tg), _p(u), _p(uli),
+                           _p(ubs), C.byref(ev), nthreads)
+    return u, uli, ubs, ev.value, st
+
+
+def pmotion_ab(dt, x, u, u1, u2, u3, inf):
+    x, u = _f(x).copy(), _f(u)
+    u1, u2, u3 = _f(u1).copy(), _f(u2).copy(), _f(u3).copy()
+    lib().qo_pmotion_ab(dt, x.shape[0], _p(x), _p(u), _p(u1), _p(u2), _p(u3), _p(_i(inf)))
+    return x, u1, u2, u3
+
+
+def pclose_tree(tree: Tree, x, inf, beh, closest, nthreads: int = 1):
+    x, inf, beh = _f(x), _i(inf), _i(beh)
+    cl = _i(closest).copy()
+    cd = np.zeros(x.shape[0])
+    lib().qo_pclose_tree(tree.h, x.shape[0], _p(x), _p(inf), _p(beh), _p(cl), _p(cd), nthreads)
+    return cl, cd
+
+
+def pclose(x, inf, beh, closest, closestd=None):
+    x, inf, beh = _f(x), _i(inf), _i(beh)
+    cl = _i(closest).copy()
+    cd = np.zeros(x.shape[0]) if closestd is None else _f(closestd).copy()
+    lib().qo_pclose(x.shape[0], _p(x), _p(inf), _p(beh), _p(cl), _p(cd))
+    return cl, cd
+
+
+def energy(p: QoParams, x, u, inf, g) -> float:
+    x, u, inf = _f(x), _f(u), _i(inf)
+    g = [_f(a) for a in g]
+    return lib().qo_energy(C.byref(p), x.shape[0], _p(x), _p(u), _p(inf), *[_p(a) for a in g])
+
+
+class State:
+    """The oracle's copy of f(:) for whole steps (qo_step)."""
+
+    def __init__(self, p: QoParams, x, inf, beh):
+        self.p = p
+        self.x = _f(x).copy()
+        self.inf, self.beh = _i(inf), _i(beh)
+        n = self.x.shape[0]
+        self.u = np.zeros((n, 3))
+        self.u1 = np.zeros((n, 3))
+        self.u2 = np.zeros((n, 3))
+        self.u3 = np.zeros((n, 3))
+        self.g = [np.zeros((n, 3)) for _ in range(4)]
+        self.closest = np.zeros(n, np.int32)
+        self.closestd = np.zeros(n)
+        self.evals = 0
+
+    def step(self, runge_kutta: bool = False, search: bool = True, nthreads: int = 1) -> int:
+        ev = C.c_longlong()
+        st = lib().qo_step(C.byref(self.p), self.x.shape[0], _p(self.x), _p(self.inf),
+                           _p(self.beh), _p(self.u), _p(self.u1), _p(self.u2), _p(self.u3),
+                           *[_p(a) for a in self.g], int(runge_kutta),
+                           _p(self.closest) if search else None,
+                           _p(self.closestd) if search else None, C.byref(ev), nthreads)
+        self.evals = ev.value
+        return st
+
+
+def dt_max(p: QoParams) -> float:
+    return lib().qo_dt_max(C.byref(p))

@@ -1,0 +1,156 @@
+// qv_closest.cu -- reconnection candidate search.
+//
+// pclose_tree / closest_tree (src/tree.f90:219-278): for every point, walk the
+// tree of the last build -- built before the move, so centroids and the
+// parray(1)%infront links are stale (src/run.f90:43-66) -- with the current
+// positions and links.  Per point the walk is sequential and order dependent
+// (closestd shrinks as it goes and prunes later cells), so the kernel keeps
+// the reference's depth-first child order per lane, with the same
+// warp-coherent (node, lane mask) stack as the velocity walk, and evaluates
+// every distance and theta with round-to-nearest FP64 intrinsics.  The pair
+// list (closest, closestd) is bit-identical to the reference arithmetic.
+//
+// pclose (src/line.f90:205-234): the N^2 scan used when tree_theta == 0.
+#include "qv_internal.cuh"
+
+#define CW 4
+#define CSTK (7 * QV_MAX_DEPTH + 16)
+
+__device__ __forceinline__ double dist_exact(const double *a, double b0, double b1, double b2) {
+  double d0 = __dsub_rn(a[0], b0), d1 = __dsub_rn(a[1], b1), d2 = __dsub_rn(a[2], b2);
+  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
+}
+
+__global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *__restrict__ x,
+                                                         const int *__restrict__ inf,
+                                                         const int *__restrict__ beh,
+                                                         const WNode64 *__restrict__ w64,
+                                                         int *closest, double *closestd,
+                                                         int *status) {
+  __shared__ int2 stk[CW][CSTK];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int2 *st = stk[wid];
+  const int nwarps = (n + 31) / 32;
+  for (int w = blockIdx.x * CW + wid; w < nwarps; w += gridDim.x * CW) {
+    int i = w * 32 + lane;
+    bool live = i < n && inf[i] != 0;
+    double xi[3] = {0., 0., 0.};
+    int ii = i + 1, fi = -1, bi = -1, cl = 0;
+    double cd = 100.;
+    if (live) {
+      xi[0] = x[3 * i]; xi[1] = x[3 * i + 1]; xi[2] = x[3 * i + 2];
+      fi = inf[i]; bi = beh[i]; cl = closest[i];
+    }
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    bool bad = false;
+    int top = 0;
+    if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+    top = live_mask ? 1 : 0;
+    __syncwarp();
+    while (top > 0) {
+      top--;
+      int2 e = st[top];
+      __syncwarp();
+      const int node = e.x;
+      const bool in = (((unsigned)e.y) >> lane) & 1u;
+      const WNode64 h = w64[node];
+      bool open = false;
+      if (in && h.count > 0) {
+        double dist = dist_exact(xi, h.cx, h.cy, h.cz);
+        double theta = __ddiv_rn(h.width, dist);
+        if (h.count == 1 || theta < .5) {
+          if (dist < cd) {
+            if (h.count > 1) {
+              cl = 0;
+            } else {
+              int j = beh[h.finf - 1];  // f(parray(1)%infront)%behind with current links
+              if (ii != j && fi != j && bi != j) {
+                cl = j;
+                cd = dist;
+              }
+            }
+          }
+        } else {
+          open = true;
+        }
+      }
+      unsigned om = __ballot_sync(0xffffffffu, open);
+      if (om) {
+        int nc = h.nchild;
+        if (top + nc > CSTK) {
+          bad = true;
+          nc = 0;
+        }
+        if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+        top += nc;
+      }
+      __syncwarp();
+    }
+    if (i < n) {
+      closestd[i] = cd;  // 100 for empty slots too (src/tree.f90:225)
+      if (live) closest[i] = cl;
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, 2);
+  }
+}
+
+#define PT 128
+__global__ void __launch_bounds__(PT) k_pclose(int n, const double *__restrict__ x,
+                                              const int *__restrict__ inf,
+                                              const int *__restrict__ beh, int *closest,
+                                              double *closestd) {
+  __shared__ double sx[PT][3];
+  __shared__ int sa[PT];
+  int i = blockIdx.x * PT + threadIdx.x;
+  bool live = i < n && inf[i] != 0;
+  double xi[3] = {0., 0., 0.};
+  int fi = -1, bi = -1, cl = 0;
+  double cd = 100.;
+  if (live) {
+    xi[0] = x[3 * i]; xi[1] = x[3 * i + 1]; xi[2] = x[3 * i + 2];
+    fi = inf[i]; bi = beh[i]; cl = closest[i];
+  }
+  for (int t0 = 0; t0 < n; t0 += PT) {
+    __syncthreads();
+    int j = t0 + threadIdx.x;
+    if (j < n) {
+      sa[threadIdx.x] = inf[j];
+      for (int c = 0; c < 3; c++) sx[threadIdx.x][c] = x[3 * j + c];
+    }
+    __syncthreads();
+    int m = min(PT, n - t0);
+    if (live) {
+      for (int k = 0; k < m; k++) {
+        int jj = t0 + k;
+        if (sa[k] == 0) continue;
+        if (i != jj && fi != jj + 1 && bi != jj + 1) {
+          double d = dist_exact(xi, sx[k][0], sx[k][1], sx[k][2]);
+          if (d < cd) {
+            cl = jj + 1;
+            cd = d;
+          }
+        }
+      }
+    }
+  }
+  if (live) {
+    closest[i] = cl;
+    closestd[i] = cd;
+  }
+}
+
+int qv_launch_closest(qv_ctx *c) {
+  if (c->n == 0) return QV_OK;
+  if (c->p.tree_theta > 0) {
+    if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
+    int nwarps = (c->n + 31) / 32;
+    k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, 0, c->stream>>>(
+        c->n, c->x, c->infront, c->behind, c->tree.w64, c->closest, c->closestd, c->dstatus);
+  } else {
+    k_pclose<<<(c->n + PT - 1) / PT, PT, 0, c->stream>>>(c->n, c->x, c->infront, c->behind,
+                                                         c->closest, c->closestd);
+  }
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}

@@ -1,0 +1,354 @@
+// qv_direct.cu -- direct desingularised Biot-Savart sum with periodic images
+// (biot_savart / biot_savart_shift, src/timestep.f90:462-507), one thread per
+// target, source segments staged tile by tile in shared memory.
+//
+// FP64 kernel: the reference's formula
+//   u += G/(2 pi) (d x s)/(4ac - b^2) [(2c+b)/sqrt(a+b+c) - b/sqrt(a)]
+// with d = x_j + shift - x_i, s = ghosti_j - x_j, a=|d|^2, b=2 d.s, c=|s|^2.
+//
+// Mixed kernel: FP32 pair terms in the stable straight-segment form the
+// reference uses for tree leaves (src/tree.f90:380-390),
+//   u += G/(4 pi) (|R1|+|R2|)/(|R1||R2|(|R1||R2| + R1.R2)) R1 x R2,
+// with R1 = x_j + shift - x_i and R2 = ghosti_j + shift - x_i recentred on the
+// target from FP64 data (every FP64 coordinate carried as a hi/lo float pair,
+// so the difference keeps FP64-level information before it is rounded), and
+// Kahan-compensated FP32 accumulation.  The two forms agree analytically; the
+// stable one avoids the (2c+b)/sqrt - b/sqrt cancellation that FP32 cannot
+// afford for far segments.
+//
+// Skip rules differ between the unshifted and shifted sums exactly as in the
+// reference (src/timestep.f90:471 vs :496).
+//
+// Work split: blockIdx.x = tile of 128 targets, blockIdx.y = chunk of sources;
+// per-chunk partial sums go to a buffer and are added in fixed chunk order,
+// so results are deterministic.
+#include "qv_internal.cuh"
+
+static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+#define DTILE 128
+
+// ------------------------------------------------------------- compaction
+__global__ void k_count_active(int n, const int *__restrict__ inf, int *blk_cnt) {
+  __shared__ int s;
+  if (threadIdx.x == 0) s = 0;
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int a = (i < n && inf[i] != 0) ? 1 : 0;
+  int w = __syncthreads_count(a);
+  if (threadIdx.x == 0) blk_cnt[blockIdx.x] = w;
+  (void)s;
+}
+__global__ void k_scan_small(int m, int *v, int *total) {
+  // single block exclusive scan of m ints (m up to a few 100k)
+  __shared__ int part[1024];
+  int per = (m + blockDim.x - 1) / blockDim.x;
+  int lo = threadIdx.x * per, hi = min(m, lo + per);
+  int s = 0;
+  for (int k = lo; k < hi; k++) s += v[k];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = 1; off < blockDim.x; off <<= 1) {
+    int t = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+    __syncthreads();
+    part[threadIdx.x] += t;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - s;
+  for (int k = lo; k < hi; k++) {
+    int t = v[k];
+    v[k] = run;
+    run += t;
+  }
+  if (threadIdx.x == blockDim.x - 1) *total = part[threadIdx.x];
+}
+__global__ void k_scatter_active(int n, const int *__restrict__ inf, const int *blk_off, int *act) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int a = (i < n && inf[i] != 0) ? 1 : 0;
+  unsigned m = __ballot_sync(0xffffffffu, a);
+  __shared__ int wsum[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) wsum[wid] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int r = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) { int t = wsum[k]; wsum[k] = r; r += t; }
+  }
+  __syncthreads();
+  if (a) act[blk_off[blockIdx.x] + wsum[wid] + __popc(m & ((1u << lane) - 1))] = i;
+}
+
+// Stable compaction of the active slots (ascending index) into c->act.
+int qv_compact_active(qv_ctx *c) {
+  int nb = nblk(c->n, 256);
+  int *tmp = nullptr;
+  QV_CUDA(c, cudaMallocAsync((void **)&tmp, sizeof(int) * (nb + 1), c->stream));
+  k_count_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp);
+  k_scan_small<<<1, 1024, 0, c->stream>>>(nb, tmp, tmp + nb);
+  k_scatter_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp, c->act);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 3);
+  QV_CUDA(c, cudaMemcpyAsync(&c->n_act, tmp + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaFreeAsync(tmp, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+// ------------------------------------------------------------ source packs
+// FP64: x(3), s=gi-x(3), c=|gi-x|^2, slot (1-based) as double.
+// FP32: x hi(3), x lo(3), gi hi(3), gi lo(3), slot bits, pad.
+__global__ void k_pack_sources(int na, const int *__restrict__ act, const double *__restrict__ x,
+                               const double *__restrict__ gi, double *s64, float *s32) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= na) return;
+  int j = act[q];
+  double X[3], G[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) { X[k] = x[3 * j + k]; G[k] = gi[3 * j + k]; }
+  double *o = s64 + 8 * q;
+  double e0 = G[0] - X[0], e1 = G[1] - X[1], e2 = G[2] - X[2];
+  o[0] = X[0]; o[1] = X[1]; o[2] = X[2];
+  o[3] = e0; o[4] = e1; o[5] = e2;
+  o[6] = __dadd_rn(__dadd_rn(__dmul_rn(e0, e0), __dmul_rn(e1, e1)), __dmul_rn(e2, e2));
+  o[7] = (double)(j + 1);
+  float *f = s32 + 16 * q;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float h = __double2float_rn(X[k]);
+    f[k] = h;
+    f[3 + k] = __double2float_rn(X[k] - (double)h);
+    float g = __double2float_rn(G[k]);
+    f[6 + k] = g;
+    f[9 + k] = __double2float_rn(G[k] - (double)g);
+  }
+  f[12] = __int_as_float(j + 1);
+  f[13] = f[14] = f[15] = 0.f;
+}
+
+// ------------------------------------------------------------ pair terms
+__device__ __forceinline__ void pair64(double dx, double dy, double dz, double sx, double sy,
+                                       double sz, double c, double &ax, double &ay, double &az) {
+  double a = dx * dx + dy * dy + dz * dz;
+  double b = 2. * (dx * sx + dy * sy + dz * sz);
+  double disc = 4. * a * c - b * b;
+  if (disc == 0.) return;  // src/timestep.f90:476
+  double fac = (2. * c + b) * rsqrt(a + b + c) - b * rsqrt(a);
+  double sc = fac / disc;
+  ax += (dy * sz - dz * sy) * sc;
+  ay += (dz * sx - dx * sz) * sc;
+  az += (dx * sy - dy * sx) * sc;
+}
+
+struct Kahan3 {
+  float s[3], c[3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 3; k++) s[k] = c[k] = 0.f;
+  }
+  __device__ __forceinline__ void add(float a0, float a1, float a2) {
+    float a[3] = {a0, a1, a2};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float y = __fsub_rn(a[k], c[k]);
+      float t = __fadd_rn(s[k], y);
+      c[k] = __fsub_rn(__fsub_rn(t, s[k]), y);
+      s[k] = t;
+    }
+  }
+  __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
+};
+
+// Stable straight-segment term without the G/(4 pi) factor.
+__device__ __forceinline__ void seg32(float r1x, float r1y, float r1z, float r2x, float r2y,
+                                      float r2z, float &ox, float &oy, float &oz) {
+  float r1s = fmaf(r1x, r1x, fmaf(r1y, r1y, r1z * r1z));
+  qv_seg32(r1x, r1y, r1z, r2x, r2y, r2z, r1s, ox, oy, oz);
+}
+
+template <int BC>
+__device__ __forceinline__ void img_mul(int m, int &a, int &b, int &c) {
+  qv_img_shift(BC, m, &a, &b, &c);
+}
+
+__device__ __forceinline__ double shifted(double v, int a, double L) {
+  return a == 0 ? v : (a > 0 ? v + L : v - L);
+}
+
+// ------------------------------------------------------------ FP64 kernel
+template <int BC>
+__global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restrict__ act,
+                                                    const double *__restrict__ x,
+                                                    const int *__restrict__ beh,
+                                                    const double *__restrict__ src, int chunk_len,
+                                                    double L, double *part) {
+  constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
+  __shared__ double tile[DTILE * 8];
+  int q = blockIdx.x * DTILE + threadIdx.x;
+  bool live = q < na;
+  int i = live ? act[q] : 0;
+  double xi0 = live ? x[3 * i] : 0., xi1 = live ? x[3 * i + 1] : 0., xi2 = live ? x[3 * i + 2] : 0.;
+  int bi = live ? beh[i] : -1, ii = i + 1;
+  double a0x = 0., a0y = 0., a0z = 0., a1x = 0., a1y = 0., a1z = 0.;
+  int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
+  for (int t0 = j0; t0 < j1; t0 += DTILE) {
+    int m = min(DTILE, j1 - t0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < m * 8; k += DTILE) tile[k] = src[8 * t0 + k];
+    __syncthreads();
+    for (int k = 0; k < m; k++) {
+      const double *s = tile + 8 * k;
+      int jj = (int)s[7];
+      double dx = s[0] - xi0, dy = s[1] - xi1, dz = s[2] - xi2;
+      if (jj != ii && jj != bi) pair64(dx, dy, dz, s[3], s[4], s[5], s[6], a0x, a0y, a0z);
+      if (NIMG > 0 && jj != bi) {
+#pragma unroll
+        for (int im = 0; im < NIMG; im++) {
+          int ma, mb, mc;
+          img_mul<BC>(im, ma, mb, mc);
+          pair64(shifted(dx, ma, L), shifted(dy, mb, L), shifted(dz, mc, L), s[3], s[4], s[5],
+                 s[6], a1x, a1y, a1z);
+        }
+      }
+    }
+  }
+  if (live) {
+    double *o = part + ((size_t)blockIdx.y * na + q) * 6;
+    o[0] = a0x; o[1] = a0y; o[2] = a0z; o[3] = a1x; o[4] = a1y; o[5] = a1z;
+  }
+}
+
+// One tile of sources against one target and one image.  The target is
+// recentred per image: t = x_i - shift as a hi/lo float pair.  skip2 is the
+// extra slot skipped by the unshifted sum (i itself), -7 for images.
+__device__ __forceinline__ void seg_tile(const float4 *tile, int m, const double *xi, int ma,
+                                         int mb, int mc, double L, int bi, int skip2,
+                                         Kahan3 &acc) {
+  float th[3], tl[3];
+  int mm[3] = {ma, mb, mc};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double t = shifted(xi[c], -mm[c], L);
+    th[c] = __double2float_rn(t);
+    tl[c] = __double2float_rn(t - (double)th[c]);
+  }
+  for (int k = 0; k < m; k++) {
+    float4 A = tile[4 * k], B = tile[4 * k + 1], Cc = tile[4 * k + 2], D = tile[4 * k + 3];
+    int jj = __float_as_int(D.x);
+    if (jj == bi || jj == skip2) continue;
+    // A = (xh0 xh1 xh2 xl0) B = (xl1 xl2 gh0 gh1) C = (gh2 gl0 gl1 gl2)
+    float r1x = (A.x - th[0]) + (A.w - tl[0]);
+    float r1y = (A.y - th[1]) + (B.x - tl[1]);
+    float r1z = (A.z - th[2]) + (B.y - tl[2]);
+    float r2x = (B.z - th[0]) + (Cc.y - tl[0]);
+    float r2y = (B.w - th[1]) + (Cc.z - tl[1]);
+    float r2z = (Cc.x - th[2]) + (Cc.w - tl[2]);
+    float ox, oy, oz;
+    seg32(r1x, r1y, r1z, r2x, r2y, r2z, ox, oy, oz);
+    acc.add(ox, oy, oz);
+  }
+}
+
+// ------------------------------------------------------------ mixed kernel
+template <int BC>
+__global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restrict__ act,
+                                                    const double *__restrict__ x,
+                                                    const int *__restrict__ beh,
+                                                    const float *__restrict__ src, int chunk_len,
+                                                    double L, double *part) {
+  constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
+  __shared__ float4 tile[DTILE * 4];
+  int q = blockIdx.x * DTILE + threadIdx.x;
+  bool live = q < na;
+  int i = live ? act[q] : 0;
+  double xi[3] = {live ? x[3 * i] : 0., live ? x[3 * i + 1] : 0., live ? x[3 * i + 2] : 0.};
+  int bi = live ? beh[i] : -1, ii = i + 1;
+  Kahan3 k0, k1;
+  k0.zero();
+  k1.zero();
+  int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
+  const float4 *src4 = reinterpret_cast<const float4 *>(src);
+  for (int t0 = j0; t0 < j1; t0 += DTILE) {
+    int m = min(DTILE, j1 - t0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < m * 4; k += DTILE) tile[k] = src4[4 * t0 + k];
+    __syncthreads();
+    seg_tile(tile, m, xi, 0, 0, 0, L, bi, ii, k0);
+#pragma unroll 1
+    for (int im = 0; im < NIMG; im++) {
+      int ma, mb, mc;
+      qv_img_shift(BC, im, &ma, &mb, &mc);
+      seg_tile(tile, m, xi, ma, mb, mc, L, bi, -7, k1);
+    }
+  }
+  if (live) {
+    double *o = part + ((size_t)blockIdx.y * na + q) * 6;
+    for (int c = 0; c < 3; c++) { o[c] = k0.get(c); o[3 + c] = k1.get(c); }
+  }
+}
+
+// u_bs = s0 + s1, u = (u_li + s0) + s1, in fixed chunk order.
+__global__ void k_direct_reduce(int na, int nchunk, const int *__restrict__ act,
+                                const double *__restrict__ part, double scale,
+                                const double *__restrict__ u_li, double *u, double *u_bs) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= na) return;
+  int i = act[q];
+  double s0[3] = {0., 0., 0.}, s1[3] = {0., 0., 0.};
+  for (int k = 0; k < nchunk; k++) {
+    const double *o = part + ((size_t)k * na + q) * 6;
+    for (int c = 0; c < 3; c++) { s0[c] += o[c]; s1[c] += o[3 + c]; }
+  }
+  for (int c = 0; c < 3; c++) {
+    double b0 = s0[c] * scale, b1 = s1[c] * scale;
+    u_bs[3 * i + c] = b0 + b1;
+    u[3 * i + c] = (u_li[3 * i + c] + b0) + b1;
+  }
+}
+
+int qv_launch_direct(qv_ctx *c) {
+  int na = c->n_act;
+  if (na == 0) return QV_OK;
+  int tb = nblk(c->n_act, 256);
+  k_pack_sources<<<tb, 256, 0, c->stream>>>(na, c->act, c->x, c->gi, c->src64, c->src32);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  int bx = nblk(na, DTILE);
+  // enough chunks to fill ~4 blocks per SM, each chunk at least 4 tiles
+  int want = (4 * c->sm_count + bx - 1) / bx;
+  int maxch = max(1, na / (4 * DTILE));
+  int nchunk = max(1, min(want, maxch));
+  int chunk_len = ((nblk(na, nchunk) + DTILE - 1) / DTILE) * DTILE;
+  nchunk = nblk(na, chunk_len);
+  double *part = nullptr;
+  QV_CUDA(c, cudaMallocAsync((void **)&part, sizeof(double) * 6 * (size_t)na * nchunk, c->stream));
+  dim3 grid(bx, nchunk);
+  double L = c->p.box_size;
+  bool mixed = c->p.precision == QV_PREC_MIXED;
+  switch (c->p.boundary) {
+#define QV_DIRECT_CASE(BCV)                                                                   \
+  case BCV:                                                                                   \
+    if (mixed)                                                                                \
+      k_direct32<BCV><<<grid, DTILE, 0, c->stream>>>(na, c->act, c->x, c->behind, c->src32,  \
+                                                     chunk_len, L, part);                     \
+    else                                                                                      \
+      k_direct64<BCV><<<grid, DTILE, 0, c->stream>>>(na, c->act, c->x, c->behind, c->src64,  \
+                                                     chunk_len, L, part);                     \
+    break;
+    QV_DIRECT_CASE(QV_BC_OPEN)
+    QV_DIRECT_CASE(QV_BC_PERIODIC)
+    QV_DIRECT_CASE(QV_BC_OPENX)
+    QV_DIRECT_CASE(QV_BC_OPENXY)
+#undef QV_DIRECT_CASE
+    default:
+      cudaFreeAsync(part, c->stream);
+      return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
+  }
+  QV_LAUNCH_CHECK(c);
+  double scale = mixed ? c->p.quant_circ / (4. * QV_PI) : c->p.quant_circ / (2. * QV_PI);
+  k_direct_reduce<<<tb, 256, 0, c->stream>>>(na, nchunk, c->act, part, scale, c->u_li, c->u,
+                                             c->u_bs);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
+  QV_CUDA(c, cudaFreeAsync(part, c->stream));
+  return QV_OK;
+}

@@ -1,0 +1,190 @@
+// qv_internal.cuh -- shared definitions of the B200 filament path.
+//
+// Device data layout (HBM): one context holds one filament system.  Point
+// arrays keep the reference's slot order and interleaved xyz (x[3*i+c]) so a
+// host gather of f(:) copies straight in; links stay 1-based with 0 = empty.
+// The octree lives in flat node tables (breadth-first levels, children of a
+// node contiguous in the fbl..btr order), with walk-ready FP64 and FP32 packs.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/qv.h"
+
+#define QV_PI 3.14159265358979324  // src/cdata.f90:176
+#define QV_DEPS 2.220446049250313e-16  // epsilon(0.) under -fdefault-real-8
+
+// Walk-ready node header, FP64 (64 B).  cent, width and the geometric offset
+// geo = |cent - cell centre| (src/tree.f90:355-357) in FP64 so that every
+// opening decision is taken exactly as the reference takes it.
+struct __align__(16) WNode64 {
+  double cx, cy, cz;
+  double width, geo;
+  int count;        // pcount (the root counts every slot, src/tree.f90:51)
+  int child_first;  // first non-empty child; children are contiguous
+  int nchild;       // number of non-empty children
+  int jb;           // leaf: f(parray(1)%infront)%behind at build time (1-based)
+  int finf;         // parray(1)%infront at build time (1-based)
+  int pad;
+};
+
+// FP64 payload (128 B): leaf -> segment x, ghosti; internal -> circ, the
+// antisymmetric contraction w_m = sum_kl eps(m,k,l) C(k,l), and C (row-major).
+struct __align__(16) WPay64 {
+  double a[3];   // leaf x | circ
+  double b[3];   // leaf gi | w
+  double C[9];
+  double pad;
+};
+
+// FP32 header (48 B): cent as a two-float (hi, lo) split of the FP64 value so
+// that target-source differences keep FP64-level information.
+struct __align__(16) WNode32 {
+  float ch[3], cl[3];
+  float width, geo;
+  int count, child_first, nchild, jb;
+};
+
+// FP32 payload (64 B): internal -> circ, w, C; leaf -> ghosti as (hi, lo).
+struct __align__(16) WPay32 {
+  float a[3];  // circ | gi hi
+  float b[3];  // w | gi lo
+  float C[9];
+  float pad;
+};
+
+struct TreeBuf {
+  int cap_nodes = 0;  // allocated node slots
+  int cap_pts = 0;    // allocated point slots (active points)
+  int cap_levels = 0; // levels of per-level order storage
+  int n_nodes = 0, depth = 0, n_act = 0;
+  bool valid = false;
+  // node records (build)
+  double *pos = nullptr, *width = nullptr, *cent = nullptr, *circ = nullptr, *C = nullptr;
+  int *count = nullptr, *start = nullptr, *parent = nullptr, *child_first = nullptr,
+      *nchild = nullptr, *first = nullptr, *level = nullptr;
+  unsigned char *digit = nullptr, *cmask = nullptr;
+  // walk packs
+  WNode64 *w64 = nullptr;
+  WPay64 *p64 = nullptr;
+  WNode32 *w32 = nullptr;
+  WPay32 *p32 = nullptr;
+  // build scratch
+  int *ord = nullptr;       // cap_levels * cap_pts: per-level orders
+  int *nodeA = nullptr, *nodeB = nullptr;  // node of each position
+  unsigned char *dig = nullptr;
+  int *rnk = nullptr;
+  int *cnt9 = nullptr, *rs9 = nullptr;     // per node of a level
+  int *chunk9 = nullptr;                   // per chunk of positions
+  int *ctl = nullptr;                      // device control block
+  int *perm = nullptr;                     // final (DFS) order of active points
+  std::vector<int> lvl_start;
+};
+
+// Phases timed with CUDA events when profiling is on (qv_profile).
+enum { PH_GHOSTS = 0, PH_BUILD, PH_LIA, PH_NONLOCAL, PH_UPDATE, PH_CLOSEST, PH_WRAP, PH_N };
+
+struct qv_ctx {
+  qv_params p;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int n = 0, cap = 0;
+  double *x = nullptr, *u = nullptr, *u1 = nullptr, *u2 = nullptr, *u3 = nullptr;
+  double *gi = nullptr, *gb = nullptr, *gii = nullptr, *gbb = nullptr;
+  double *u_li = nullptr, *u_bs = nullptr, *closestd = nullptr;
+  int *infront = nullptr, *behind = nullptr, *closest = nullptr;
+  int *act = nullptr;  // compacted active slots (direct sums)
+  int n_act = 0;
+  double *src64 = nullptr;  // direct-sum source pack (FP64)
+  float *src32 = nullptr;   // direct-sum source pack (FP32 hi/lo)
+  unsigned long long *evals = nullptr;  // device eval counter
+  int *dstatus = nullptr;               // device status word
+  double *dscalar = nullptr;            // device scalar scratch
+  bool ghosts_valid = false;
+  TreeBuf tree;
+  int sm_count = 148;
+  // instrumentation
+  bool profile = false;
+  cudaEvent_t ev_beg[PH_N] = {}, ev_end[PH_N] = {};
+  bool ev_open[PH_N] = {};
+  double phase_ms[PH_N] = {};
+  long long launches = 0;
+  unsigned long long *evals_far = nullptr;
+  long long last_leaf = 0, last_far = 0;
+  char err[512] = {0};
+};
+
+// ---------------------------------------------------------------- errors
+int qv_fail(qv_ctx *c, int code, const char *fmt, ...);
+#define QV_CUDA(ctx, call)                                                     \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      return qv_fail((ctx), QV_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__,   \
+                     #call, cudaGetErrorString(e_));                           \
+  } while (0)
+#define QV_LAUNCH_CHECK(ctx) QV_CUDA(ctx, cudaGetLastError())
+
+int qv_grow(qv_ctx *c, void **ptr, size_t bytes);
+void qv_phase_begin(qv_ctx *c, int ph);
+void qv_phase_end(qv_ctx *c, int ph);
+void qv_phase_collect(qv_ctx *c);
+#define QV_COUNT(c, k) ((c)->launches += (k))
+
+// ---------------------------------------------------------------- kernels
+int qv_launch_ghosts(qv_ctx *c);
+int qv_launch_lia(qv_ctx *c);
+int qv_launch_direct(qv_ctx *c);
+int qv_launch_tree_build(qv_ctx *c);
+int qv_launch_walk(qv_ctx *c);
+int qv_launch_ab(qv_ctx *c);
+int qv_launch_rk3_stage(qv_ctx *c, int stage);
+int qv_launch_wrap(qv_ctx *c);
+int qv_launch_closest(qv_ctx *c);
+int qv_launch_energy(qv_ctx *c, double *out_host);
+int qv_compact_active(qv_ctx *c);
+
+// ---------------------------------------------------------------- helpers
+// Straight-segment Biot-Savart term in FP32, without the G/(4 pi) factor:
+//   (|R1|+|R2|) / (|R1||R2| (|R1||R2| + R1.R2)) * (R1 x R2)
+// (src/tree.f90:380-390), written with q = 1/(|R1||R2|) as
+//   (1/|R1| + 1/|R2|) q / (1 + cos) * (R1 x R2),  cos = R1.R2 q.
+// When cos < 0 the sum 1 + cos cancels; it is then taken from the identity
+// (1 + cos)(1 - cos) = sin^2 = |R1 x R2|^2 q^2, which has no cancellation.
+__device__ __forceinline__ void qv_seg32(float r1x, float r1y, float r1z, float r2x, float r2y,
+                                         float r2z, float r1s, float &ox, float &oy, float &oz) {
+  float r2s = fmaf(r2x, r2x, fmaf(r2y, r2y, r2z * r2z));
+  float dd = fmaf(r1x, r2x, fmaf(r1y, r2y, r1z * r2z));
+  float ra = rsqrtf(r1s), rb = rsqrtf(r2s);
+  float q = ra * rb;
+  float cx = fmaf(r1y, r2z, -r1z * r2y);
+  float cy = fmaf(r1z, r2x, -r1x * r2z);
+  float cz = fmaf(r1x, r2y, -r1y * r2x);
+  float cs = dd * q;
+  float den = cs >= 0.f ? 1.f + cs
+                        : fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
+  float f = (ra + rb) * q;
+  f = den > 0.f ? __fdividef(f, den) : 0.f;
+  ox = f * cx;
+  oy = f * cy;
+  oz = f * cz;
+}
+
+__host__ __device__ inline int qv_img_count(int bc) {
+  return bc == QV_BC_PERIODIC ? 26 : bc == QV_BC_OPENX ? 8 : bc == QV_BC_OPENXY ? 2 : 0;
+}
+// Shift multipliers of image m in the reference's loop order
+// (src/timestep.f90:235-257): peri, perj, perk from -1..1, skipping 0,0,0.
+__host__ __device__ inline void qv_img_shift(int bc, int m, int *a, int *b, int *cc) {
+  if (bc == QV_BC_PERIODIC) {
+    int q = m < 13 ? m : m + 1;
+    *a = q / 9 - 1; *b = (q / 3) % 3 - 1; *cc = q % 3 - 1;
+  } else if (bc == QV_BC_OPENX) {
+    int q = m < 4 ? m : m + 1;
+    *a = 0; *b = q / 3 - 1; *cc = q % 3 - 1;
+  } else {
+    *a = 0; *b = 0; *cc = m == 0 ? -1 : 1;
+  }
+}

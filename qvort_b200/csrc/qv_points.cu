@@ -1,0 +1,361 @@
+// qv_points.cu -- per-point O(N) kernels: ghost gather, LIA local term, the
+// Adams-Bashforth ladder, the RK3 stages, the periodic wrap and the energy.
+// All HBM-bound; one thread per slot, interleaved xyz loads.
+#include <cstdarg>
+#include <cstdio>
+
+#include "qv_internal.cuh"
+
+int qv_fail(qv_ctx *c, int code, const char *fmt, ...) {
+  if (c) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(c->err, sizeof(c->err), fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+int qv_grow(qv_ctx *c, void **ptr, size_t bytes) {
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  if (bytes == 0) return QV_OK;
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    cudaGetLastError();
+    return qv_fail(c, QV_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return QV_OK;
+}
+
+static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+// ---------------------------------------------------------------- ghosts
+// get_ghost_p, src/periodic.f90:23-165: positions of the +-1 and +-2
+// neighbours, shifted by +-L on every periodic axis where they differ from
+// x_i by more than L/2 (strict comparisons).
+__global__ void k_ghosts(int n, const double *__restrict__ x, const int *__restrict__ inf,
+                         const int *__restrict__ beh, double *gi, double *gb, double *gii,
+                         double *gbb, int lo_axis, double L) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int a = inf[i];
+  if (a == 0) return;
+  int b = beh[i];
+  int aa = inf[a - 1], bb = beh[b - 1];
+  int src[4] = {a - 1, b - 1, aa - 1, bb - 1};
+  double *dst[4] = {gi, gb, gii, gbb};
+  double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+  double h = L / 2.;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double g = x[3 * src[k] + c];
+      if (c >= lo_axis) {
+        if ((xi[c] - g) > h)
+          g = g + L;
+        else if ((xi[c] - g) < (-h))
+          g = g - L;
+      }
+      dst[k][3 * i + c] = g;
+    }
+  }
+}
+
+static int lo_axis_of(int bc) {
+  return bc == QV_BC_PERIODIC ? 0 : bc == QV_BC_OPENX ? 1 : bc == QV_BC_OPENXY ? 2 : 3;
+}
+
+int qv_launch_ghosts(qv_ctx *c) {
+  if (c->n == 0) return QV_OK;
+  k_ghosts<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->x, c->infront, c->behind, c->gi,
+                                                   c->gb, c->gii, c->gbb,
+                                                   lo_axis_of(c->p.boundary), c->p.box_size);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  c->ghosts_valid = true;
+  return QV_OK;
+}
+
+// ---------------------------------------------------------------- LIA
+__device__ __forceinline__ double ddist(const double *a, const double *b) {
+  double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+  return sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+}
+
+// get_deriv_1 / get_deriv_2, src/derivatives.f90:11-75 (second and fourth
+// order non-uniform finite differences on the ghost stencil).
+__device__ void derivs(int order, const double *x, const double *gi, const double *gb,
+                       const double *gii, const double *gbb, double *s1, double *s2) {
+  double disti = ddist(x, gi), distb = ddist(x, gb);
+  if (order != 4) {
+    double den1 = 2. * distb * disti;
+    double q1 = disti * (disti + distb), q2 = disti * distb, q3 = distb * (disti + distb);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      s1[c] = (distb * gi[c] + (disti - distb) * x[c] - disti * gb[c]) / den1;
+      s2[c] = 2. * (gi[c] / q1 - x[c] / q2 + gb[c] / q3);
+    }
+    return;
+  }
+  double dii = ddist(gii, gi), dbb = ddist(gbb, gb);
+  double di2 = disti * disti, db2 = distb * distb;
+  double dA = dbb * (dbb + distb) * (dbb + distb + disti) * (dbb + distb + disti + dii);
+  double dB = dbb * distb * (distb + disti) * (distb + disti + dii);
+  double dD = disti * dii * (distb + disti) * (dbb + distb + disti);
+  double dE = dii * (disti + dii) * (distb + disti + dii) * (dbb + distb + disti + dii);
+  double A = (distb * di2 + distb * disti * dii) / dA;
+  double B = (-dbb * di2 - distb * di2 - dbb * disti * dii - distb * disti * dii) / dB;
+  double D = (dbb * distb * disti + db2 * disti + dbb * distb * dii + db2 * dii) / dD;
+  double E = (-disti * db2 - dbb * distb * disti) / dE;
+  double C = -(A + B + D + E);
+  double A2 = 2. * (-2. * distb * disti + di2 - distb * dii + disti * dii) / dA;
+  double B2 = 2. * (2. * dbb * disti + 2. * distb * disti - di2 + dbb * dii + distb * dii - disti * dii) / dB;
+  double D2 = 2. * (-dbb * distb - db2 + dbb * disti + 2. * distb * disti + dbb * dii + 2. * distb * dii) / dD;
+  double E2 = 2. * (dbb * distb + db2 - dbb * disti - 2. * distb * disti) / dE;
+  double C2 = -(A2 + B2 + D2 + E2);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    s1[c] = A * gbb[c] + B * gb[c] + C * x[c] + D * gi[c] + E * gii[c];
+    s2[c] = A2 * gbb[c] + B2 * gb[c] + C2 * x[c] + D2 * gi[c] + E2 * gii[c];
+  }
+}
+
+// Local term of calc_velocity: LIA arm (src/timestep.f90:196-217) or the
+// local part of the BS/Tree arms (src/timestep.f90:221-225, 270-274).  The
+// log term stays FP64.  Writes u_li; for velocity LIA/Off also u.
+__global__ void k_lia(int n, const double *__restrict__ x, const int *__restrict__ inf,
+                      const double *__restrict__ gi, const double *__restrict__ gb,
+                      const double *__restrict__ gii, const double *__restrict__ gbb,
+                      double *u_li, double *u, int velocity, int order, int fixed_beta,
+                      double quant_circ, double corea) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (inf[i] == 0) return;
+  double X[3], GI[3], GB[3], GII[3], GBB[3], s1[3], s2[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    X[c] = x[3 * i + c]; GI[c] = gi[3 * i + c]; GB[c] = gb[3 * i + c];
+    GII[c] = gii[3 * i + c]; GBB[c] = gbb[3 * i + c];
+  }
+  double out[3] = {0., 0., 0.};
+  if (velocity != QV_VEL_OFF) {
+    derivs(order, X, GI, GB, GII, GBB, s1, s2);
+    double beta;
+    if (velocity == QV_VEL_LIA) {
+      if (fixed_beta) {
+        beta = 1.3E-3;
+      } else {
+        double curv = sqrt(s2[0] * s2[0] + s2[1] * s2[1] + s2[2] * s2[2]);
+        curv = curv < QV_DEPS ? QV_DEPS : 1. / curv;
+        beta = (quant_circ / (4. * QV_PI)) * log(curv / corea);
+      }
+    } else {
+      beta = (quant_circ / (4. * QV_PI)) * log((1.21 / corea) * sqrt(ddist(X, GI) * ddist(X, GB)));
+    }
+    out[0] = beta * (s1[1] * s2[2] - s1[2] * s2[1]);
+    out[1] = beta * (s1[2] * s2[0] - s1[0] * s2[2]);
+    out[2] = beta * (s1[0] * s2[1] - s1[1] * s2[0]);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) u_li[3 * i + c] = out[c];
+  if (velocity == QV_VEL_LIA || velocity == QV_VEL_OFF)
+#pragma unroll
+    for (int c = 0; c < 3; c++) u[3 * i + c] = out[c];
+}
+
+int qv_launch_lia(qv_ctx *c) {
+  if (c->n == 0) return QV_OK;
+  k_lia<<<nblk(c->n, 128), 128, 0, c->stream>>>(
+      c->n, c->x, c->infront, c->gi, c->gb, c->gii, c->gbb, c->u_li, c->u, c->p.velocity,
+      c->p.deriv_order, c->p.fixed_lia_beta, c->p.quant_circ, c->p.corea);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
+// ---------------------------------------------------------------- AB ladder
+// pmotion, src/timestep.f90:48-71.  The rung is picked per point by exact
+// zero tests on the history; products and sums are rounded one at a time
+// (no FMA) in the reference's evaluation order, so given the same velocities
+// the positions agree bit for bit with the reference arithmetic.
+__global__ void k_ab(int n, double dt, double *x, const double *__restrict__ u, double *u1,
+                     double *u2, double *u3, const int *__restrict__ inf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (inf[i] == 0) return;
+  double X[3], U[3], U1[3], U2[3], U3[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    X[c] = x[3 * i + c]; U[c] = u[3 * i + c]; U1[c] = u1[3 * i + c];
+    U2[c] = u2[3 * i + c]; U3[c] = u3[3 * i + c];
+  }
+  bool z1 = fabs(U1[0]) == 0 && fabs(U1[1]) == 0 && fabs(U1[2]) == 0;
+  bool z2 = fabs(U2[0]) == 0 && fabs(U2[1]) == 0 && fabs(U2[2]) == 0;
+  bool z3 = fabs(U3[0]) == 0 && fabs(U3[1]) == 0 && fabs(U3[2]) == 0;
+  const double three_twos = 3. / 2., one_half = 1. / 2., c23_12 = 23. / 12.,
+               c4_3 = 4. / 3., c5_12 = 5. / 12.;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double r;
+    if (z1) {
+      r = __dadd_rn(X[c], __dmul_rn(dt, U[c]));
+    } else if (z2) {
+      r = __dadd_rn(X[c], __dmul_rn(__dmul_rn(three_twos, dt), U[c]));
+      r = __dsub_rn(r, __dmul_rn(__dmul_rn(one_half, dt), U1[c]));
+    } else if (z3) {
+      r = __dadd_rn(X[c], __dmul_rn(__dmul_rn(c23_12, dt), U[c]));
+      r = __dsub_rn(r, __dmul_rn(__dmul_rn(c4_3, dt), U1[c]));
+      r = __dadd_rn(r, __dmul_rn(__dmul_rn(c5_12, dt), U2[c]));
+    } else {
+      double s = __dsub_rn(__dmul_rn(55., U[c]), __dmul_rn(59., U1[c]));
+      s = __dadd_rn(s, __dmul_rn(37., U2[c]));
+      s = __dsub_rn(s, __dmul_rn(9., U3[c]));
+      r = __dadd_rn(X[c], __ddiv_rn(__dmul_rn(dt, s), 24.));
+    }
+    x[3 * i + c] = r;
+    u3[3 * i + c] = U2[c];
+    u2[3 * i + c] = U1[c];
+    u1[3 * i + c] = U[c];
+  }
+}
+
+int qv_launch_ab(qv_ctx *c) {
+  if (c->n == 0) return QV_OK;
+  k_ab<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->p.dt, c->x, c->u, c->u1, c->u2,
+                                               c->u3, c->infront);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
+// ---------------------------------------------------------------- RK3
+// pmotion_RK3 stage updates, src/timestep.f90:105-175 (u1 is the RK register).
+__global__ void k_rk3(int n, int stage, double dt, double *x, const double *__restrict__ u,
+                      double *u1, const int *__restrict__ inf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (inf[i] == 0) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double uu = u[3 * i + c], q = u1[3 * i + c], xx = x[3 * i + c];
+    if (stage == 0) {
+      q = __dmul_rn(uu, dt);
+      xx = __dadd_rn(xx, __ddiv_rn(q, 3.));
+    } else if (stage == 1) {
+      q = __dadd_rn(__dmul_rn(-(2. / 3.), q), __dmul_rn(uu, dt));
+      xx = __dadd_rn(xx, q);
+    } else {
+      q = __dadd_rn(-q, __dmul_rn(uu, dt));
+      xx = __dadd_rn(xx, __dmul_rn(0.5, q));
+    }
+    u1[3 * i + c] = q;
+    x[3 * i + c] = xx;
+  }
+}
+
+int qv_launch_rk3_stage(qv_ctx *c, int stage) {
+  if (c->n == 0) return QV_OK;
+  k_rk3<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, stage, c->p.dt, c->x, c->u, c->u1,
+                                                c->infront);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
+// ---------------------------------------------------------------- wrap
+// enforce_periodic, src/periodic.f90:188-214 (and its yz / z variants).
+__global__ void k_wrap(int n, double *x, const int *__restrict__ inf, int lo_axis, double L) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (inf[i] == 0) return;
+  double h = L / 2.;
+  for (int c = lo_axis; c < 3; c++) {
+    double v = x[3 * i + c];
+    if (v > h)
+      x[3 * i + c] = v - L;
+    else if (v < (-h))
+      x[3 * i + c] = v + L;
+  }
+}
+
+int qv_launch_wrap(qv_ctx *c) {
+  int lo = lo_axis_of(c->p.boundary);
+  if (c->n == 0 || lo > 2) return QV_OK;
+  k_wrap<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->x, c->infront, lo, c->p.box_size);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
+// ---------------------------------------------------------------- energy
+// energy_info, src/diagnostic.f90:259-280.  Per-point terms in parallel, then
+// a fixed-order two-level sum (deterministic).
+__global__ void k_energy_terms(int n, const double *__restrict__ x, const double *__restrict__ u,
+                               const int *__restrict__ inf, const double *__restrict__ gi,
+                               const double *__restrict__ gb, const double *__restrict__ gii,
+                               const double *__restrict__ gbb, int order, double *blk_out) {
+  __shared__ double red[256];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.;
+  if (i < n && inf[i] != 0) {
+    int a = inf[i] - 1;
+    double s1[3], s2[3], t1[3], t2[3];
+    const int idx[2] = {i, a};
+    double dots[2];
+    for (int q = 0; q < 2; q++) {
+      int k = idx[q];
+      double X[3], GI[3], GB[3], GII[3], GBB[3];
+      for (int c = 0; c < 3; c++) {
+        X[c] = x[3 * k + c]; GI[c] = gi[3 * k + c]; GB[c] = gb[3 * k + c];
+        GII[c] = gii[3 * k + c]; GBB[c] = gbb[3 * k + c];
+      }
+      derivs(order, X, GI, GB, GII, GBB, s1, s2);
+      t1[0] = X[1] * s1[2] - X[2] * s1[1];
+      t1[1] = X[2] * s1[0] - X[0] * s1[2];
+      t1[2] = X[0] * s1[1] - X[1] * s1[0];
+      dots[q] = u[3 * k] * t1[0] + u[3 * k + 1] * t1[1] + u[3 * k + 2] * t1[2];
+      (void)t2;
+    }
+    double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+    double g[3] = {gi[3 * i], gi[3 * i + 1], gi[3 * i + 2]};
+    e = 0.5 * ddist(xi, g) * (dots[0] + dots[1]);
+  }
+  red[threadIdx.x] = e;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) blk_out[blockIdx.x] = red[0];
+}
+
+__global__ void k_energy_final(int nb, const double *blk, double *out, double quant_circ) {
+  __shared__ double red[256];
+  double s = 0.;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) s += blk[k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int t = blockDim.x / 2; t > 0; t >>= 1) {
+    if (threadIdx.x < t) red[threadIdx.x] += red[threadIdx.x + t];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = red[0] * quant_circ;
+}
+
+int qv_launch_energy(qv_ctx *c, double *out_host) {
+  int nb = nblk(c->n, 256);
+  double *blk = nullptr;
+  QV_CUDA(c, cudaMallocAsync((void **)&blk, sizeof(double) * (nb + 1), c->stream));
+  k_energy_terms<<<nb, 256, 0, c->stream>>>(c->n, c->x, c->u, c->infront, c->gi, c->gb, c->gii,
+                                            c->gbb, c->p.deriv_order, blk);
+  k_energy_final<<<1, 256, 0, c->stream>>>(nb, blk, blk + nb, c->p.quant_circ);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
+  QV_CUDA(c, cudaMemcpyAsync(out_host, blk + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaFreeAsync(blk, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}

@@ -1,0 +1,624 @@
+// qv_tree.cu -- the octree of construct_tree / build_tree / new_tree
+// (src/tree.f90:44-186), built bit-exactly on the GPU.
+//
+// What "bit-exact" has to reproduce:
+//  * cell corners are formed by repeated FP64 additions pos + width/2 along
+//    the path from the root (src/tree.f90:92-114), and membership is the
+//    half-open test x >= pos, x < pos + width on every axis
+//    (src/tree.f90:148-150).  Rounding in those additions can leave a point of
+//    a parent in no child; such a point is counted by the parent only.
+//  * the root counts every slot, empty ones included (src/tree.f90:51); its
+//    centroid is the masked mean of all active points; its circ and Cij are 0.
+//  * every other node's moments are sequential FP64 sums over its points in
+//    ascending slot order (src/tree.f90:146-179): cent = sum x / n,
+//    circ = (circ + ghosti) - x, Cij(:,k) += x (ghosti_k - x_k), then
+//    Cij(i,k) -= cent_i circ_k.
+//
+// How: a level-synchronous build in one cooperative kernel.  Each point of a
+// splitting node gets its child digit (0..7 in fbl..btr order, 8 = in no
+// child) from the node's corner with __dadd_rn arithmetic; a stable segmented
+// partition by digit then yields, for every level, an order array in which
+// each node's points are contiguous and still in ascending slot order (the
+// key (node prefix, slot) -- the Morton-style ordering, radix-partitioned one
+// octal digit per level).  A separate kernel runs the moment chains of all
+// nodes of all levels concurrently, one warp per node, with explicit
+// round-to-nearest FP64 intrinsics so no FMA contraction changes a bit.
+#include <cooperative_groups.h>
+
+#include "qv_internal.cuh"
+
+namespace cg = cooperative_groups;
+
+static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+#define BT 256       // build threads per block
+#define PPT 4        // positions per thread in a chunk
+#define CH (BT * PPT)  // positions per chunk
+#define NOD 0xFF     // digit marker: position not in a splitting node
+
+// control block layout
+#define CTL_NNODES 0
+#define CTL_NSPLIT 1
+#define CTL_NSPLIT_NEXT 2
+#define CTL_OVERFLOW 3  // 1 = node capacity, 2 = level capacity
+#define CTL_DEPTH 4
+#define CTL_LVL 8       // lvl_start[0..QV_MAX_DEPTH+2]
+#define CTL_SIZE (CTL_LVL + QV_MAX_DEPTH + 4)
+
+struct BuildArgs {
+  int n_act, n_slots, cap_pts, cap_nodes, cap_levels, nchunks;
+  const double *x, *gi;
+  double *pos, *width;
+  int *count, *start, *parent, *child_first, *nchild, *level;
+  unsigned char *digit, *cmask;
+  int *ord, *nodeA, *nodeB, *rnk, *cnt9A, *cnt9B, *rs9, *chunk9, *ctl;
+  unsigned char *dig;
+};
+
+// packed per-digit counters: digits 0..4 in lo (12-bit fields), 5..8 in hi
+struct Pack2 {
+  unsigned long long lo, hi;
+};
+__device__ __forceinline__ Pack2 pk_one(int g) {
+  Pack2 r{0ull, 0ull};
+  if (g < 5) r.lo = 1ull << (12 * g);
+  else if (g < 9) r.hi = 1ull << (12 * (g - 5));
+  return r;
+}
+__device__ __forceinline__ int pk_get(const Pack2 &p, int g) {
+  return g < 5 ? (int)((p.lo >> (12 * g)) & 0xFFF) : (int)((p.hi >> (12 * (g - 5))) & 0xFFF);
+}
+
+// Block-wide exclusive scan of Pack2 (BT threads); returns exclusive prefix
+// and writes the block total to *tot (all threads).
+__device__ Pack2 block_scan_pack(Pack2 v, Pack2 *tot, Pack2 *sh) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Pack2 inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long a = __shfl_up_sync(0xffffffffu, inc.lo, o);
+    unsigned long long b = __shfl_up_sync(0xffffffffu, inc.hi, o);
+    if (lane >= o) { inc.lo += a; inc.hi += b; }
+  }
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Pack2 r{0ull, 0ull};
+    for (int k = 0; k < BT / 32; k++) {
+      Pack2 t = sh[k];
+      sh[k] = r;
+      r.lo += t.lo; r.hi += t.hi;
+    }
+    sh[BT / 32] = r;
+  }
+  __syncthreads();
+  Pack2 ex;
+  ex.lo = sh[wid].lo + inc.lo - v.lo;
+  ex.hi = sh[wid].hi + inc.hi - v.hi;
+  *tot = sh[BT / 32];
+  __syncthreads();
+  return ex;
+}
+
+// child digit of point X in the node with corner P and width W
+// (src/tree.f90:92-114, 148-150).  8 = in no child.
+__device__ __forceinline__ int child_digit(const double *X, const double *P, double W) {
+  double w = W * 0.5;
+  int b[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double cm = __dadd_rn(P[c], w);   // child corner (right) = upper bound (left)
+    double up = __dadd_rn(cm, w);     // upper bound (right)
+    if (X[c] >= P[c] && X[c] < cm) b[c] = 0;
+    else if (X[c] >= cm && X[c] < up) b[c] = 1;
+    else b[c] = -1;
+  }
+  if (b[0] < 0 || b[1] < 0 || b[2] < 0) return 8;
+  return b[0] + 2 * b[2] + 4 * b[1];
+}
+
+__global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ Pack2 sh[BT / 32 + 1];
+  __shared__ int s9[BT / 32][9];
+  volatile int *ctl = a.ctl;
+  int d = 0;
+  for (;;) {
+    int nsplit = ctl[CTL_NSPLIT];
+    if (nsplit == 0) break;
+    if (d + 1 >= a.cap_levels || d + 1 > QV_MAX_DEPTH) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_OVERFLOW] = 2;
+      break;
+    }
+    const int ls = ctl[CTL_LVL + d], le = ctl[CTL_LVL + d + 1];
+    const int *ordc = a.ord + (size_t)d * a.cap_pts;
+    int *ordn = a.ord + (size_t)(d + 1) * a.cap_pts;
+    const int *nodc = (d & 1) ? a.nodeB : a.nodeA;
+    int *nodn = (d & 1) ? a.nodeA : a.nodeB;
+    int *cntc = (d & 1) ? a.cnt9B : a.cnt9A;
+    int *cntn = (d & 1) ? a.cnt9A : a.cnt9B;
+
+    // ---- P1: digits, node counts, chunk counts
+    for (int ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+      Pack2 loc{0ull, 0ull};
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        int p = ch * CH + threadIdx.x * PPT + j;
+        int g = NOD, key = -1;
+        if (p < a.n_act) {
+          int k = nodc[p];
+          if (k >= 0 && a.count[k] >= 2) {
+            int s = ordc[p];
+            double X[3] = {a.x[3 * s], a.x[3 * s + 1], a.x[3 * s + 2]};
+            double P[3] = {a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]};
+            g = child_digit(X, P, a.width[k]);
+            key = (k - ls) * 9 + g;
+          }
+          a.dig[p] = (unsigned char)g;
+        }
+        // warp-aggregated node counts
+        unsigned act = __ballot_sync(0xffffffffu, key >= 0);
+        if (key >= 0) {
+          unsigned peers = __match_any_sync(act, key);
+          int leader = __ffs(peers) - 1;
+          if ((int)(threadIdx.x & 31) == leader) atomicAdd(&cntc[key], __popc(peers));
+        }
+        if (g != NOD) {
+          Pack2 o = pk_one(g);
+          loc.lo += o.lo; loc.hi += o.hi;
+        }
+      }
+      Pack2 tot;
+      block_scan_pack(loc, &tot, sh);
+      if (threadIdx.x < 9) a.chunk9[ch * 9 + threadIdx.x] = pk_get(tot, threadIdx.x);
+    }
+    grid.sync();
+
+    // ---- P2: children (all blocks), chunk prefix scan (block 0)
+    for (int k = ls + blockIdx.x * BT + threadIdx.x; k < le; k += gridDim.x * BT) {
+      if (a.count[k] < 2) { a.nchild[k] = 0; a.cmask[k] = 0; continue; }
+      int c9[9];
+      int nc = 0, nsp = 0;
+      unsigned mask = 0;
+      for (int g = 0; g < 9; g++) c9[g] = cntc[(k - ls) * 9 + g];
+      for (int g = 0; g < 8; g++)
+        if (c9[g] > 0) { nc++; mask |= 1u << g; if (c9[g] >= 2) nsp++; }
+      int base = atomicAdd((int *)&ctl[CTL_NNODES], nc);
+      if (base + nc > a.cap_nodes) {
+        ctl[CTL_OVERFLOW] = 1;
+        continue;
+      }
+      if (nsp) atomicAdd((int *)&ctl[CTL_NSPLIT_NEXT], nsp);
+      a.child_first[k] = base;
+      a.nchild[k] = nc;
+      a.cmask[k] = (unsigned char)mask;
+      double W = a.width[k], w = W * 0.5;
+      double P[3] = {a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]};
+      double M[3] = {__dadd_rn(P[0], W / 2), __dadd_rn(P[1], W / 2), __dadd_rn(P[2], W / 2)};
+      int off = 0, id = base;
+      for (int g = 0; g < 8; g++) {
+        if (c9[g] > 0) {
+          int bx = g & 1, bz = (g >> 1) & 1, by = (g >> 2) & 1;
+          a.pos[3 * id] = bx ? M[0] : P[0];
+          a.pos[3 * id + 1] = by ? M[1] : P[1];
+          a.pos[3 * id + 2] = bz ? M[2] : P[2];
+          a.width[id] = w;
+          a.count[id] = c9[g];
+          a.start[id] = a.start[k] + off;
+          a.parent[id] = k;
+          a.level[id] = d + 1;
+          a.digit[id] = (unsigned char)g;
+          a.nchild[id] = 0;
+          a.cmask[id] = 0;
+          a.child_first[id] = -1;
+          id++;
+        }
+        off += c9[g];
+      }
+    }
+    if (blockIdx.x == 0) {
+      // exclusive scan of chunk9 over chunks, 9 channels
+      int per = (a.nchunks + BT - 1) / BT;
+      int lo = threadIdx.x * per, hi = min(a.nchunks, lo + per);
+      int sum[9];
+#pragma unroll
+      for (int g = 0; g < 9; g++) sum[g] = 0;
+      for (int q = lo; q < hi; q++)
+#pragma unroll
+        for (int g = 0; g < 9; g++) sum[g] += a.chunk9[q * 9 + g];
+      int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      int inc[9];
+#pragma unroll
+      for (int g = 0; g < 9; g++) {
+        int v = sum[g];
+        for (int o = 1; o < 32; o <<= 1) {
+          int t = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o) v += t;
+        }
+        inc[g] = v;
+        if (lane == 31) s9[wid][g] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < 9) {
+        int r = 0;
+        for (int w2 = 0; w2 < BT / 32; w2++) { int t = s9[w2][threadIdx.x]; s9[w2][threadIdx.x] = r; r += t; }
+      }
+      __syncthreads();
+      int run[9];
+#pragma unroll
+      for (int g = 0; g < 9; g++) run[g] = s9[wid][g] + inc[g] - sum[g];
+      for (int q = lo; q < hi; q++)
+#pragma unroll
+        for (int g = 0; g < 9; g++) {
+          int t = a.chunk9[q * 9 + g];
+          a.chunk9[q * 9 + g] = run[g];
+          run[g] += t;
+        }
+    }
+    grid.sync();
+    if (ctl[CTL_OVERFLOW]) break;
+
+    // ---- P3: stable ranks within digit channels; node-start snapshots
+    for (int ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+      Pack2 loc{0ull, 0ull};
+      int gs[PPT];
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        int p = ch * CH + threadIdx.x * PPT + j;
+        gs[j] = p < a.n_act ? a.dig[p] : NOD;
+        if (gs[j] != NOD) { Pack2 o = pk_one(gs[j]); loc.lo += o.lo; loc.hi += o.hi; }
+      }
+      Pack2 tot;
+      Pack2 ex = block_scan_pack(loc, &tot, sh);
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        int p = ch * CH + threadIdx.x * PPT + j;
+        int g = gs[j];
+        if (g != NOD) {
+          int k = nodc[p];
+          a.rnk[p] = a.chunk9[ch * 9 + g] + pk_get(ex, g);
+          if (p == a.start[k]) {
+            for (int h = 0; h < 9; h++) a.rs9[(k - ls) * 9 + h] = a.chunk9[ch * 9 + h] + pk_get(ex, h);
+          }
+          Pack2 o = pk_one(g);
+          ex.lo += o.lo; ex.hi += o.hi;
+        }
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_LVL + d + 2] = ctl[CTL_NNODES];
+    grid.sync();
+
+    // ---- P4: scatter into the next level's order; reset counters
+    const int le2 = ctl[CTL_LVL + d + 2];
+    for (int p = blockIdx.x * BT + threadIdx.x; p < a.n_act; p += gridDim.x * BT) {
+      int g = a.dig[p];
+      if (g == NOD) {
+        ordn[p] = ordc[p];
+        nodn[p] = -1;
+      } else {
+        int k = nodc[p], kl = k - ls;
+        int off = 0;
+        for (int h = 0; h < g; h++) off += cntc[kl * 9 + h];
+        int np = a.start[k] + off + a.rnk[p] - a.rs9[kl * 9 + g];
+        ordn[np] = ordc[p];
+        nodn[np] = g < 8 ? a.child_first[k] + __popc(a.cmask[k] & ((1u << g) - 1)) : -1;
+      }
+    }
+    for (int q = blockIdx.x * BT + threadIdx.x; q < (le2 - le) * 9; q += gridDim.x * BT) cntn[q] = 0;
+    grid.sync();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl[CTL_NSPLIT] = ctl[CTL_NSPLIT_NEXT];
+      ctl[CTL_NSPLIT_NEXT] = 0;
+    }
+    d++;
+    grid.sync();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_DEPTH] = d;
+}
+
+// --------------------------------------------------------------- moments
+#define MW 8  // warps per block
+__global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__restrict__ level,
+                                                     const int *__restrict__ start,
+                                                     const int *__restrict__ count,
+                                                     const int *__restrict__ ord, int cap_pts,
+                                                     const double *__restrict__ x,
+                                                     const double *__restrict__ gi, double *cent,
+                                                     double *circ, double *C, int *first) {
+  __shared__ double buf[MW][32][15];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = 1 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
+    int s = start[k], n = count[k];
+    const int *o = ord + (size_t)level[k] * cap_pts + s;
+    double acc = 0.;
+    for (int base = 0; base < n; base += 32) {
+      int m = min(32, n - base);
+      if (lane < m) {
+        int idx = o[base + lane];
+        double X[3], G[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
+        double *b = buf[wid][lane];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { b[c] = X[c]; b[3 + c] = G[c]; }
+#pragma unroll
+        for (int mm = 0; mm < 3; mm++)
+#pragma unroll
+          for (int kk = 0; kk < 3; kk++) b[6 + 3 * mm + kk] = __dmul_rn(X[mm], __dsub_rn(G[kk], X[kk]));
+      }
+      __syncwarp();
+      if (lane < 3) {
+        for (int q = 0; q < m; q++) acc = __dadd_rn(acc, buf[wid][q][lane]);
+      } else if (lane < 6) {
+        int c = lane - 3;
+        for (int q = 0; q < m; q++) acc = __dsub_rn(__dadd_rn(acc, buf[wid][q][3 + c]), buf[wid][q][c]);
+      } else if (lane < 15) {
+        for (int q = 0; q < m; q++) acc = __dadd_rn(acc, buf[wid][q][lane]);
+      }
+      __syncwarp();
+    }
+    double cm = lane < 3 ? __ddiv_rn(acc, (double)n) : 0.;
+    // C(i,k) -= cent_i circ_k  (lane 6+3i+k)
+    int ci = (lane - 6) / 3, ck = (lane - 6) % 3;
+    double cen = __shfl_sync(0xffffffffu, cm, lane >= 6 && lane < 15 ? ci : 0);
+    double cir = __shfl_sync(0xffffffffu, acc, lane >= 6 && lane < 15 ? 3 + ck : 0);
+    if (lane < 3) cent[3 * k + lane] = cm;
+    else if (lane < 6) circ[3 * k + lane - 3] = acc;
+    else if (lane < 15) C[9 * k + 3 * ci + ck] = __dsub_rn(acc, __dmul_rn(cen, cir));
+    if (lane == 0) first[k] = o[0];
+  }
+}
+
+// Root centroid: masked mean over all slots in ascending order
+// (src/tree.f90:53-55), sequential per component.
+__global__ void k_root_cent(int n, const double *__restrict__ x, const int *__restrict__ inf,
+                            double *cent) {
+  __shared__ double bx[32][3];
+  __shared__ int ba[32];
+  int lane = threadIdx.x;
+  double acc = 0.;
+  int cnt = 0;
+  for (int base = 0; base < n; base += 32) {
+    int m = min(32, n - base);
+    if (lane < m) {
+      int i = base + lane;
+      ba[lane] = inf[i] > 0;
+      for (int c = 0; c < 3; c++) bx[lane][c] = x[3 * i + c];
+    }
+    __syncwarp();
+    if (lane < 3)
+      for (int q = 0; q < m; q++)
+        if (ba[q]) acc = __dadd_rn(acc, bx[q][lane]);
+    if (lane == 3)
+      for (int q = 0; q < m; q++) cnt += ba[q];
+    __syncwarp();
+  }
+  cnt = __shfl_sync(0xffffffffu, cnt, 3);
+  if (lane < 3) cent[lane] = __ddiv_rn(acc, (double)cnt);
+}
+
+// ------------------------------------------------------------ walk packs
+__device__ __forceinline__ void split2(double v, float &h, float &l) {
+  h = __double2float_rn(v);
+  l = __double2float_rn(v - (double)h);
+}
+
+__global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict__ pos,
+                             const double *__restrict__ width, const double *__restrict__ cent,
+                             const double *__restrict__ circ, const double *__restrict__ C,
+                             const int *__restrict__ count, const int *__restrict__ child_first,
+                             const int *__restrict__ nchild, const int *__restrict__ first,
+                             const double *__restrict__ x, const double *__restrict__ gi,
+                             const int *__restrict__ inf, const int *__restrict__ beh,
+                             WNode64 *w64, WPay64 *p64, WNode32 *w32, WPay32 *p32) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_nodes) return;
+  WNode64 h;
+  h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
+  h.width = width[k];
+  // geo_dist = |cent - (pos + width/2.)|, src/tree.f90:355-357
+  double hw = width[k] / 2.;
+  double g0 = __dsub_rn(h.cx, __dadd_rn(pos[3 * k], hw));
+  double g1 = __dsub_rn(h.cy, __dadd_rn(pos[3 * k + 1], hw));
+  double g2 = __dsub_rn(h.cz, __dadd_rn(pos[3 * k + 2], hw));
+  h.geo = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(g0, g0), __dmul_rn(g1, g1)), __dmul_rn(g2, g2)));
+  int cnt = k == 0 ? n_slots : count[k];
+  h.count = cnt;
+  h.child_first = child_first[k];
+  h.nchild = nchild[k];
+  int f = first[k];
+  h.finf = (f >= 0) ? inf[f] : 0;
+  h.jb = (f >= 0 && h.finf > 0) ? beh[h.finf - 1] : 0;
+  h.pad = 0;
+  w64[k] = h;
+  WPay64 q;
+  WPay32 r;
+  WNode32 h32;
+  split2(h.cx, h32.ch[0], h32.cl[0]);
+  split2(h.cy, h32.ch[1], h32.cl[1]);
+  split2(h.cz, h32.ch[2], h32.cl[2]);
+  h32.width = __double2float_rn(h.width);
+  h32.geo = __double2float_rn(h.geo);
+  h32.count = cnt;
+  h32.child_first = h.child_first;
+  h32.nchild = h.nchild;
+  h32.jb = h.jb;
+  w32[k] = h32;
+  if (cnt == 1 && f >= 0) {
+    for (int c = 0; c < 3; c++) {
+      q.a[c] = x[3 * f + c];
+      q.b[c] = gi[3 * f + c];
+      split2(q.b[c], r.a[c], r.b[c]);
+    }
+    for (int c = 0; c < 9; c++) { q.C[c] = 0.; r.C[c] = 0.f; }
+  } else {
+    const double *M = C + 9 * k;
+    for (int c = 0; c < 3; c++) q.a[c] = k == 0 ? 0. : circ[3 * k + c];
+    if (k == 0) {
+      for (int c = 0; c < 9; c++) q.C[c] = 0.;
+    } else {
+      for (int c = 0; c < 9; c++) q.C[c] = M[c];
+    }
+    // w_m = sum_kl eps(m,k,l) C(k,l)
+    q.b[0] = q.C[5] - q.C[7];
+    q.b[1] = q.C[6] - q.C[2];
+    q.b[2] = q.C[1] - q.C[3];
+    for (int c = 0; c < 3; c++) { r.a[c] = (float)q.a[c]; r.b[c] = (float)q.b[c]; }
+    for (int c = 0; c < 9; c++) r.C[c] = (float)q.C[c];
+  }
+  q.pad = 0.;
+  r.pad = 0.f;
+  p64[k] = q;
+  p32[k] = r;
+}
+
+__global__ void k_root_record(double *pos, double *width, int *count, int *start, int *parent,
+                              int *child_first, int *nchild, int *level, unsigned char *digit,
+                              unsigned char *cmask, int *first, double L, int n_slots) {
+  pos[0] = -L / 2.; pos[1] = -L / 2.; pos[2] = -L / 2.;
+  width[0] = L;
+  count[0] = n_slots;
+  start[0] = 0;
+  parent[0] = -1;
+  child_first[0] = -1;
+  nchild[0] = 0;
+  level[0] = 0;
+  digit[0] = 0xFF;
+  cmask[0] = 0;
+  first[0] = n_slots > 0 ? 0 : -1;
+}
+
+// --------------------------------------------------------------- host side
+static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
+  TreeBuf &t = c->tree;
+  int rc;
+  if (n_act > t.cap_pts || cap_levels > t.cap_levels) {
+    int np = std::max(n_act, t.cap_pts);
+    int nl = std::max(cap_levels, t.cap_levels);
+    if ((rc = qv_grow(c, (void **)&t.ord, sizeof(int) * (size_t)np * nl))) return rc;
+    t.cap_levels = nl;
+    if (np > t.cap_pts) {
+      if ((rc = qv_grow(c, (void **)&t.nodeA, sizeof(int) * np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.nodeB, sizeof(int) * np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.dig, np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.rnk, sizeof(int) * np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.cnt9, sizeof(int) * 9 * (size_t)(2 * np + 2)))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.rs9, sizeof(int) * 9 * (size_t)(np + 1)))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.chunk9, sizeof(int) * 9 * (size_t)(np / CH + 2)))) return rc;
+      t.cap_pts = np;
+    }
+  }
+  if (!t.ctl)
+    if ((rc = qv_grow(c, (void **)&t.ctl, sizeof(int) * CTL_SIZE))) return rc;
+  if (cap_nodes > t.cap_nodes) {
+    size_t m = cap_nodes;
+    if ((rc = qv_grow(c, (void **)&t.pos, sizeof(double) * 3 * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.width, sizeof(double) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.cent, sizeof(double) * 3 * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.circ, sizeof(double) * 3 * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.C, sizeof(double) * 9 * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.count, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.start, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.parent, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.child_first, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.nchild, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.first, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.level, sizeof(int) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.digit, m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.cmask, m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.w64, sizeof(WNode64) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.p64, sizeof(WPay64) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.w32, sizeof(WNode32) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.p32, sizeof(WPay32) * m))) return rc;
+    t.cap_nodes = cap_nodes;
+  }
+  return QV_OK;
+}
+
+static int build_grid(qv_ctx *c) {
+  static int cached = 0;
+  if (cached) return cached;
+  int per = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_build, BT, 0);
+  if (per < 1) per = 1;
+  if (per > 2) per = 2;
+  cached = per * c->sm_count;
+  return cached;
+}
+
+int qv_launch_tree_build(qv_ctx *c) {
+  TreeBuf &t = c->tree;
+  t.valid = false;
+  int rc;
+  if (!c->ghosts_valid)
+    if ((rc = qv_launch_ghosts(c))) return rc;
+  if ((rc = qv_compact_active(c))) return rc;
+  int na = c->n_act;
+  int cap_nodes = std::max(t.cap_nodes, 4 * na + 64);
+  int cap_levels = std::max(t.cap_levels, std::min(QV_MAX_DEPTH + 1, 40));
+  for (int attempt = 0; attempt < 8; attempt++) {
+    if ((rc = tree_reserve(c, na, cap_nodes, cap_levels))) return rc;
+    k_root_record<<<1, 1, 0, c->stream>>>(t.pos, t.width, t.count, t.start, t.parent,
+                                          t.child_first, t.nchild, t.level, t.digit, t.cmask,
+                                          t.first, c->p.box_size, c->n);
+    QV_LAUNCH_CHECK(c);
+    if (na > 0)
+      QV_CUDA(c, cudaMemcpyAsync(t.ord, c->act, sizeof(int) * na, cudaMemcpyDeviceToDevice, c->stream));
+    QV_CUDA(c, cudaMemsetAsync(t.nodeA, 0, sizeof(int) * std::max(na, 1), c->stream));
+    QV_CUDA(c, cudaMemsetAsync(t.cnt9, 0, sizeof(int) * 9 * (size_t)(2 * t.cap_pts + 2), c->stream));
+    int h[CTL_SIZE] = {0};
+    h[CTL_NNODES] = 1;
+    h[CTL_NSPLIT] = (c->n > 1 && na > 0) ? 1 : 0;
+    h[CTL_LVL + 0] = 0;
+    h[CTL_LVL + 1] = 1;
+    QV_CUDA(c, cudaMemcpyAsync(t.ctl, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    BuildArgs a;
+    a.n_act = na; a.n_slots = c->n; a.cap_pts = t.cap_pts; a.cap_nodes = t.cap_nodes;
+    a.cap_levels = t.cap_levels; a.nchunks = std::max(1, nblk(na, CH));
+    a.x = c->x; a.gi = c->gi; a.pos = t.pos; a.width = t.width; a.count = t.count;
+    a.start = t.start; a.parent = t.parent; a.child_first = t.child_first; a.nchild = t.nchild;
+    a.level = t.level; a.digit = t.digit; a.cmask = t.cmask; a.ord = t.ord; a.nodeA = t.nodeA;
+    a.nodeB = t.nodeB; a.rnk = t.rnk; a.cnt9A = t.cnt9; a.cnt9B = t.cnt9 + 9 * (size_t)(t.cap_pts + 1);
+    a.rs9 = t.rs9; a.chunk9 = t.chunk9; a.ctl = t.ctl; a.dig = t.dig;
+    int grid = std::min(build_grid(c), std::max(1, a.nchunks) * 4);
+    grid = std::max(grid, 1);
+    void *args[] = {&a};
+    QV_CUDA(c, cudaLaunchCooperativeKernel((void *)k_build, grid, BT, args, 0, c->stream));
+    QV_COUNT(c, 2);
+    QV_CUDA(c, cudaMemcpyAsync(h, t.ctl, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    QV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (h[CTL_OVERFLOW] == 1) { cap_nodes *= 2; continue; }
+    if (h[CTL_OVERFLOW] == 2) {
+      if (cap_levels >= QV_MAX_DEPTH + 1)
+        return qv_fail(c, QV_ERR_TREE_DEPTH,
+                       "octree deeper than %d levels (coincident or nearly coincident points)",
+                       QV_MAX_DEPTH);
+      cap_levels = QV_MAX_DEPTH + 1;
+      continue;
+    }
+    t.n_nodes = h[CTL_NNODES];
+    t.depth = h[CTL_DEPTH];
+    t.n_act = na;
+    t.lvl_start.assign(h + CTL_LVL, h + CTL_LVL + t.depth + 2);
+    t.perm = t.ord + (size_t)t.depth * t.cap_pts;
+    // moments of all non-root nodes, then the root centroid
+    if (t.n_nodes > 1) {
+      int nb = std::min(nblk(t.n_nodes - 1, MW), 16 * c->sm_count);
+      k_moments<<<nb, MW * 32, 0, c->stream>>>(t.n_nodes, t.level, t.start, t.count, t.ord,
+                                               t.cap_pts, c->x, c->gi, t.cent, t.circ, t.C,
+                                               t.first);
+      QV_LAUNCH_CHECK(c);
+      QV_COUNT(c, 1);
+    }
+    k_root_cent<<<1, 32, 0, c->stream>>>(c->n, c->x, c->infront, t.cent);
+    QV_LAUNCH_CHECK(c);
+    k_pack_nodes<<<nblk(t.n_nodes, 128), 128, 0, c->stream>>>(
+        t.n_nodes, c->n, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first, t.nchild,
+        t.first, c->x, c->gi, c->infront, c->behind, t.w64, t.p64, t.w32, t.p32);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 2);
+    t.valid = true;
+    return QV_OK;
+  }
+  return qv_fail(c, QV_ERR_NOMEM, "tree build did not fit after repeated growth");
+}

@@ -1,0 +1,415 @@
+// qv_walk.cu -- Barnes-Hut tree walk of calc_velocity's Tree arm
+// (tree_walk, src/tree.f90:336-421; image loop src/timestep.f90:276-307).
+//
+// Execution model: one warp walks the tree for 32 targets that are adjacent
+// in the tree's depth-first point order (so their traversals overlap).  The
+// warp keeps one explicit stack of (node, lane mask) in shared memory: at each
+// node every lane in the mask takes its own decision exactly as the reference
+// does (leaf -> exact segment, theta < tree_theta -> far-field multipole,
+// else open), and children are pushed with the mask of the lanes that opened
+// the node.  Each lane therefore visits exactly the nodes its own recursive
+// walk would visit, in the same depth-first child order, while node headers
+// are fetched once per warp (broadcast loads) instead of once per target.
+//
+// Opening decisions are always the reference's FP64 decisions: the FP64 walk
+// computes them with round-to-nearest intrinsics; the mixed walk evaluates
+// them in FP32 with a rigorous margin and falls back to the FP64 expression
+// when a decision is within that margin, so both walks visit identical nodes.
+//
+// The root counts every slot and carries zero circ/Cij (src/tree.f90:51-58):
+// when an image's root passes the opening test the image adds nothing, as in
+// the reference.
+#include "qv_internal.cuh"
+
+#define WW 4                           // warps per block
+#define STK (7 * QV_MAX_DEPTH + 16)    // stack entries per warp
+
+struct WalkArgs {
+  int n_act;
+  const int *perm;
+  const double *x;
+  const int *inf, *beh;
+  const WNode64 *w64;
+  const WPay64 *p64;
+  const WNode32 *w32;
+  const WPay32 *p32;
+  const double *u_li;
+  double *u, *u_bs;
+  double L, theta, gfac;
+  int extra;
+  unsigned long long *evals, *evals_far;
+  int *status;
+};
+
+__device__ __forceinline__ double shift_of(int m, double L) {
+  return m == 0 ? 0. : (m > 0 ? L : -L);
+}
+
+// dist = |x_i - (cent + shift)| in the reference's operation order.
+__device__ __forceinline__ double exact_dist(const double *xi, const WNode64 &h, const double *s) {
+  double d0 = __dsub_rn(xi[0], __dadd_rn(h.cx, s[0]));
+  double d1 = __dsub_rn(xi[1], __dadd_rn(h.cy, s[1]));
+  double d2 = __dsub_rn(xi[2], __dadd_rn(h.cz, s[2]));
+  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
+}
+
+// theta test of src/tree.f90:354-365,394 on a non-leaf node; true = open.
+__device__ __forceinline__ bool exact_open(double dist, const WNode64 &h, double theta_tree,
+                                           int extra) {
+  double th;
+  if (extra) {
+    double r = __dsub_rn(dist, h.geo);
+    th = r > 0. ? __ddiv_rn(h.width, r) : __ddiv_rn(h.width, dist);
+  } else {
+    th = __ddiv_rn(h.width, dist);
+  }
+  return !(th < theta_tree);
+}
+
+__device__ __forceinline__ void cross3(const double *a, const double *b, double *c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+struct Kahan3w {
+  float s[3], c[3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 3; k++) s[k] = c[k] = 0.f;
+  }
+  __device__ __forceinline__ void add(float a0, float a1, float a2) {
+    float a[3] = {a0, a1, a2};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float y = __fsub_rn(a[k], c[k]);
+      float t = __fadd_rn(s[k], y);
+      c[k] = __fsub_rn(__fsub_rn(t, s[k]), y);
+      s[k] = t;
+    }
+  }
+  __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
+};
+
+// ---------------------------------------------------------------- FP64 walk
+template <int BC>
+__global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
+  constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
+  __shared__ int2 stk[WW][STK];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int2 *st = stk[wid];
+  const int nwarps = (a.n_act + 31) / 32;
+  for (int w = blockIdx.x * WW + wid; w < nwarps; w += gridDim.x * WW) {
+    int q = w * 32 + lane;
+    bool live = q < a.n_act;
+    int i = live ? a.perm[q] : 0;
+    double xi[3] = {0., 0., 0.};
+    int bi = -1, fi = -1, ii = -1;
+    if (live) {
+      xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
+      bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
+    }
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    double acc0[3] = {0., 0., 0.}, acc1[3] = {0., 0., 0.};
+    unsigned long long ev = 0, evf = 0;
+    bool bad = false;
+#pragma unroll 1
+    for (int im = -1; im < NIMG; im++) {
+      int ma = 0, mb = 0, mc = 0;
+      if (im >= 0) qv_img_shift(BC, im, &ma, &mb, &mc);
+      const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
+      int top = 0;
+      if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+      top = 1;
+      __syncwarp();
+      while (top > 0) {
+        top--;
+        int2 e = st[top];
+        __syncwarp();
+        const int node = e.x;
+        const bool in = (((unsigned)e.y) >> lane) & 1u;
+        const WNode64 h = a.w64[node];
+        if (h.count == 1) {
+          if (in) {
+            int j = h.jb;
+            if (j != ii && j != bi && j != fi) {
+              double dist = exact_dist(xi, h, s);
+              if (dist < QV_DEPS) {
+                bad = true;
+              } else {
+                const WPay64 &P = a.p64[node];
+                double R1[3], R2[3], cr[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                  R1[c] = P.a[c] + s[c] - xi[c];
+                  R2[c] = P.b[c] + s[c] - xi[c];
+                }
+                double ra = sqrt(R1[0] * R1[0] + R1[1] * R1[1] + R1[2] * R1[2]);
+                double rb = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
+                double cc = ra * rb * (ra * rb + (R1[0] * R2[0] + R1[1] * R2[1] + R1[2] * R2[2]));
+                cross3(R1, R2, cr);
+                double f = (ra + rb) / cc;
+                if (im < 0) {
+#pragma unroll
+                  for (int c = 0; c < 3; c++) acc0[c] += f * cr[c];
+                } else {
+#pragma unroll
+                  for (int c = 0; c < 3; c++) acc1[c] += f * cr[c];
+                }
+                ev++;
+              }
+            }
+          }
+        } else {
+          bool open = false;
+          if (in) {
+            double dist = exact_dist(xi, h, s);
+            if (exact_open(dist, h, a.theta, a.extra)) {
+              open = true;
+            } else {
+              ev++;
+              evf++;
+              if (node != 0) {
+                const WPay64 &P = a.p64[node];
+                double v[3] = {__dsub_rn(xi[0], __dadd_rn(h.cx, s[0])),
+                               __dsub_rn(xi[1], __dadd_rn(h.cy, s[1])),
+                               __dsub_rn(xi[2], __dadd_rn(h.cz, s[2]))};
+                double d2 = dist * dist, d3 = d2 * dist, d5 = d2 * d2 * dist;
+                double cv[3], z[3], vz[3];
+                cross3(P.a, v, cv);
+#pragma unroll
+                for (int l = 0; l < 3; l++) z[l] = v[0] * P.C[l] + v[1] * P.C[3 + l] + v[2] * P.C[6 + l];
+                cross3(v, z, vz);
+                double o[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) o[c] = (cv[c] - P.b[c]) / d3 + 3. * vz[c] / d5;
+                if (im < 0) {
+#pragma unroll
+                  for (int c = 0; c < 3; c++) acc0[c] += o[c];
+                } else {
+#pragma unroll
+                  for (int c = 0; c < 3; c++) acc1[c] += o[c];
+                }
+              }
+            }
+          }
+          unsigned om = __ballot_sync(0xffffffffu, open);
+          if (om) {
+            int nc = h.nchild;
+            if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+              bad = true;
+              nc = 0;
+            }
+            if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+            top += nc;
+          }
+          __syncwarp();
+        }
+      }
+    }
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double b0 = acc0[c] * a.gfac, b1 = acc1[c] * a.gfac;
+        a.u_bs[3 * i + c] = b0 + b1;
+        a.u[3 * i + c] = (a.u_li[3 * i + c] + b0) + b1;
+      }
+    }
+      for (int o = 16; o > 0; o >>= 1) {
+      ev += __shfl_down_sync(0xffffffffu, ev, o);
+      evf += __shfl_down_sync(0xffffffffu, evf, o);
+    }
+    if (lane == 0 && ev) atomicAdd(a.evals, ev);
+    if (lane == 0 && evf) atomicAdd(a.evals_far, evf);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, 1);
+  }
+}
+
+// ---------------------------------------------------------------- mixed walk
+template <int BC>
+__global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
+  constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
+  __shared__ int2 stk[WW][STK];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int2 *st = stk[wid];
+  const int nwarps = (a.n_act + 31) / 32;
+  const float th32 = (float)a.theta;
+  for (int w = blockIdx.x * WW + wid; w < nwarps; w += gridDim.x * WW) {
+    int q = w * 32 + lane;
+    bool live = q < a.n_act;
+    int i = live ? a.perm[q] : 0;
+    double xi[3] = {0., 0., 0.};
+    int bi = -1, fi = -1, ii = -1;
+    if (live) {
+      xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
+      bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
+    }
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    Kahan3w k0, k1;
+    k0.zero();
+    k1.zero();
+    unsigned long long ev = 0, evf = 0;
+    bool bad = false;
+#pragma unroll 1
+    for (int im = -1; im < NIMG; im++) {
+      int ma = 0, mb = 0, mc = 0;
+      if (im >= 0) qv_img_shift(BC, im, &ma, &mb, &mc);
+      const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
+      // target recentred for this image, t = x_i - shift as (hi, lo) floats
+      float th[3], tl[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double t = xi[c] - s[c];
+        th[c] = __double2float_rn(t);
+        tl[c] = __double2float_rn(t - (double)th[c]);
+      }
+      int top = 0;
+      if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+      top = 1;
+      __syncwarp();
+      while (top > 0) {
+        top--;
+        int2 e = st[top];
+        __syncwarp();
+        const int node = e.x;
+        const bool in = (((unsigned)e.y) >> lane) & 1u;
+        const WNode32 h = a.w32[node];
+        // v = t - cent  (= x_i - (cent + shift))
+        float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
+        float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
+        float v2 = (th[2] - h.ch[2]) + (tl[2] - h.cl[2]);
+        float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+        if (h.count == 1) {
+          if (in) {
+            int j = h.jb;
+            if (j != ii && j != bi && j != fi) {
+              bool sing = false;
+              if (d2 < 1e-20f) {
+                double dist = exact_dist(xi, a.w64[node], s);
+                sing = dist < QV_DEPS;
+              }
+              if (sing) {
+                bad = true;
+              } else {
+                const WPay32 &P = a.p32[node];
+                float r2x = (P.a[0] - th[0]) + (P.b[0] - tl[0]);
+                float r2y = (P.a[1] - th[1]) + (P.b[1] - tl[1]);
+                float r2z = (P.a[2] - th[2]) + (P.b[2] - tl[2]);
+                float ox, oy, oz;
+                qv_seg32(-v0, -v1, -v2, r2x, r2y, r2z, d2, ox, oy, oz);
+                if (im < 0) k0.add(ox, oy, oz); else k1.add(ox, oy, oz);
+                ev++;
+              }
+            }
+          }
+        } else {
+          bool open = false;
+          if (in) {
+            float dist = sqrtf(d2);
+            float dg = dist - h.geo;
+            float eps = 4e-6f * (dist + h.geo);
+            bool amb = false;
+            float r = dist;
+            if (a.extra) {
+              if (dg > eps) r = dg;
+              else if (dg < -eps) r = dist;
+              else amb = true;
+            }
+            if (!amb) {
+              float diff = h.width - th32 * r;
+              float tol = 4e-6f * (h.width + th32 * (dist + h.geo));
+              if (fabsf(diff) > tol) open = diff >= 0.f;
+              else amb = true;
+            }
+            if (amb) {
+              const WNode64 h64 = a.w64[node];
+              open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+            }
+            if (!open) {
+              ev++;
+              evf++;
+              if (node != 0) {
+                const WPay32 &P = a.p32[node];
+                float rd = rsqrtf(d2);
+                float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
+                float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
+                float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
+                float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
+                float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
+                float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
+                float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
+                float wx = fmaf(v1, z2, -v2 * z1);
+                float wy = fmaf(v2, z0, -v0 * z2);
+                float wz = fmaf(v0, z1, -v1 * z0);
+                float t5 = 3.f * rd5;
+                float ox = fmaf(cx, rd3, wx * t5);
+                float oy = fmaf(cy, rd3, wy * t5);
+                float oz = fmaf(cz, rd3, wz * t5);
+                if (im < 0) k0.add(ox, oy, oz); else k1.add(ox, oy, oz);
+              }
+            }
+          }
+          unsigned om = __ballot_sync(0xffffffffu, open);
+          if (om) {
+            int nc = h.nchild;
+            if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+              bad = true;
+              nc = 0;
+            }
+            if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+            top += nc;
+          }
+          __syncwarp();
+        }
+      }
+    }
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        double b0 = k0.get(c) * a.gfac, b1 = k1.get(c) * a.gfac;
+        a.u_bs[3 * i + c] = b0 + b1;
+        a.u[3 * i + c] = (a.u_li[3 * i + c] + b0) + b1;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      ev += __shfl_down_sync(0xffffffffu, ev, o);
+      evf += __shfl_down_sync(0xffffffffu, evf, o);
+    }
+    if (lane == 0 && ev) atomicAdd(a.evals, ev);
+    if (lane == 0 && evf) atomicAdd(a.evals_far, evf);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, 1);
+  }
+}
+
+int qv_launch_walk(qv_ctx *c) {
+  TreeBuf &t = c->tree;
+  if (!t.valid) return qv_fail(c, QV_ERR_STATE, "tree walk without a built tree");
+  if (t.n_act == 0) return QV_OK;
+  WalkArgs a;
+  a.n_act = t.n_act; a.perm = t.perm; a.x = c->x; a.inf = c->infront; a.beh = c->behind;
+  a.w64 = t.w64; a.p64 = t.p64; a.w32 = t.w32; a.p32 = t.p32;
+  a.u_li = c->u_li; a.u = c->u; a.u_bs = c->u_bs;
+  a.L = c->p.box_size; a.theta = c->p.tree_theta; a.gfac = c->p.quant_circ / 4. / QV_PI;
+  a.extra = c->p.tree_extra_correction; a.evals = c->evals; a.evals_far = c->evals_far;
+  a.status = c->dstatus;
+  int nwarps = (t.n_act + 31) / 32;
+  int nb = (nwarps + WW - 1) / WW;
+  bool mixed = c->p.precision == QV_PREC_MIXED;
+  switch (c->p.boundary) {
+#define QV_WALK_CASE(BCV)                                                        \
+  case BCV:                                                                      \
+    if (mixed) k_walk32<BCV><<<nb, WW * 32, 0, c->stream>>>(a);                  \
+    else k_walk64<BCV><<<nb, WW * 32, 0, c->stream>>>(a);                        \
+    break;
+    QV_WALK_CASE(QV_BC_OPEN)
+    QV_WALK_CASE(QV_BC_PERIODIC)
+    QV_WALK_CASE(QV_BC_OPENX)
+    QV_WALK_CASE(QV_BC_OPENXY)
+#undef QV_WALK_CASE
+    default:
+      return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
+  }
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}

@@ -1,0 +1,319 @@
+"""ctypes binding of the C ABI declared in include/qv.h (libqvort_b200.so).
+
+This is the Python face of the same entry points the Fortran driver binds
+through ISO_C_BINDING.  Arrays cross as numpy buffers: positions and
+velocities (n, 3) float64 C-contiguous (= Fortran x(3,n)), links (n,) int32
+with 1-based indices and 0 for an empty slot.  A failing call raises
+QvError carrying the status code and qv_last_error()'s message.
+
+There is no fallback: importing this module loads the CUDA library, and a
+missing or unloadable library raises at import time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libqvort_b200.so"
+
+QV_OK = 0
+QV_ERR_ARG = -1
+QV_ERR_CUDA = -2
+QV_ERR_SINGULAR = -3
+QV_ERR_TREE_DEPTH = -4
+QV_ERR_STATE = -5
+QV_ERR_NOMEM = -6
+QV_ERR_UNSUPPORTED = -7
+QV_ERR_NAN = -8
+QV_MAX_DEPTH = 64
+
+BC = {"open": 0, "periodic": 1, "openx": 2, "openxy": 3}
+VELOCITY = {"Off": 0, "LIA": 1, "BS": 2, "Tree": 3}
+PREC = {"fp64": 0, "mixed": 1}
+
+
+class QvParams(C.Structure):
+    _fields_ = [
+        ("quant_circ", C.c_double),
+        ("corea", C.c_double),
+        ("box_size", C.c_double),
+        ("delta", C.c_double),
+        ("dt", C.c_double),
+        ("tree_theta", C.c_double),
+        ("boundary", C.c_int),
+        ("velocity", C.c_int),
+        ("deriv_order", C.c_int),
+        ("tree_extra_correction", C.c_int),
+        ("fixed_lia_beta", C.c_int),
+        ("precision", C.c_int),
+        ("runge_kutta", C.c_int),
+        ("recon_shots", C.c_int),
+    ]
+
+
+class QvError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"qv error {code}: {msg}")
+        self.code = code
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `python -m qvort_b200.build` (nvcc, sm_100a)")
+    return C.CDLL(str(LIB_PATH))
+
+
+_lib = _load()
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+_SIGS = {
+    "qv_default_params": [C.POINTER(QvParams)],
+    "qv_create": [C.POINTER(QvParams), _P, C.POINTER(_P)],
+    "qv_destroy": [_P],
+    "qv_set_params": [_P, C.POINTER(QvParams)],
+    "qv_set_points": [_P, C.c_int, _P, _P, _P],
+    "qv_set_points_device": [_P, C.c_int, _P, _P, _P],
+    "qv_set_history": [_P, _P, _P, _P],
+    "qv_get_history": [_P, _P, _P, _P],
+    "qv_set_closest": [_P, _P],
+    "qv_get_points": [_P, _P, _P],
+    "qv_device_arrays": [_P, _P, _P, _P, _P],
+    "qv_ghosts": [_P],
+    "qv_get_ghosts": [_P, _P, _P, _P, _P],
+    "qv_build_tree": [_P],
+    "qv_tree_info": [_P, _I, _I],
+    "qv_tree_export": [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "qv_velocity": [_P, _P, _P, _P, C.POINTER(C.c_longlong)],
+    "qv_step_ab": [_P],
+    "qv_step_rk3": [_P],
+    "qv_enforce_periodic": [_P],
+    "qv_closest": [_P, _P, _P],
+    "qv_energy": [_P, _D],
+    "qv_step": [_P, C.c_int],
+    "qv_sync": [_P],
+    "qv_profile": [_P, C.c_int],
+    "qv_phase_times": [_P, _P, C.c_int],
+    "qv_counters": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                    C.POINTER(C.c_longlong)],
+    "qv_probe_fp32": [_P, _D],
+}
+for _name, _args in _SIGS.items():
+    _f = getattr(_lib, _name)
+    _f.argtypes = _args
+    _f.restype = C.c_int
+_lib.qv_last_error.argtypes = [_P]
+_lib.qv_last_error.restype = C.c_char_p
+
+EXPORTED = tuple(_SIGS) + ("qv_last_error",)
+
+
+def lib() -> C.CDLL:
+    return _lib
+
+
+def default_params(**kw) -> QvParams:
+    p = QvParams()
+    _lib.qv_default_params(C.byref(p))
+    for k, v in kw.items():
+        if k == "boundary" and isinstance(v, str):
+            v = BC[v]
+        elif k == "velocity" and isinstance(v, str):
+            v = VELOCITY[v]
+        elif k == "precision" and isinstance(v, str):
+            v = PREC[v]
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f64(a, n=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None:
+        a = a.reshape(n, 3)
+    return a
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Context:
+    """One filament system on the device (a qv_ctx)."""
+
+    def __init__(self, params: QvParams | None = None, stream: int | None = None, **kw):
+        self.params = params if params is not None else default_params(**kw)
+        h = C.c_void_p()
+        self._check(_lib.qv_create(C.byref(self.params), stream, C.byref(h)), None)
+        self._h = h
+        self.n = 0
+
+    def _check(self, rc: int, h=-1):
+        if rc < 0:
+            hh = self._h if h == -1 else h
+            msg = _lib.qv_last_error(hh).decode() if hh else "qv_create failed"
+            raise QvError(rc, msg)
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.qv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- state
+    def set_params(self, params: QvParams):
+        self._check(_lib.qv_set_params(self._h, C.byref(params)))
+        self.params = params
+
+    def set_points(self, x, infront, behind):
+        x = _f64(x)
+        n = x.shape[0]
+        inf, beh = _i32(infront), _i32(behind)
+        assert inf.shape == (n,) and beh.shape == (n,)
+        self._check(_lib.qv_set_points(self._h, n, _ptr(x), _ptr(inf), _ptr(beh)))
+        self.n = n
+
+    def set_points_device(self, n: int, x_ptr: int, inf_ptr: int, beh_ptr: int):
+        self._check(_lib.qv_set_points_device(self._h, n, x_ptr, inf_ptr, beh_ptr))
+        self.n = n
+
+    def set_history(self, u1=None, u2=None, u3=None):
+        arrs = [None if u is None else _f64(u, self.n) for u in (u1, u2, u3)]
+        self._check(_lib.qv_set_history(self._h, *[_ptr(a) for a in arrs]))
+
+    def get_history(self):
+        out = [np.empty((self.n, 3)) for _ in range(3)]
+        self._check(_lib.qv_get_history(self._h, *[_ptr(a) for a in out]))
+        return out
+
+    def set_closest(self, closest):
+        c = _i32(closest)
+        self._check(_lib.qv_set_closest(self._h, _ptr(c)))
+
+    def get_points(self):
+        x = np.empty((self.n, 3))
+        u = np.empty((self.n, 3))
+        self._check(_lib.qv_get_points(self._h, _ptr(x), _ptr(u)))
+        return x, u
+
+    def device_arrays(self):
+        px, pu, pi, pb = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+        self._check(_lib.qv_device_arrays(self._h, C.byref(px), C.byref(pu), C.byref(pi),
+                                          C.byref(pb)))
+        return px.value, pu.value, pi.value, pb.value
+
+    # ---- path entry points
+    def ghosts(self):
+        self._check(_lib.qv_ghosts(self._h))
+
+    def get_ghosts(self):
+        out = [np.empty((self.n, 3)) for _ in range(4)]
+        self._check(_lib.qv_get_ghosts(self._h, *[_ptr(a) for a in out]))
+        return out
+
+    def build_tree(self):
+        self._check(_lib.qv_build_tree(self._h))
+
+    def tree_info(self):
+        a, b = C.c_int(), C.c_int()
+        self._check(_lib.qv_tree_info(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def tree_export(self):
+        m, _ = self.tree_info()
+        parent = np.empty(m, np.int32)
+        digit = np.empty(m, np.int32)
+        depth = np.empty(m, np.int32)
+        pos = np.empty((m, 3))
+        width = np.empty(m)
+        pcount = np.empty(m, np.int32)
+        cent = np.empty((m, 3))
+        circ = np.empty((m, 3))
+        cij = np.empty((m, 9))
+        first = np.empty(m, np.int32)
+        arrs = [parent, digit, depth, pos, width, pcount, cent, circ, cij, first]
+        self._check(_lib.qv_tree_export(self._h, m, *[_ptr(a) for a in arrs]))
+        return dict(parent=parent, digit=digit, depth=depth, pos=pos, width=width,
+                    pcount=pcount, cent=cent, circ=circ, Cij=cij, first=first)
+
+    def velocity(self, want_parts: bool = True):
+        u = np.empty((self.n, 3))
+        uli = np.empty((self.n, 3)) if want_parts else None
+        ubs = np.empty((self.n, 3)) if want_parts else None
+        ev = C.c_longlong()
+        self._check(_lib.qv_velocity(self._h, _ptr(u), _ptr(uli), _ptr(ubs), C.byref(ev)))
+        return u, uli, ubs, ev.value
+
+    def step_ab(self):
+        self._check(_lib.qv_step_ab(self._h))
+
+    def step_rk3(self):
+        self._check(_lib.qv_step_rk3(self._h))
+
+    def enforce_periodic(self):
+        self._check(_lib.qv_enforce_periodic(self._h))
+
+    def closest(self):
+        cl = np.empty(self.n, np.int32)
+        cd = np.empty(self.n)
+        self._check(_lib.qv_closest(self._h, _ptr(cl), _ptr(cd)))
+        return cl, cd
+
+    def energy(self) -> float:
+        e = C.c_double()
+        self._check(_lib.qv_energy(self._h, C.byref(e)))
+        return e.value
+
+    def step(self, itime: int = 1):
+        self._check(_lib.qv_step(self._h, itime))
+
+    def sync(self):
+        self._check(_lib.qv_sync(self._h))
+
+    # ---- instrumentation
+    PHASES = ("ghosts", "build", "local", "nonlocal", "update", "search", "wrap")
+
+    def profile(self, enable: bool = True):
+        self._check(_lib.qv_profile(self._h, int(enable)))
+
+    def phase_times(self, reset: bool = True) -> dict:
+        ms = np.zeros(len(self.PHASES))
+        self._check(_lib.qv_phase_times(self._h, _ptr(ms), int(reset)))
+        return dict(zip(self.PHASES, ms.tolist()))
+
+    def counters(self):
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._check(_lib.qv_counters(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return dict(launches=a.value, leaf_evals=b.value, far_evals=c.value)
+
+
+def probe_fp32(stream: int | None = None) -> float:
+    """Measured FP32 FMA throughput of the current device, TFLOP/s."""
+    t = C.c_double()
+    rc = _lib.qv_probe_fp32(stream, C.byref(t))
+    if rc < 0:
+        raise QvError(rc, "qv_probe_fp32 failed")
+    return t.value

@@ -1,0 +1,359 @@
+"""GPU parity of the CUDA path against the oracle, through the C ABI.
+
+Bars (written per test): integer/index results and the tree are bit-exact;
+FP64 velocities agree with the oracle to 1e-10 relative (different but
+equivalent FP64 evaluation orders); the mixed-precision path agrees with the
+FP64 path to 1e-6 RMS relative velocity error.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qvort_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def L():
+    from qvort_b200 import lib
+
+    return lib
+
+
+def ctx_for(L, w, **over):
+    prm = dict(w.params)
+    prm.update(over)
+    c = L.Context(L.default_params(**prm))
+    c.set_points(w.x, w.infront, w.behind)
+    return c
+
+
+def opar(w, **over):
+    prm = dict(w.params)
+    prm.update(over)
+    prm.pop("precision", None)
+    return O.params(**prm)
+
+
+def rel_rms(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+def rel_max(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def small_tangle(seed=1, n_rings=20):
+    return W.random_rings(n_rings, 0.006, 0.012, 5e-4, 0.1, seed=seed, theta=0.4)
+
+
+# ------------------------------------------------------------------ ghosts
+@pytest.mark.parametrize("bc", ["open", "periodic", "openx", "openxy"])
+def test_ghosts_bit_exact(L, bc):
+    w = small_tangle()
+    c = ctx_for(L, w, boundary=bc)
+    c.ghosts()
+    g = c.get_ghosts()
+    og = O.ghosts(opar(w, boundary=bc), w.x, w.infront, w.behind)
+    for a, b in zip(g, og):
+        np.testing.assert_array_equal(a, b)
+
+
+# ------------------------------------------------------------------ direct
+def test_direct_fp64_ring_matches_oracle(L):
+    w = W.ring()
+    c = ctx_for(L, w, precision="fp64")
+    u, uli, ubs, ev = c.velocity()
+    p = opar(w)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    ou, ouli, oubs, *_ = O.velocity(p, w.x, w.infront, w.behind, og)
+    assert rel_max(uli, ouli) < 1e-12
+    assert rel_max(u, ou) < 1e-10
+    assert ev == w.n * w.n
+
+
+@pytest.mark.parametrize("bc", ["periodic", "openx", "openxy", "open"])
+def test_direct_fp64_images_match_oracle(L, bc, nthreads):
+    w = small_tangle(2, 8)
+    c = ctx_for(L, w, velocity="BS", tree_theta=0.0, boundary=bc, precision="fp64")
+    u, uli, ubs, ev = c.velocity()
+    p = opar(w, velocity="BS", tree_theta=0.0, boundary=bc)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    ou, ouli, oubs, *_ = O.velocity(p, w.x, w.infront, w.behind, og, nthreads=nthreads)
+    assert rel_max(u, ou) < 1e-10
+    assert rel_max(ubs, oubs) < 1e-10
+
+
+def _seg_terms(P, pts):
+    """|field| of each straight segment of the loop pts at P (numpy FP64)."""
+    out = []
+    for a, b in zip(pts, pts[1:] + pts[:1]):
+        R1, R2 = a - P, b - P
+        r1, r2 = np.linalg.norm(R1), np.linalg.norm(R2)
+        f = (r1 + r2) / (r1 * r2 * (r1 * r2 + R1 @ R2))
+        out.append(np.linalg.norm(9.97e-4 / (4 * np.pi) * f * np.cross(R1, R2)))
+    return out
+
+
+def test_direct_segment_known_answers(L):
+    """The 50-digit triangle-loop fixtures.  FP64: 1e-9 of the net field.  Mixed:
+    1e-6 of the summed segment magnitudes (far loops are dipoles whose net field
+    is ~d/size times smaller than each segment's, a cancellation no FP32 term
+    survives; the bar is on the per-term accuracy)."""
+    from pathlib import Path
+
+    g = np.load(Path(__file__).resolve().parent / "golden" / "segment_kat.npz")
+    worst = {"fp64": 0.0, "mixed": 0.0}
+    for prec in worst:
+        for k in range(g["P"].shape[0]):
+            x = np.array([g["P"][k], g["P2"][k], g["A"][k], g["B"][k], g["C"][k]])
+            inf = np.array([2, 1, 4, 5, 3], np.int32)
+            beh = np.array([2, 1, 5, 3, 4], np.int32)
+            c = L.Context(L.default_params(velocity="BS", boundary="open", box_size=0.2,
+                                           quant_circ=float(g["gamma"]), precision=prec))
+            c.set_points(x, inf, beh)
+            u, uli, *_ = c.velocity()
+            np.testing.assert_array_equal(uli[0], 0.0)
+            if prec == "fp64":
+                scale = np.abs(g["U"][k]).max()
+            else:
+                scale = sum(_seg_terms(g["P"][k], [g["A"][k], g["B"][k], g["C"][k]]))
+            worst[prec] = max(worst[prec], np.abs(u[0] - g["U"][k]).max() / scale)
+            c.close()
+    assert worst["fp64"] < 1e-9, worst
+    assert worst["mixed"] < 1e-6, worst
+
+
+def test_direct_mixed_vs_fp64(L):
+    w = small_tangle(3, 12)
+    c64 = ctx_for(L, w, velocity="BS", tree_theta=0.0, precision="fp64")
+    c32 = ctx_for(L, w, velocity="BS", tree_theta=0.0, precision="mixed")
+    u64 = c64.velocity()[0]
+    u32 = c32.velocity()[0]
+    assert rel_rms(u32, u64) < 1e-6
+
+
+# ------------------------------------------------------------------ tree
+def _compare_trees(g, o):
+    assert len(g["parent"]) == len(o["parent"])
+    for k in ("parent", "digit", "depth", "pcount", "first"):
+        np.testing.assert_array_equal(g[k], o[k], err_msg=k)
+    for k in ("pos", "width", "cent", "circ", "Cij"):
+        np.testing.assert_array_equal(g[k], o[k], err_msg=k)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_tree_bit_exact_tangle(L, seed):
+    w = W.tangle(seed)
+    c = ctx_for(L, w)
+    c.ghosts()
+    c.build_tree()
+    gt = c.tree_export()
+    p = opar(w)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    ot = O.Tree(p, w.x, og[0], w.infront).export()
+    _compare_trees(gt, ot)
+
+
+def test_tree_bit_exact_edge_cases(L):
+    rng = np.random.default_rng(7)
+    n = 3000
+    x = rng.uniform(-0.055, 0.055, (n, 3))        # some outside the box
+    x[:50] = np.round(x[:50] * 40) / 40            # points on cell boundaries
+    x[50:60] = x[60:70] + 1e-13                    # near-coincident pairs
+    inf = np.roll(np.arange(1, n + 1), -1).astype(np.int32)
+    beh = np.roll(np.arange(1, n + 1), 1).astype(np.int32)
+    inf[::11] = 0                                   # empty slots
+    prm = dict(velocity="Tree", tree_theta=0.5, boundary="open", box_size=0.1)
+    c = L.Context(L.default_params(**prm))
+    c.set_points(x, inf, beh)
+    c.ghosts()
+    c.build_tree()
+    gt = c.tree_export()
+    p = O.params(**prm)
+    og = O.ghosts(p, x, np.where(inf == 0, 1, inf), beh)
+    gg = c.get_ghosts()
+    act = inf != 0
+    np.testing.assert_array_equal(gg[0][act], og[0][act])
+    ot = O.Tree(p, x, gg[0], inf).export()
+    _compare_trees(gt, ot)
+
+
+def test_tree_depth_error_not_hang(L):
+    """Coincident points exactly at the origin never separate: the corner
+    stays 0 and every cell [0, w) keeps them down to widths that underflow
+    (~1075 levels in the reference).  The build stops at QV_MAX_DEPTH with an
+    error instead.  Coincident points elsewhere terminate (the corner sums stop
+    changing and the points fall out), as in the reference."""
+    n = 8
+    x = np.zeros((n, 3))
+    inf = np.roll(np.arange(1, n + 1), -1).astype(np.int32)
+    beh = np.roll(np.arange(1, n + 1), 1).astype(np.int32)
+    c = L.Context(L.default_params(velocity="Tree", tree_theta=0.5, box_size=0.1))
+    c.set_points(x, inf, beh)
+    with pytest.raises(L.QvError) as e:
+        c.build_tree()
+    assert e.value.code == L.QV_ERR_TREE_DEPTH
+
+
+# ------------------------------------------------------------------ walk
+@pytest.mark.parametrize("bc", ["periodic", "open"])
+def test_walk_fp64_matches_oracle(L, bc, nthreads):
+    w = W.tangle(0)
+    c = ctx_for(L, w, boundary=bc, precision="fp64")
+    c.ghosts()
+    c.build_tree()
+    u, uli, ubs, ev = c.velocity()
+    p = opar(w, boundary=bc)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    tr = O.Tree(p, w.x, og[0], w.infront)
+    ou, ouli, oubs, oev, st = O.velocity(p, w.x, w.infront, w.behind, og, tr, nthreads=nthreads)
+    assert st == 0
+    assert ev == oev           # identical traversals: identical evaluation counts
+    assert rel_max(u, ou) < 1e-10
+    assert rel_max(ubs, oubs) < 1e-9
+
+
+def test_walk_mixed_vs_fp64(L):
+    w = W.tangle(0)
+    c64 = ctx_for(L, w, precision="fp64")
+    c32 = ctx_for(L, w, precision="mixed")
+    r = []
+    for c in (c64, c32):
+        c.ghosts()
+        c.build_tree()
+        r.append(c.velocity())
+    assert r[0][3] == r[1][3]  # same nodes visited
+    assert rel_rms(r[1][0], r[0][0]) < 1e-6
+    assert rel_rms(r[1][2], r[0][2]) < 1e-5
+
+
+# ------------------------------------------------------------------ steps
+def test_ab_step_bit_exact_given_velocity(L):
+    w = small_tangle(4, 10)
+    c = ctx_for(L, w, precision="fp64")
+    rng = np.random.default_rng(0)
+    h = [rng.normal(size=(w.n, 3)) * 0.1 for _ in range(3)]
+    h[2][::3] = 0.0
+    h[1][::5] = 0.0
+    h[0][::7] = 0.0
+    c.set_history(*h)
+    c.ghosts()
+    c.build_tree()
+    u, *_ = c.velocity()
+    c.step_ab()
+    x, _ = c.get_points()
+    hist = c.get_history()
+    ox, ou1, ou2, ou3 = O.pmotion_ab(w.params["dt"], w.x, u, *h, w.infront)
+    np.testing.assert_array_equal(x, ox)
+    np.testing.assert_array_equal(hist[0], ou1)
+    np.testing.assert_array_equal(hist[1], ou2)
+    np.testing.assert_array_equal(hist[2], ou3)
+
+
+def test_closest_tree_bit_exact(L, nthreads):
+    w = W.tangle(1)
+    c = ctx_for(L, w, precision="fp64")
+    c.ghosts()
+    c.build_tree()
+    c.velocity()
+    c.step_ab()                     # move; the tree is now stale
+    rng = np.random.default_rng(5)
+    seedcl = rng.integers(0, w.n, w.n).astype(np.int32)
+    c.set_closest(seedcl)
+    cl, cd = c.closest()
+    xn, _ = c.get_points()
+    p = opar(w)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    tr = O.Tree(p, w.x, og[0], w.infront)
+    ocl, ocd = O.pclose_tree(tr, xn, w.infront, w.behind, seedcl, nthreads)
+    np.testing.assert_array_equal(cl, ocl)
+    np.testing.assert_array_equal(cd, ocd)
+
+
+def test_pclose_bit_exact(L):
+    w = small_tangle(6, 10)
+    c = ctx_for(L, w, velocity="BS", tree_theta=0.0)
+    cl, cd = c.closest()
+    ocl, ocd = O.pclose(w.x, w.infront, w.behind, np.zeros(w.n, np.int32))
+    np.testing.assert_array_equal(cl, ocl)
+    np.testing.assert_array_equal(cd, ocd)
+
+
+def test_energy_matches_oracle(L):
+    w = W.ring()
+    c = ctx_for(L, w)
+    u, *_ = c.velocity()
+    e = c.energy()
+    p = opar(w)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    assert e == pytest.approx(O.energy(p, w.x, u, w.infront, og), rel=1e-12)
+
+
+def test_ring_trajectory_1000_steps(L):
+    """Configuration 1: ring, FP64 direct BS + LIA, AB ladder, 1000 steps,
+    against the oracle's own 1000 steps and the analytic speed."""
+    w = W.ring()
+    c = ctx_for(L, w, precision="fp64")
+    st = O.State(opar(w), w.x, w.infront, w.behind)
+    nsteps = 1000
+    for it in range(1, nsteps + 1):
+        c.step(it)
+        st.step()
+    x, _ = c.get_points()
+    assert rel_max(x - w.x, st.x - w.x) < 1e-8
+    dz = (x[:, 2] - w.x[:, 2]).mean()
+    speed = abs(dz) / (nsteps * w.params["dt"])
+    ana = 9.97e-4 / (4 * np.pi * 0.01) * (np.log(8 * 0.01 / 1.3e-8) - 0.5)
+    assert abs(speed / ana - 1) < 0.01
+
+
+def test_rk3_step_matches_oracle(L):
+    w = small_tangle(8, 6)
+    prm = dict(runge_kutta=1, precision="fp64")
+    c = ctx_for(L, w, **prm)
+    st = O.State(opar(w), w.x, w.infront, w.behind)
+    for it in range(1, 4):
+        c.step(it)
+        st.step(runge_kutta=True)
+    x, _ = c.get_points()
+    assert rel_max(x - w.x, st.x - w.x) < 1e-8
+
+
+def test_tangle_steps_match_oracle(L, nthreads):
+    w = small_tangle(9, 30)
+    c = ctx_for(L, w, precision="fp64")
+    st = O.State(opar(w), w.x, w.infront, w.behind)
+    for it in range(1, 6):
+        c.step(it)
+        st.step(nthreads=nthreads)
+    x, _ = c.get_points()
+    d = x - st.x
+    d -= np.round(d / 0.1) * 0.1   # a wrap decision may differ at the box face
+    assert np.abs(d).max() / np.abs(st.x - w.x).max() < 1e-6
+
+
+def test_unsupported_boundary_is_an_error(L):
+    with pytest.raises(L.QvError) as e:
+        L.Context(L.default_params(boundary=5))
+    assert e.value.code == L.QV_ERR_UNSUPPORTED
+
+
+def test_coincident_points_off_origin_match_oracle(L):
+    n = 8
+    x = np.zeros((n, 3)) + 0.0123
+    x[4:] += np.array([1e-3, -2e-3, 5e-4])
+    inf = np.roll(np.arange(1, n + 1), -1).astype(np.int32)
+    beh = np.roll(np.arange(1, n + 1), 1).astype(np.int32)
+    prm = dict(velocity="Tree", tree_theta=0.5, box_size=0.1)
+    c = L.Context(L.default_params(**prm))
+    c.set_points(x, inf, beh)
+    c.ghosts()
+    c.build_tree()
+    gt = c.tree_export()
+    p = O.params(**prm)
+    og = O.ghosts(p, x, inf, beh)
+    t = O.Tree(p, x, og[0], inf)
+    assert t.status == 0
+    _compare_trees(gt, t.export())

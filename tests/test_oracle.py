@@ -1,0 +1,193 @@
+"""CPU tests of the oracle (the C restatement in oracle/qv_oracle.c).
+
+The reference ships no tests or golden data for this path, and it cannot be run
+here (no Fortran compiler), so the oracle is pinned by known answers that do
+not depend on it: the 50-digit finite-segment field (tests/golden), the ring
+speed/energy the reference prints at set-up, the reference's own dt bound, and
+structural identities of the tree and the skip rules.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from qvort_b200 import workloads as W
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+def _kat_system(row):
+    P, P2, A, B, Cc = row
+    x = np.array([P, P2, A, B, Cc])
+    inf = np.array([2, 1, 4, 5, 3], np.int32)
+    beh = np.array([2, 1, 5, 3, 4], np.int32)
+    return x, inf, beh
+
+
+@pytest.mark.parametrize("velocity,theta", [("BS", 0.0), ("Tree", 1e-9)])
+def test_segment_known_answers(velocity, theta):
+    g = np.load(GOLD / "segment_kat.npz")
+    p = O.params(velocity=velocity, tree_theta=theta, boundary="open", box_size=0.2,
+                 quant_circ=float(g["gamma"]))
+    worst = 0.0
+    for k in range(g["P"].shape[0]):
+        x, inf, beh = _kat_system([g[n][k] for n in ("P", "P2", "A", "B", "C")])
+        gh = O.ghosts(p, x, inf, beh)
+        tree = O.Tree(p, x, gh[0], inf) if velocity == "Tree" else None
+        u, uli, ubs, ev, st = O.velocity(p, x, inf, beh, gh, tree)
+        assert st == 0
+        np.testing.assert_array_equal(uli[0], 0.0)
+        ref = g["U"][k]
+        worst = max(worst, np.abs(u[0] - ref).max() / np.abs(ref).max())
+    assert worst < 1e-9, worst
+
+
+def test_ring_speed_energy_known_answer():
+    kat = np.load(GOLD / "ring_kat.npz")
+    w = W.ring(200, float(kat["R"]), 0.0)
+    p = O.params(**w.params)
+    gh = O.ghosts(p, w.x, w.infront, w.behind)
+    u, *_ = O.velocity(p, w.x, w.infront, w.behind, gh)
+    speed = np.abs(u[:, 2].mean())
+    assert abs(speed / float(kat["speed"]) - 1) < 0.01
+    # all points translate together (axisymmetric ring)
+    assert np.std(u[:, 2]) / speed < 1e-6
+    assert np.abs(u[:, :2]).max() / speed < 1e-6
+    # energy_info's line integral G * sum u.(s x s') dl of a ring of radius R
+    # moving at speed v is 2 pi G R^2 v (the Kelvin impulse relation)
+    e = O.energy(p, w.x, u, w.infront, gh)
+    G, R = float(kat["gamma"]), float(kat["R"])
+    assert abs(abs(e) / (2 * np.pi * G * R ** 2 * speed) - 1) < 1e-3
+
+
+def test_dt_bound():
+    # timestep_check, src/initial.f90:606-622
+    p = O.params(delta=5e-4, corea=1.3e-8)
+    dm = 2.5e-4
+    expect = abs(dm ** 2 / (9.97e-4 * np.log(dm / (np.pi * 1.3e-8))))
+    assert O.dt_max(p) == pytest.approx(expect, rel=1e-15)
+    assert 1e-7 < O.dt_max(p)
+
+
+def _tree_invariants(ex, x, inf, L):
+    m = len(ex["parent"])
+    kids = {}
+    for k in range(1, m):
+        kids.setdefault(ex["parent"][k], []).append(k)
+    for k in range(m):
+        ch = kids.get(k, [])
+        dig = [ex["digit"][c] for c in ch]
+        assert dig == sorted(dig) and len(set(dig)) == len(dig)
+        if k > 0:
+            assert sum(ex["pcount"][c] for c in ch) <= ex["pcount"][k]
+            if ex["pcount"][k] == 1:
+                assert not ch
+        for c in ch:
+            assert ex["width"][c] == ex["width"][k] / 2
+            assert ex["depth"][c] == ex["depth"][k] + 1
+    assert ex["pcount"][0] == len(x)
+    leaves = np.where(ex["pcount"] == 1)[0]
+    firsts = ex["first"][leaves]
+    assert len(set(firsts)) == len(firsts)
+
+
+def test_tree_structure_tangle():
+    w = W.tangle()
+    p = O.params(**w.params)
+    gh = O.ghosts(p, w.x, w.infront, w.behind)
+    t = O.Tree(p, w.x, gh[0], w.infront)
+    assert t.status == 0
+    ex = t.export()
+    _tree_invariants(ex, w.x, w.infront, 0.1)
+    # every in-box active point ends in exactly one leaf
+    assert (ex["pcount"] == 1).sum() == w.n
+
+
+def test_tree_drops_out_of_box_and_empty():
+    rng = np.random.default_rng(3)
+    n = 400
+    x = rng.uniform(-0.06, 0.06, (n, 3))   # some points outside [-0.05, 0.05)
+    inf = np.roll(np.arange(1, n + 1), -1).astype(np.int32)
+    beh = np.roll(np.arange(1, n + 1), 1).astype(np.int32)
+    inf[::7] = 0                            # empty slots
+    p = O.params(velocity="Tree", tree_theta=0.5, boundary="open", box_size=0.1)
+    gh = O.ghosts(p, x, np.where(inf == 0, 1, inf), beh)
+    t = O.Tree(p, x, gh[0], inf)
+    ex = t.export()
+    inside = np.all((x >= -0.05) & (x < 0.05), axis=1) & (inf != 0)
+    assert (ex["pcount"] == 1).sum() == inside.sum()
+    assert ex["pcount"][0] == n
+
+
+def test_tree_minus_direct_is_infront_segment():
+    """With theta -> 0 every node opens to its leaves, so the tree sum is the
+    direct sum minus the segment infront(i) -> infront(infront(i)), which the
+    leaf rule skips (src/tree.f90:371) and the direct sum keeps
+    (src/timestep.f90:471)."""
+    w = W.random_rings(6, 0.005, 0.01, 5e-4, 0.1, seed=5)
+    base = dict(w.params, boundary="open")
+    pd = O.params(**dict(base, velocity="BS", tree_theta=0.0))
+    pt = O.params(**dict(base, velocity="Tree", tree_theta=1e-12))
+    gh = O.ghosts(pd, w.x, w.infront, w.behind)
+    ud, *_ = O.velocity(pd, w.x, w.infront, w.behind, gh)
+    t = O.Tree(pt, w.x, gh[0], w.infront)
+    ut, *_ = O.velocity(pt, w.x, w.infront, w.behind, gh, t)
+    a = w.infront - 1
+    R1 = w.x[a] - w.x
+    R2 = gh[0][a] - w.x
+    r1 = np.linalg.norm(R1, axis=1)
+    r2 = np.linalg.norm(R2, axis=1)
+    f = (r1 + r2) / (r1 * r2 * (r1 * r2 + (R1 * R2).sum(1)))
+    seg = 9.97e-4 / (4 * np.pi) * f[:, None] * np.cross(R1, R2)
+    err = np.abs(ud - ut - seg).max() / np.abs(ud).max()
+    assert err < 1e-9, err
+
+
+def test_ab_ladder_rungs():
+    """Euler -> AB2 -> AB3 -> AB4 selected by exact-zero history
+    (src/timestep.f90:51-61)."""
+    n = 4
+    x = np.zeros((n, 3))
+    u = np.ones((n, 3))
+    h = [np.zeros((n, 3)) for _ in range(3)]
+    inf = np.arange(1, n + 1, dtype=np.int32)
+    for k in range(1, n):
+        for j in range(k):
+            h[j][k] = 2.0
+    dt = 0.5
+    xn, u1, u2, u3 = O.pmotion_ab(dt, x, u, *h, inf)
+    assert xn[0, 0] == dt * 1.0
+    assert xn[1, 0] == 1.5 * dt * 1.0 - 0.5 * dt * 2.0
+    assert xn[2, 0] == pytest.approx(23 / 12 * dt - 4 / 3 * dt * 2 + 5 / 12 * dt * 2, rel=1e-15)
+    assert xn[3, 0] == pytest.approx(dt * (55 - 59 * 2 + 37 * 2 - 9 * 2) / 24, rel=1e-15)
+    np.testing.assert_array_equal(u1, u)
+    np.testing.assert_array_equal(u2, h[0])
+    np.testing.assert_array_equal(u3, h[1])
+
+
+def test_ghost_unwrap_periodic():
+    L = 0.1
+    x = np.array([[0.049, 0.0, 0.0], [-0.049, 0.0, 0.0], [-0.045, 0.0, 0.0]])
+    inf = np.array([2, 3, 1], np.int32)
+    beh = np.array([3, 1, 2], np.int32)
+    p = O.params(boundary="periodic", box_size=L)
+    gi, gb, gii, gbb = O.ghosts(p, x, inf, beh)
+    assert gi[0, 0] == pytest.approx(-0.049 + L)
+    assert gb[1, 0] == pytest.approx(0.049 - L)
+    po = O.params(boundary="open", box_size=L)
+    gi2, *_ = O.ghosts(po, x, inf, beh)
+    assert gi2[0, 0] == -0.049
+
+
+def test_pclose_matches_bruteforce_numpy():
+    w = W.random_rings(5, 0.004, 0.008, 5e-4, 0.1, seed=11)
+    cl, cd = O.pclose(w.x, w.infront, w.behind, np.zeros(w.n, np.int32))
+    d = np.linalg.norm(w.x[:, None, :] - w.x[None, :, :], axis=2)
+    idx = np.arange(w.n)
+    d[idx, idx] = np.inf
+    d[idx, w.infront - 1] = np.inf
+    d[idx, w.behind - 1] = np.inf
+    j = d.argmin(axis=1)
+    np.testing.assert_array_equal(cl, j + 1)
+    np.testing.assert_allclose(cd, d[idx, j], rtol=1e-15)
