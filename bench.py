@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark of the velocity-and-timestep path on B200.
+
+Workload (one "step"): the loop body of src/run.f90:41-107 restricted to the
+path -- ghost gather, octree build, Biot-Savart velocity (LIA + Barnes-Hut
+walk with 26 periodic images, FP32 pair terms with FP64 recentring and
+compensated sums), Adams-Bashforth update, reconnection candidate search,
+periodic wrap -- on the random-ring tangle: 100 rings, R ~ U(0.008, 0.02) cm,
+delta 5e-4 cm (N ~ 24.7k points), periodic box 0.1 cm, theta 0.4, dt 1e-7 s.
+Inputs are seeded synthetic rings (no dataset).
+
+Metric: direct-equivalent Biot-Savart pair interactions per second,
+N * N_active * 27 per step / step time (the unit the O(N^2) direct form would
+have to evaluate), whole job over all ranks.  Every rank runs an independent
+replica (the path does not shard; "replicas only").
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank drives cuda:LOCAL_RANK; the timed region is bracketed
+by a barrier and a synchronize, and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "BS direct-equivalent pair-interactions/s (mixed BH velocity+step)"
+UNIT = "pairs/s"
+FLOP_LEAF = 38.0   # algorithmic FP32 FLOP of one straight-segment pair term
+FLOP_FAR = 50.0    # algorithmic FP32 FLOP of one monopole+dipole cell term
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--quick", action="store_true",
+                    help="headline timing only (no comparators, e2e or CPU baseline)")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait(timeout=5)
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(seed: int):
+    from qvort_b200 import workloads as W
+
+    return W.tangle(seed)
+
+
+# ----------------------------------------------------------------------- CPU
+def cpu_step_rate(w, seconds_budget: float = 12.0, nthreads: int | None = None):
+    """Oracle (the C restatement, OpenMP over targets) on the host cores: time
+    the path's step on a bounded sample -- full ghost gather, tree build, AB
+    update and wrap; velocity and candidate search on a strided subset of
+    targets, scaled to all targets.  Returns (step seconds, sample text, cores)."""
+    from oracle import oracle as O
+
+    nthreads = nthreads or os.cpu_count() or 1
+    p = O.params(**w.params)
+    x, inf, beh = w.x.copy(), w.infront, w.behind
+    t0 = time.perf_counter()
+    g = O.ghosts(p, x, inf, beh)
+    t_g = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tree = O.Tree(p, x, g[0], inf)
+    t_b = time.perf_counter() - t0
+    # probe the per-target cost on a small stride, then size the sample
+    probe = np.arange(0, w.n, max(1, w.n // 256), dtype=np.int32)
+    t0 = time.perf_counter()
+    O.velocity(p, x, inf, beh, g, tree, targets=probe, nthreads=nthreads)
+    per = (time.perf_counter() - t0) / len(probe)
+    m = int(min(w.n, max(len(probe), seconds_budget / max(per, 1e-9))))
+    tg = np.linspace(0, w.n - 1, m).astype(np.int32)
+    t0 = time.perf_counter()
+    u, *_ = O.velocity(p, x, inf, beh, g, tree, targets=tg, nthreads=nthreads)
+    t_v = (time.perf_counter() - t0) * w.n / m
+    uf = np.zeros_like(x)
+    uf[tg] = u
+    h = [np.zeros_like(x) for _ in range(3)]
+    t0 = time.perf_counter()
+    xn, *_ = O.pmotion_ab(p.dt, x, uf, *h, inf)
+    t_ab = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.pclose_tree(tree, xn, inf, beh, np.zeros(w.n, np.int32), nthreads)
+    t_c = time.perf_counter() - t0
+    t_step = t_g * 2 + t_b + t_v + t_ab + t_c
+    sample = (f"1 step of the same workload: ghosts, tree build, AB, candidate search on all "
+              f"{w.n} points; velocity on {m} evenly strided targets scaled by {w.n}/{m}")
+    return t_step, sample, nthreads
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = workload(args.seed)
+    pairs = float(w.n) * w.n * 27
+    for _ in range(args.warmup):
+        cpu_step_rate(w, seconds_budget=1.0)
+    ts = []
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        t, sample, cores = cpu_step_rate(w, seconds_budget=4.0)
+        ts.append(t)
+    wall = time.perf_counter() - t_wall
+    t = float(np.mean(ts))
+    v = pairs / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded random rings)",
+        "config": {"workload": "tangle: 100 rings R~U(0.008,0.02) cm, delta 5e-4, N=%d, "
+                               "periodic L=0.1, Tree theta 0.4, AB, dt 1e-7" % w.n,
+                   "n_points": w.n},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample,
+                         "note": "no Fortran compiler on this image: the reference's own "
+                                 "Fortran/OpenMP path cannot be built; this is the C "
+                                 "restatement of it (oracle/qv_oracle.c)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------- GPU
+def our_arm(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from qvort_b200 import lib as L
+
+    w = workload(args.seed)
+    n = w.n
+    pairs_step = float(n) * n * 27
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    ctx = L.Context(L.default_params(**w.params, precision="mixed"), stream=sp)
+    ctx.set_points(w.x, w.infront, w.behind)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    itime = 0
+    for _ in range(max(3, args.warmup)):
+        itime += 1
+        ctx.step(itime)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    launches0 = ctx.counters()["launches"]
+    clocks = Clocks(local)
+    clocks.start()
+    evs = []
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)       # L2 flush between timed steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            itime += 1
+            ctx.step(itime)
+            e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ctx.counters()["launches"] - launches0
+    ms_total = sum(a.elapsed_time(b) for a, b in evs)
+    if ws > 1:
+        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_total = float(t.item())
+        torch.distributed.barrier()
+    ms_step = ms_total / args.steps
+    value = ws * pairs_step / (ms_step * 1e-3)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair terms, f64 recentring/LIA/AB",
+        "data": "synthetic (seeded random rings)",
+        "config": {"workload": "tangle: 100 rings R~U(0.008,0.02) cm, delta 5e-4, N=%d, "
+                               "periodic L=0.1 (26 images), Tree theta 0.4, mixed precision, "
+                               "AB ladder, dt 1e-7, candidate search every step" % n,
+                   "n_points": n, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{ws} (path does not shard)"},
+        "steps_per_s": 1e3 / ms_step * ws,
+        "clocks": clk,
+        "gpu_launches": int(launches),
+    }
+    if not args.quick and rank == 0:
+        line.update(extras(ctx, w, stream, L, torch, itime))
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _rel(a, b):
+    return (float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum())),
+            float((np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)).max()))
+
+
+def extras(ctx, w, stream, L, torch, itime):
+    out = {}
+    n = w.n
+    pairs_step = float(n) * n * 27
+    sp = stream.cuda_stream
+
+    # ---- phase breakdown and the dominant kernel (the tree walk)
+    ctx.profile(True)
+    ctx.phase_times(reset=True)
+    nprof = 5
+    for _ in range(nprof):
+        itime += 1
+        ctx.step(itime)
+    ph = ctx.phase_times(reset=True)
+    ctx.profile(False)
+    cnt = ctx.counters()
+    walk_ms = ph["nonlocal"] / nprof
+    flops = cnt["leaf_evals"] * FLOP_LEAF + cnt["far_evals"] * FLOP_FAR
+    peak = L.probe_fp32(sp)
+    achieved = flops / (walk_ms * 1e-3) / 1e12
+    traffic = None
+    prof = ROOT / "profiles" / "walk_tangle_traffic.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("bytes_per_launch")
+    out["phases_ms_per_step"] = {k: v / nprof for k, v in ph.items()}
+    out["roofline"] = {
+        "kernel": "k_walk32 (Barnes-Hut walk, mixed)", "bound": "fp32",
+        "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+        "traffic": traffic,
+        "peak_source": "measured FP32 FMA throughput on this GPU (qv_probe_fp32); "
+                       "MEASURED_PEAKS.json has no FP32-pipe figure",
+        "flop_model": f"{FLOP_LEAF:.0f} FLOP/leaf pair + {FLOP_FAR:.0f} FLOP/far cell "
+                      "(algorithmic; theta tests, recentring and Kahan excluded)",
+        "leaf_evals": cnt["leaf_evals"], "far_evals": cnt["far_evals"],
+        "walk_ms": walk_ms,
+    }
+    out["evals_per_step"] = cnt["leaf_evals"] + cnt["far_evals"] + 2 * n
+
+    # ---- accuracy at the initial state: mixed BH vs FP64 BH vs FP64 direct
+    vel = {}
+    for key, prm in (("bh_mixed", dict(precision="mixed")), ("bh_fp64", dict(precision="fp64")),
+                     ("direct_fp64", dict(precision="fp64", velocity="BS", tree_theta=0.0))):
+        pr = dict(w.params)
+        pr.update(prm)
+        c = L.Context(L.default_params(**pr), stream=sp)
+        c.set_points(w.x, w.infront, w.behind)
+        vel[key] = c.velocity(False)[0]
+        if key == "direct_fp64":
+            # time the FP64 direct form: velocity + step
+            c.step(1)
+            torch.cuda.synchronize()
+            ts = []
+            for k in range(2):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                c.step(2 + k)
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = float(np.mean(ts))
+            out["fp64_direct"] = {"ms_per_step": ms, "pairs_per_s": pairs_step / (ms * 1e-3)}
+        c.close()
+    rms, mx = _rel(vel["bh_mixed"], vel["bh_fp64"])
+    rms_a, mx_a = _rel(vel["bh_fp64"], vel["direct_fp64"])
+    out["error"] = {"mixed_vs_fp64_bh_rms_rel": rms, "mixed_vs_fp64_bh_max_rel": mx,
+                    "bh_vs_fp64_direct_rms_rel": rms_a, "bh_vs_fp64_direct_max_rel": mx_a}
+
+    # ---- end to end through the C ABI with pinned host buffers (the Fortran
+    # shim's per-step pattern: gather f(:) in, step, scatter f(:) out)
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+    hx = pin((n, 3), torch.float64); hx[:] = w.x
+    hinf = pin((n,), torch.int32); hinf[:] = w.infront
+    hbeh = pin((n,), torch.int32); hbeh[:] = w.behind
+    hist = [pin((n, 3), torch.float64) for _ in range(3)]
+    for h in hist:
+        h[:] = 0
+    hcl = pin((n,), torch.int32); hcl[:] = 0
+    hu = pin((n, 3), torch.float64)
+    hcd = pin((n,), torch.float64)
+    c = L.Context(L.default_params(**w.params, precision="mixed"), stream=sp)
+    def e2e_step(it):
+        c.set_points(hx, hinf, hbeh)
+        c.set_history(*hist)
+        c.set_closest(hcl)
+        c.step(it)
+        c.get_points(hx, hu)
+        c.get_history(*hist)
+        c.get_closest(hcl, hcd)
+
+    for it in range(3):
+        e2e_step(it + 1)
+    torch.cuda.synchronize()
+    K = 10
+    t0 = time.perf_counter()
+    for it in range(K):
+        e2e_step(it + 4)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / K
+    c.close()
+    h2d = n * (24 + 8 + 72 + 4)
+    d2h = n * (24 + 24 + 72 + 4 + 8)
+    out["e2e"] = {"value": pairs_step / (e2e_ms * 1e-3), "unit": UNIT,
+                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                  "path": "qv_set_points/qv_set_history/qv_set_closest (pinned host) -> qv_step "
+                          "-> qv_get_points/qv_get_history/qv_get_closest (pinned host), "
+                          "wall clock"}
+
+    # ---- CPU baseline (oracle port on this host's cores), bounded sample
+    t, sample, cores = cpu_step_rate(w)
+    out["cpu_baseline"] = {"value": pairs_step / t, "unit": UNIT, "cores": cores, "kind": "port",
+                           "sample": sample, "ms_per_step": t * 1e3}
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

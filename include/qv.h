@@ -91,6 +91,8 @@ int qv_get_history(qv_ctx *ctx, double *u1, double *u2, double *u3);
 int qv_set_closest(qv_ctx *ctx, const int *closest);
 /* Scatter back f(:)%x and f(:)%u (host; NULL skips). */
 int qv_get_points(qv_ctx *ctx, double *x, double *u);
+/* Scatter back f(:)%closest and f(:)%closestd of the last candidate search. */
+int qv_get_closest(qv_ctx *ctx, int *closest, double *closestd);
 /* Device pointers of the context's arrays (valid until the next set_points). */
 int qv_device_arrays(qv_ctx *ctx, double **x, double **u, int **infront, int **behind);
 

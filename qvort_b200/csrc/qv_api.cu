@@ -127,6 +127,12 @@ extern "C" int qv_destroy(qv_ctx *c) {
   }
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->dscalar) cudaFree(c->dscalar);
+  if (c->walk_part) cudaFree(c->walk_part);
+  for (int k = 0; k < 2; k++) {
+    if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
+    if (c->ev_join[k]) cudaEventDestroy(c->ev_join[k]);
+  }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return QV_OK;
@@ -234,6 +240,16 @@ extern "C" int qv_get_points(qv_ctx *c, double *x, double *u) {
   size_t v = sizeof(double) * 3 * (size_t)c->n;
   if (x && v) QV_CUDA(c, cudaMemcpyAsync(x, c->x, v, cudaMemcpyDeviceToHost, c->stream));
   if (u && v) QV_CUDA(c, cudaMemcpyAsync(u, c->u, v, cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+extern "C" int qv_get_closest(qv_ctx *c, int *closest, double *closestd) {
+  QV_CHECK_CTX(c);
+  if (closest && c->n)
+    QV_CUDA(c, cudaMemcpyAsync(closest, c->closest, sizeof(int) * c->n, cudaMemcpyDeviceToHost, c->stream));
+  if (closestd && c->n)
+    QV_CUDA(c, cudaMemcpyAsync(closestd, c->closestd, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
   return QV_OK;
 }

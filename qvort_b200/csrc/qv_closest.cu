@@ -21,10 +21,15 @@ __device__ __forceinline__ double dist_exact(const double *a, double b0, double 
   return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
 }
 
+// Every comparison is first taken in FP32 from (hi, lo) float pairs of the
+// FP64 coordinates; only when it falls within a relative 1e-5 of its
+// threshold (or a distance must be stored) is the FP64 expression of the
+// reference evaluated, so the outcome is always the FP64 outcome.
 __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *__restrict__ x,
                                                          const int *__restrict__ inf,
                                                          const int *__restrict__ beh,
                                                          const WNode64 *__restrict__ w64,
+                                                         const WNode32 *__restrict__ w32,
                                                          int *closest, double *closestd,
                                                          int *status) {
   __shared__ int2 stk[CW][CSTK];
@@ -37,9 +42,16 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
     double xi[3] = {0., 0., 0.};
     int ii = i + 1, fi = -1, bi = -1, cl = 0;
     double cd = 100.;
+    float cd32 = 100.f;
+    float xh[3] = {0.f, 0.f, 0.f}, xl[3] = {0.f, 0.f, 0.f};
     if (live) {
       xi[0] = x[3 * i]; xi[1] = x[3 * i + 1]; xi[2] = x[3 * i + 2];
       fi = inf[i]; bi = beh[i]; cl = closest[i];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        xh[c] = __double2float_rn(xi[c]);
+        xl[c] = __double2float_rn(xi[c] - (double)xh[c]);
+      }
     }
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
     bool bad = false;
@@ -53,20 +65,53 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
       __syncwarp();
       const int node = e.x;
       const bool in = (((unsigned)e.y) >> lane) & 1u;
-      const WNode64 h = w64[node];
+      const WNode32 h = w32[node];
       bool open = false;
       if (in && h.count > 0) {
-        double dist = dist_exact(xi, h.cx, h.cy, h.cz);
-        double theta = __ddiv_rn(h.width, dist);
-        if (h.count == 1 || theta < .5) {
-          if (dist < cd) {
+        float v0 = (xh[0] - h.ch[0]) + (xl[0] - h.cl[0]);
+        float v1 = (xh[1] - h.ch[1]) + (xl[1] - h.cl[1]);
+        float v2 = (xh[2] - h.ch[2]) + (xl[2] - h.cl[2]);
+        float d32 = sqrtf(fmaf(v0, v0, fmaf(v1, v1, v2 * v2)));
+        bool tiny = d32 < 1e-10f;
+        double d64 = -1.;  // exact distance, computed on demand
+        bool pass;
+        if (h.count == 1) {
+          pass = true;
+        } else {
+          // theta = width/dist < 0.5  (src/tree.f90:248-249)
+          float diff = 0.5f * d32 - h.width;
+          if (!tiny && fabsf(diff) > 1e-5f * h.width) {
+            pass = diff > 0.f;
+          } else {
+            const WNode64 hh = w64[node];
+            d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
+            pass = __ddiv_rn(hh.width, d64) < .5;
+          }
+        }
+        if (pass) {
+          // dist < closestd
+          bool closer;
+          float dc = d32 - cd32;
+          if (!tiny && fabsf(dc) > 1e-5f * cd32 && d64 < 0.) {
+            closer = dc < 0.f;
+          } else {
+            if (d64 < 0.) {
+              const WNode64 hh = w64[node];
+              d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
+            }
+            closer = d64 < cd;
+          }
+          if (closer) {
             if (h.count > 1) {
               cl = 0;
             } else {
-              int j = beh[h.finf - 1];  // f(parray(1)%infront)%behind with current links
+              const WNode64 hh = w64[node];
+              int j = beh[hh.finf - 1];  // f(parray(1)%infront)%behind with current links
               if (ii != j && fi != j && bi != j) {
+                if (d64 < 0.) d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
                 cl = j;
-                cd = dist;
+                cd = d64;
+                cd32 = __double2float_rn(cd);
               }
             }
           }
@@ -145,7 +190,8 @@ int qv_launch_closest(qv_ctx *c) {
     if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
     int nwarps = (c->n + 31) / 32;
     k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, 0, c->stream>>>(
-        c->n, c->x, c->infront, c->behind, c->tree.w64, c->closest, c->closestd, c->dstatus);
+        c->n, c->x, c->infront, c->behind, c->tree.w64, c->tree.w32, c->closest, c->closestd,
+        c->dstatus);
   } else {
     k_pclose<<<(c->n + PT - 1) / PT, PT, 0, c->stream>>>(c->n, c->x, c->infront, c->behind,
                                                          c->closest, c->closestd);

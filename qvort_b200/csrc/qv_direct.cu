@@ -96,7 +96,7 @@ int qv_compact_active(qv_ctx *c) {
 
 // ------------------------------------------------------------ source packs
 // FP64: x(3), s=gi-x(3), c=|gi-x|^2, slot (1-based) as double.
-// FP32: x hi(3), x lo(3), gi hi(3), gi lo(3), slot bits, pad.
+// FP32: x hi(3), x lo(3), gi hi(3), gi lo(3), slot bits, s = gi - x (3).
 __global__ void k_pack_sources(int na, const int *__restrict__ act, const double *__restrict__ x,
                                const double *__restrict__ gi, double *s64, float *s32) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,7 +122,9 @@ __global__ void k_pack_sources(int na, const int *__restrict__ act, const double
     f[9 + k] = __double2float_rn(G[k] - (double)g);
   }
   f[12] = __int_as_float(j + 1);
-  f[13] = f[14] = f[15] = 0.f;
+  f[13] = __double2float_rn(e0);
+  f[14] = __double2float_rn(e1);
+  f[15] = __double2float_rn(e2);
 }
 
 // ------------------------------------------------------------ pair terms
@@ -158,12 +160,6 @@ struct Kahan3 {
   __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
 };
 
-// Stable straight-segment term without the G/(4 pi) factor.
-__device__ __forceinline__ void seg32(float r1x, float r1y, float r1z, float r2x, float r2y,
-                                      float r2z, float &ox, float &oy, float &oz) {
-  float r1s = fmaf(r1x, r1x, fmaf(r1y, r1y, r1z * r1z));
-  qv_seg32(r1x, r1y, r1z, r2x, r2y, r2z, r1s, ox, oy, oz);
-}
 
 template <int BC>
 __device__ __forceinline__ void img_mul(int m, int &a, int &b, int &c) {
@@ -235,7 +231,7 @@ __device__ __forceinline__ void seg_tile(const float4 *tile, int m, const double
     float4 A = tile[4 * k], B = tile[4 * k + 1], Cc = tile[4 * k + 2], D = tile[4 * k + 3];
     int jj = __float_as_int(D.x);
     if (jj == bi || jj == skip2) continue;
-    // A = (xh0 xh1 xh2 xl0) B = (xl1 xl2 gh0 gh1) C = (gh2 gl0 gl1 gl2)
+    // A = (xh0 xh1 xh2 xl0) B = (xl1 xl2 gh0 gh1) C = (gh2 gl0 gl1 gl2) D = (slot s0 s1 s2)
     float r1x = (A.x - th[0]) + (A.w - tl[0]);
     float r1y = (A.y - th[1]) + (B.x - tl[1]);
     float r1z = (A.z - th[2]) + (B.y - tl[2]);
@@ -243,7 +239,8 @@ __device__ __forceinline__ void seg_tile(const float4 *tile, int m, const double
     float r2y = (B.w - th[1]) + (Cc.z - tl[1]);
     float r2z = (Cc.x - th[2]) + (Cc.w - tl[2]);
     float ox, oy, oz;
-    seg32(r1x, r1y, r1z, r2x, r2y, r2z, ox, oy, oz);
+    float r1s = fmaf(r1x, r1x, fmaf(r1y, r1y, r1z * r1z));
+    qv_seg32(r1x, r1y, r1z, r2x, r2y, r2z, D.y, D.z, D.w, r1s, ox, oy, oz);
     acc.add(ox, oy, oz);
   }
 }

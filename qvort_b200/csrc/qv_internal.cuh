@@ -47,11 +47,12 @@ struct __align__(16) WNode32 {
   int count, child_first, nchild, jb;
 };
 
-// FP32 payload (64 B): internal -> circ, w, C; leaf -> ghosti as (hi, lo).
+// FP32 payload (64 B): internal -> circ, w, C; leaf -> ghosti as (hi, lo)
+// and the segment vector s = ghosti - x in C[0..2].
 struct __align__(16) WPay32 {
   float a[3];  // circ | gi hi
   float b[3];  // w | gi lo
-  float C[9];
+  float C[9];  // C | s
   float pad;
 };
 
@@ -102,6 +103,8 @@ struct qv_ctx {
   unsigned long long *evals = nullptr;  // device eval counter
   int *dstatus = nullptr;               // device status word
   double *dscalar = nullptr;            // device scalar scratch
+  double *walk_part = nullptr;          // per-image partial sums of the walk
+  size_t walk_part_bytes = 0;
   bool ghosts_valid = false;
   TreeBuf tree;
   int sm_count = 148;
@@ -112,6 +115,8 @@ struct qv_ctx {
   double phase_ms[PH_N] = {};
   long long launches = 0;
   unsigned long long *evals_far = nullptr;
+  cudaStream_t aux[2] = {nullptr, nullptr};  // side streams for independent chains
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   long long last_leaf = 0, last_far = 0;
   char err[512] = {0};
 };
@@ -145,23 +150,28 @@ int qv_launch_wrap(qv_ctx *c);
 int qv_launch_closest(qv_ctx *c);
 int qv_launch_energy(qv_ctx *c, double *out_host);
 int qv_compact_active(qv_ctx *c);
+int qv_aux_streams(qv_ctx *c);
 
 // ---------------------------------------------------------------- helpers
 // Straight-segment Biot-Savart term in FP32, without the G/(4 pi) factor:
 //   (|R1|+|R2|) / (|R1||R2| (|R1||R2| + R1.R2)) * (R1 x R2)
 // (src/tree.f90:380-390), written with q = 1/(|R1||R2|) as
-//   (1/|R1| + 1/|R2|) q / (1 + cos) * (R1 x R2),  cos = R1.R2 q.
+//   (1/|R1| + 1/|R2|) q / (1 + cos) * (R1 x s),  cos = R1.R2 q,
+// where s = ghosti - x is the segment vector (R2 = R1 + s).  R1 x R2 equals
+// R1 x s, and the latter does not cancel when the segment is far away
+// (R1 ~ R2); s is an FP64 difference rounded once to FP32.
 // When cos < 0 the sum 1 + cos cancels; it is then taken from the identity
-// (1 + cos)(1 - cos) = sin^2 = |R1 x R2|^2 q^2, which has no cancellation.
+// (1 + cos)(1 - cos) = sin^2 = |R1 x s|^2 q^2, which has no cancellation.
 __device__ __forceinline__ void qv_seg32(float r1x, float r1y, float r1z, float r2x, float r2y,
-                                         float r2z, float r1s, float &ox, float &oy, float &oz) {
+                                         float r2z, float sx, float sy, float sz, float r1s,
+                                         float &ox, float &oy, float &oz) {
   float r2s = fmaf(r2x, r2x, fmaf(r2y, r2y, r2z * r2z));
   float dd = fmaf(r1x, r2x, fmaf(r1y, r2y, r1z * r2z));
   float ra = rsqrtf(r1s), rb = rsqrtf(r2s);
   float q = ra * rb;
-  float cx = fmaf(r1y, r2z, -r1z * r2y);
-  float cy = fmaf(r1z, r2x, -r1x * r2z);
-  float cz = fmaf(r1x, r2y, -r1y * r2x);
+  float cx = fmaf(r1y, sz, -r1z * sy);
+  float cy = fmaf(r1z, sx, -r1x * sz);
+  float cz = fmaf(r1x, sy, -r1y * sx);
   float cs = dd * q;
   float den = cs >= 0.f ? 1.f + cs
                         : fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);

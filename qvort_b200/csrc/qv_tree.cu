@@ -42,6 +42,7 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 #define CTL_NSPLIT_NEXT 2
 #define CTL_OVERFLOW 3  // 1 = node capacity, 2 = level capacity
 #define CTL_DEPTH 4
+#define CTL_NBIG 5      // number of nodes handled by k_moments_big
 #define CTL_LVL 8       // lvl_start[0..QV_MAX_DEPTH+2]
 #define CTL_SIZE (CTL_LVL + QV_MAX_DEPTH + 4)
 
@@ -317,7 +318,15 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
 }
 
 // --------------------------------------------------------------- moments
-#define MW 8  // warps per block
+// A node's moments are 15 independent sequential FP64 chains over its points
+// in ascending slot order: cent (3), circ (3) and Cij (9).  The chains cannot
+// be reassociated, so their latency is the floor; the kernels below keep the
+// chain lanes fed from shared memory while other warps gather and precompute.
+#define MW 8      // warps per block (small nodes: one warp per node)
+#define BIGN 256  // nodes with more points use a whole block
+#define MC 256    // points per shared-memory chunk in the block kernel
+
+// One warp per node with at most BIGN points.
 __global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__restrict__ level,
                                                      const int *__restrict__ start,
                                                      const int *__restrict__ count,
@@ -329,6 +338,7 @@ __global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__r
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int k = 1 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
     int s = start[k], n = count[k];
+    if (n > BIGN) continue;
     const int *o = ord + (size_t)level[k] * cap_pts + s;
     double acc = 0.;
     for (int base = 0; base < n; base += 32) {
@@ -369,32 +379,131 @@ __global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__r
   }
 }
 
-// Root centroid: masked mean over all slots in ascending order
-// (src/tree.f90:53-55), sequential per component.
-__global__ void k_root_cent(int n, const double *__restrict__ x, const int *__restrict__ inf,
-                            double *cent) {
-  __shared__ double bx[32][3];
-  __shared__ int ba[32];
-  int lane = threadIdx.x;
-  double acc = 0.;
-  int cnt = 0;
-  for (int base = 0; base < n; base += 32) {
-    int m = min(32, n - base);
-    if (lane < m) {
-      int i = base + lane;
-      ba[lane] = inf[i] > 0;
-      for (int c = 0; c < 3; c++) bx[lane][c] = x[3 * i + c];
+// List the nodes with more than BIGN points (order irrelevant).
+__global__ void k_list_big(int n_nodes, const int *__restrict__ count, int *list, int *nlist) {
+  for (int k = 1 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
+    if (count[k] > BIGN) list[atomicAdd(nlist, 1)] = k;
+}
+
+// One block per node with more than BIGN points: warps 1.. gather x, ghosti and
+// the Cij products of the next chunk into shared memory while warp 0's lanes
+// 0..14 run the chains over the current chunk (double buffered).
+__global__ void __launch_bounds__(256) k_moments_big(const int *__restrict__ list,
+                                                     const int *__restrict__ nlist,
+                                                     const int *__restrict__ level,
+                                                     const int *__restrict__ start,
+                                                     const int *__restrict__ count,
+                                                     const int *__restrict__ ord, int cap_pts,
+                                                     const double *__restrict__ x,
+                                                     const double *__restrict__ gi, double *cent,
+                                                     double *circ, double *C, int *first) {
+  extern __shared__ double mb[];  // [2][MC][15]
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nl = *nlist;
+  for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    const int k = list[li];
+    const int s = start[k], n = count[k];
+    const int *o = ord + (size_t)level[k] * cap_pts + s;
+    const int nch = (n + MC - 1) / MC;
+    auto produce = [&](int ch, double *dst) {
+      int base = ch * MC, m = min(MC, n - base);
+      for (int q = threadIdx.x - 32; q < m; q += blockDim.x - 32) {
+        int idx = o[base + q];
+        double X[3], G[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
+        double *b = dst + 15 * q;
+#pragma unroll
+        for (int c = 0; c < 3; c++) { b[c] = X[c]; b[3 + c] = G[c]; }
+#pragma unroll
+        for (int mm = 0; mm < 3; mm++)
+#pragma unroll
+          for (int kk = 0; kk < 3; kk++) b[6 + 3 * mm + kk] = __dmul_rn(X[mm], __dsub_rn(G[kk], X[kk]));
+      }
+    };
+    __syncthreads();
+    if (wid > 0) produce(0, mb);
+    __syncthreads();
+    double acc = 0.;
+    for (int ch = 0; ch < nch; ch++) {
+      double *cur = mb + (ch & 1) * MC * 15;
+      if (wid > 0) {
+        if (ch + 1 < nch) produce(ch + 1, mb + ((ch + 1) & 1) * MC * 15);
+      } else if (lane < 15) {
+        const int m = min(MC, n - ch * MC);
+        const double *b = cur + lane;
+        if (lane < 3 || lane >= 6) {
+          int q = 0;
+          for (; q + 4 <= m; q += 4) {
+            double a0 = b[15 * q], a1 = b[15 * (q + 1)], a2 = b[15 * (q + 2)], a3 = b[15 * (q + 3)];
+            acc = __dadd_rn(acc, a0);
+            acc = __dadd_rn(acc, a1);
+            acc = __dadd_rn(acc, a2);
+            acc = __dadd_rn(acc, a3);
+          }
+          for (; q < m; q++) acc = __dadd_rn(acc, b[15 * q]);
+        } else {
+          const double *gx = cur + (lane - 3);
+          for (int q = 0; q < m; q++) acc = __dsub_rn(__dadd_rn(acc, gx[15 * q + 3]), gx[15 * q]);
+        }
+      }
+      __syncthreads();
     }
-    __syncwarp();
-    if (lane < 3)
-      for (int q = 0; q < m; q++)
-        if (ba[q]) acc = __dadd_rn(acc, bx[q][lane]);
-    if (lane == 3)
-      for (int q = 0; q < m; q++) cnt += ba[q];
-    __syncwarp();
+    if (wid == 0) {
+      double cm = lane < 3 ? __ddiv_rn(acc, (double)n) : 0.;
+      int ci = (lane - 6) / 3, ck = (lane - 6) % 3;
+      double cen = __shfl_sync(0xffffffffu, cm, lane >= 6 && lane < 15 ? ci : 0);
+      double cir = __shfl_sync(0xffffffffu, acc, lane >= 6 && lane < 15 ? 3 + ck : 0);
+      if (lane < 3) cent[3 * k + lane] = cm;
+      else if (lane < 6) circ[3 * k + lane - 3] = acc;
+      else if (lane < 15) C[9 * k + 3 * ci + ck] = __dsub_rn(acc, __dmul_rn(cen, cir));
+      if (lane == 0) first[k] = o[0];
+    }
   }
-  cnt = __shfl_sync(0xffffffffu, cnt, 3);
-  if (lane < 3) cent[lane] = __ddiv_rn(acc, (double)cnt);
+}
+
+// Root centroid: masked mean over all slots in ascending order
+// (src/tree.f90:53-55) = sequential sums over the compacted active list.
+// Warps 1.. stage chunks of positions in shared memory (double buffered);
+// lanes 0..2 of warp 0 run the three chains.
+#define RC 2048
+__global__ void __launch_bounds__(512) k_root_cent(int n_act, const int *__restrict__ act,
+                                                   const double *__restrict__ x, double *cent) {
+  extern __shared__ double rb[];  // [2][RC][3]
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nch = (n_act + RC - 1) / RC;
+  auto produce = [&](int ch, double *dst) {
+    int base = ch * RC, m = min(RC, n_act - base);
+    for (int q = threadIdx.x - 32; q < m; q += blockDim.x - 32) {
+      int i = act[base + q];
+      dst[3 * q] = x[3 * i];
+      dst[3 * q + 1] = x[3 * i + 1];
+      dst[3 * q + 2] = x[3 * i + 2];
+    }
+  };
+  if (wid > 0 && nch > 0) produce(0, rb);
+  __syncthreads();
+  double acc = 0.;
+  for (int ch = 0; ch < nch; ch++) {
+    double *cur = rb + (ch & 1) * RC * 3;
+    if (wid > 0) {
+      if (ch + 1 < nch) produce(ch + 1, rb + ((ch + 1) & 1) * RC * 3);
+    } else if (lane < 3) {
+      const int m = min(RC, n_act - ch * RC);
+      const double *b = cur + lane;
+      int q = 0;
+      for (; q + 8 <= m; q += 8) {
+        double a[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) a[u] = b[3 * (q + u)];
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc = __dadd_rn(acc, a[u]);
+      }
+      for (; q < m; q++) acc = __dadd_rn(acc, b[3 * q]);
+    }
+    __syncthreads();
+  }
+  if (wid == 0 && lane < 3) cent[lane] = __ddiv_rn(acc, (double)n_act);
 }
 
 // ------------------------------------------------------------ walk packs
@@ -451,6 +560,7 @@ __global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict_
       split2(q.b[c], r.a[c], r.b[c]);
     }
     for (int c = 0; c < 9; c++) { q.C[c] = 0.; r.C[c] = 0.f; }
+    for (int c = 0; c < 3; c++) r.C[c] = __double2float_rn(q.b[c] - q.a[c]);
   } else {
     const double *M = C + 9 * k;
     for (int c = 0; c < 3; c++) q.a[c] = k == 0 ? 0. : circ[3 * k + c];
@@ -535,6 +645,20 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
   return QV_OK;
 }
 
+int qv_aux_streams(qv_ctx *c) {
+  if (c->aux[0]) return QV_OK;
+  for (int k = 0; k < 2; k++) {
+    QV_CUDA(c, cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+    QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));
+  }
+  QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  QV_CUDA(c, cudaFuncSetAttribute(k_moments_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  2 * MC * 15 * (int)sizeof(double)));
+  QV_CUDA(c, cudaFuncSetAttribute(k_root_cent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  2 * RC * 3 * (int)sizeof(double)));
+  return QV_OK;
+}
+
 static int build_grid(qv_ctx *c) {
   static int cached = 0;
   if (cached) return cached;
@@ -601,17 +725,32 @@ int qv_launch_tree_build(qv_ctx *c) {
     t.n_act = na;
     t.lvl_start.assign(h + CTL_LVL, h + CTL_LVL + t.depth + 2);
     t.perm = t.ord + (size_t)t.depth * t.cap_pts;
-    // moments of all non-root nodes, then the root centroid
+    // moments of all non-root nodes and the root centroid, on three streams
+    if ((rc = qv_aux_streams(c))) return rc;
+    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
+    QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
+    k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(na, c->act, c->x, t.cent);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
     if (t.n_nodes > 1) {
+      QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
+      k_list_big<<<std::max(1, std::min(nblk(t.n_nodes, 256), 4 * c->sm_count)), 256, 0,
+                   c->aux[0]>>>(t.n_nodes, t.count, t.rnk, t.ctl + CTL_NBIG);
+      k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
+          t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
+          t.cent, t.circ, t.C, t.first);
       int nb = std::min(nblk(t.n_nodes - 1, MW), 16 * c->sm_count);
       k_moments<<<nb, MW * 32, 0, c->stream>>>(t.n_nodes, t.level, t.start, t.count, t.ord,
                                                t.cap_pts, c->x, c->gi, t.cent, t.circ, t.C,
                                                t.first);
       QV_LAUNCH_CHECK(c);
-      QV_COUNT(c, 1);
+      QV_COUNT(c, 3);
     }
-    k_root_cent<<<1, 32, 0, c->stream>>>(c->n, c->x, c->infront, t.cent);
-    QV_LAUNCH_CHECK(c);
+    QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
+    QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
     k_pack_nodes<<<nblk(t.n_nodes, 128), 128, 0, c->stream>>>(
         t.n_nodes, c->n, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first, t.nchild,
         t.first, c->x, c->gi, c->infront, c->behind, t.w64, t.p64, t.w32, t.p32);

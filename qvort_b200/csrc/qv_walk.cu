@@ -1,8 +1,12 @@
 // qv_walk.cu -- Barnes-Hut tree walk of calc_velocity's Tree arm
 // (tree_walk, src/tree.f90:336-421; image loop src/timestep.f90:276-307).
 //
-// Execution model: one warp walks the tree for 32 targets that are adjacent
-// in the tree's depth-first point order (so their traversals overlap).  The
+// Execution model: a warp task is (32 targets adjacent in the tree's
+// depth-first point order, one periodic image); a target's 27 image walks are
+// independent, so splitting them across warps gives the GPU 27x more warps to
+// hide latency with.  Each task writes per-target partial sums; a second
+// kernel adds them in the reference's image order (main image, then images
+// peri,perj,perk = -1..1), so results do not depend on scheduling.  The
 // warp keeps one explicit stack of (node, lane mask) in shared memory: at each
 // node every lane in the mask takes its own decision exactly as the reference
 // does (leaf -> exact segment, theta < tree_theta -> far-field multipole,
@@ -19,6 +23,8 @@
 // The root counts every slot and carries zero circ/Cij (src/tree.f90:51-58):
 // when an image's root passes the opening test the image adds nothing, as in
 // the reference.
+#include <algorithm>
+
 #include "qv_internal.cuh"
 
 #define WW 4                           // warps per block
@@ -35,8 +41,9 @@ struct WalkArgs {
   const WPay32 *p32;
   const double *u_li;
   double *u, *u_bs;
+  double *part;  // (NIMG+1) x n_act x 3 partial sums, image-major
   double L, theta, gfac;
-  int extra;
+  int extra, ngroups;
   unsigned long long *evals, *evals_far;
   int *status;
 };
@@ -98,9 +105,10 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
   __shared__ int2 stk[WW][STK];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int2 *st = stk[wid];
-  const int nwarps = (a.n_act + 31) / 32;
-  for (int w = blockIdx.x * WW + wid; w < nwarps; w += gridDim.x * WW) {
-    int q = w * 32 + lane;
+  const int items = a.ngroups * (NIMG + 1);
+  for (int item = blockIdx.x * WW + wid; item < items; item += gridDim.x * WW) {
+    const int m = item / a.ngroups, g = item - m * a.ngroups;
+    int q = g * 32 + lane;
     bool live = q < a.n_act;
     int i = live ? a.perm[q] : 0;
     double xi[3] = {0., 0., 0.};
@@ -110,112 +118,92 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
       bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
     }
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-    double acc0[3] = {0., 0., 0.}, acc1[3] = {0., 0., 0.};
+    double acc[3] = {0., 0., 0.};
     unsigned long long ev = 0, evf = 0;
     bool bad = false;
-#pragma unroll 1
-    for (int im = -1; im < NIMG; im++) {
-      int ma = 0, mb = 0, mc = 0;
-      if (im >= 0) qv_img_shift(BC, im, &ma, &mb, &mc);
-      const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
-      int top = 0;
-      if (lane == 0) st[0] = make_int2(0, (int)live_mask);
-      top = 1;
+    int ma = 0, mb = 0, mc = 0;
+    if (m > 0) qv_img_shift(BC, m - 1, &ma, &mb, &mc);
+    const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
+    int top = 0;
+    if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+    top = live_mask ? 1 : 0;
+    __syncwarp();
+    while (top > 0) {
+      top--;
+      int2 e = st[top];
       __syncwarp();
-      while (top > 0) {
-        top--;
-        int2 e = st[top];
-        __syncwarp();
-        const int node = e.x;
-        const bool in = (((unsigned)e.y) >> lane) & 1u;
-        const WNode64 h = a.w64[node];
-        if (h.count == 1) {
-          if (in) {
-            int j = h.jb;
-            if (j != ii && j != bi && j != fi) {
-              double dist = exact_dist(xi, h, s);
-              if (dist < QV_DEPS) {
-                bad = true;
-              } else {
-                const WPay64 &P = a.p64[node];
-                double R1[3], R2[3], cr[3];
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                  R1[c] = P.a[c] + s[c] - xi[c];
-                  R2[c] = P.b[c] + s[c] - xi[c];
-                }
-                double ra = sqrt(R1[0] * R1[0] + R1[1] * R1[1] + R1[2] * R1[2]);
-                double rb = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
-                double cc = ra * rb * (ra * rb + (R1[0] * R2[0] + R1[1] * R2[1] + R1[2] * R2[2]));
-                cross3(R1, R2, cr);
-                double f = (ra + rb) / cc;
-                if (im < 0) {
-#pragma unroll
-                  for (int c = 0; c < 3; c++) acc0[c] += f * cr[c];
-                } else {
-#pragma unroll
-                  for (int c = 0; c < 3; c++) acc1[c] += f * cr[c];
-                }
-                ev++;
-              }
-            }
-          }
-        } else {
-          bool open = false;
-          if (in) {
+      const int node = e.x;
+      const bool in = (((unsigned)e.y) >> lane) & 1u;
+      const WNode64 h = a.w64[node];
+      if (h.count == 1) {
+        if (in) {
+          int j = h.jb;
+          if (j != ii && j != bi && j != fi) {
             double dist = exact_dist(xi, h, s);
-            if (exact_open(dist, h, a.theta, a.extra)) {
-              open = true;
-            } else {
-              ev++;
-              evf++;
-              if (node != 0) {
-                const WPay64 &P = a.p64[node];
-                double v[3] = {__dsub_rn(xi[0], __dadd_rn(h.cx, s[0])),
-                               __dsub_rn(xi[1], __dadd_rn(h.cy, s[1])),
-                               __dsub_rn(xi[2], __dadd_rn(h.cz, s[2]))};
-                double d2 = dist * dist, d3 = d2 * dist, d5 = d2 * d2 * dist;
-                double cv[3], z[3], vz[3];
-                cross3(P.a, v, cv);
-#pragma unroll
-                for (int l = 0; l < 3; l++) z[l] = v[0] * P.C[l] + v[1] * P.C[3 + l] + v[2] * P.C[6 + l];
-                cross3(v, z, vz);
-                double o[3];
-#pragma unroll
-                for (int c = 0; c < 3; c++) o[c] = (cv[c] - P.b[c]) / d3 + 3. * vz[c] / d5;
-                if (im < 0) {
-#pragma unroll
-                  for (int c = 0; c < 3; c++) acc0[c] += o[c];
-                } else {
-#pragma unroll
-                  for (int c = 0; c < 3; c++) acc1[c] += o[c];
-                }
-              }
-            }
-          }
-          unsigned om = __ballot_sync(0xffffffffu, open);
-          if (om) {
-            int nc = h.nchild;
-            if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+            if (dist < QV_DEPS) {
               bad = true;
-              nc = 0;
+            } else {
+              const WPay64 &P = a.p64[node];
+              double R1[3], R2[3], cr[3];
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                R1[c] = P.a[c] + s[c] - xi[c];
+                R2[c] = P.b[c] + s[c] - xi[c];
+              }
+              double ra = sqrt(R1[0] * R1[0] + R1[1] * R1[1] + R1[2] * R1[2]);
+              double rb = sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
+              double cc = ra * rb * (ra * rb + (R1[0] * R2[0] + R1[1] * R2[1] + R1[2] * R2[2]));
+              cross3(R1, R2, cr);
+              double f = (ra + rb) / cc;
+#pragma unroll
+              for (int c = 0; c < 3; c++) acc[c] += f * cr[c];
+              ev++;
             }
-            if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
-            top += nc;
           }
-          __syncwarp();
         }
+      } else {
+        bool open = false;
+        if (in) {
+          double dist = exact_dist(xi, h, s);
+          if (exact_open(dist, h, a.theta, a.extra)) {
+            open = true;
+          } else {
+            ev++;
+            evf++;
+            if (node != 0) {
+              const WPay64 &P = a.p64[node];
+              double v[3] = {__dsub_rn(xi[0], __dadd_rn(h.cx, s[0])),
+                             __dsub_rn(xi[1], __dadd_rn(h.cy, s[1])),
+                             __dsub_rn(xi[2], __dadd_rn(h.cz, s[2]))};
+              double d2 = dist * dist, d3 = d2 * dist, d5 = d2 * d2 * dist;
+              double cv[3], z[3], vz[3];
+              cross3(P.a, v, cv);
+#pragma unroll
+              for (int l = 0; l < 3; l++) z[l] = v[0] * P.C[l] + v[1] * P.C[3 + l] + v[2] * P.C[6 + l];
+              cross3(v, z, vz);
+#pragma unroll
+              for (int c = 0; c < 3; c++) acc[c] += (cv[c] - P.b[c]) / d3 + 3. * vz[c] / d5;
+            }
+          }
+        }
+        unsigned om = __ballot_sync(0xffffffffu, open);
+        if (om) {
+          int nc = h.nchild;
+          if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+            bad = true;
+            nc = 0;
+          }
+          if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+          top += nc;
+        }
+        __syncwarp();
       }
     }
     if (live) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        double b0 = acc0[c] * a.gfac, b1 = acc1[c] * a.gfac;
-        a.u_bs[3 * i + c] = b0 + b1;
-        a.u[3 * i + c] = (a.u_li[3 * i + c] + b0) + b1;
-      }
+      double *o = a.part + ((size_t)m * a.n_act + q) * 3;
+      o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2];
     }
-      for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 16; o > 0; o >>= 1) {
       ev += __shfl_down_sync(0xffffffffu, ev, o);
       evf += __shfl_down_sync(0xffffffffu, evf, o);
     }
@@ -232,10 +220,11 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
   __shared__ int2 stk[WW][STK];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int2 *st = stk[wid];
-  const int nwarps = (a.n_act + 31) / 32;
   const float th32 = (float)a.theta;
-  for (int w = blockIdx.x * WW + wid; w < nwarps; w += gridDim.x * WW) {
-    int q = w * 32 + lane;
+  const int items = a.ngroups * (NIMG + 1);
+  for (int item = blockIdx.x * WW + wid; item < items; item += gridDim.x * WW) {
+    const int m = item / a.ngroups, g = item - m * a.ngroups;
+    int q = g * 32 + lane;
     bool live = q < a.n_act;
     int i = live ? a.perm[q] : 0;
     double xi[3] = {0., 0., 0.};
@@ -245,131 +234,120 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
       bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
     }
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-    Kahan3w k0, k1;
+    Kahan3w k0;
     k0.zero();
-    k1.zero();
     unsigned long long ev = 0, evf = 0;
     bool bad = false;
-#pragma unroll 1
-    for (int im = -1; im < NIMG; im++) {
-      int ma = 0, mb = 0, mc = 0;
-      if (im >= 0) qv_img_shift(BC, im, &ma, &mb, &mc);
-      const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
-      // target recentred for this image, t = x_i - shift as (hi, lo) floats
-      float th[3], tl[3];
+    int ma = 0, mb = 0, mc = 0;
+    if (m > 0) qv_img_shift(BC, m - 1, &ma, &mb, &mc);
+    const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
+    // target recentred for this image, t = x_i - shift as (hi, lo) floats
+    float th[3], tl[3];
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        double t = xi[c] - s[c];
-        th[c] = __double2float_rn(t);
-        tl[c] = __double2float_rn(t - (double)th[c]);
-      }
-      int top = 0;
-      if (lane == 0) st[0] = make_int2(0, (int)live_mask);
-      top = 1;
+    for (int c = 0; c < 3; c++) {
+      double t = xi[c] - s[c];
+      th[c] = __double2float_rn(t);
+      tl[c] = __double2float_rn(t - (double)th[c]);
+    }
+    int top = 0;
+    if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+    top = live_mask ? 1 : 0;
+    __syncwarp();
+    while (top > 0) {
+      top--;
+      int2 e = st[top];
       __syncwarp();
-      while (top > 0) {
-        top--;
-        int2 e = st[top];
-        __syncwarp();
-        const int node = e.x;
-        const bool in = (((unsigned)e.y) >> lane) & 1u;
-        const WNode32 h = a.w32[node];
-        // v = t - cent  (= x_i - (cent + shift))
-        float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
-        float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
-        float v2 = (th[2] - h.ch[2]) + (tl[2] - h.cl[2]);
-        float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
-        if (h.count == 1) {
-          if (in) {
-            int j = h.jb;
-            if (j != ii && j != bi && j != fi) {
-              bool sing = false;
-              if (d2 < 1e-20f) {
-                double dist = exact_dist(xi, a.w64[node], s);
-                sing = dist < QV_DEPS;
-              }
-              if (sing) {
-                bad = true;
-              } else {
-                const WPay32 &P = a.p32[node];
-                float r2x = (P.a[0] - th[0]) + (P.b[0] - tl[0]);
-                float r2y = (P.a[1] - th[1]) + (P.b[1] - tl[1]);
-                float r2z = (P.a[2] - th[2]) + (P.b[2] - tl[2]);
-                float ox, oy, oz;
-                qv_seg32(-v0, -v1, -v2, r2x, r2y, r2z, d2, ox, oy, oz);
-                if (im < 0) k0.add(ox, oy, oz); else k1.add(ox, oy, oz);
-                ev++;
-              }
+      const int node = e.x;
+      const bool in = (((unsigned)e.y) >> lane) & 1u;
+      const WNode32 h = a.w32[node];
+      // v = t - cent  (= x_i - (cent + shift))
+      float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
+      float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
+      float v2 = (th[2] - h.ch[2]) + (tl[2] - h.cl[2]);
+      float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+      if (h.count == 1) {
+        if (in) {
+          int j = h.jb;
+          if (j != ii && j != bi && j != fi) {
+            bool sing = false;
+            if (d2 < 1e-20f) {
+              double dist = exact_dist(xi, a.w64[node], s);
+              sing = dist < QV_DEPS;
             }
-          }
-        } else {
-          bool open = false;
-          if (in) {
-            float dist = sqrtf(d2);
-            float dg = dist - h.geo;
-            float eps = 4e-6f * (dist + h.geo);
-            bool amb = false;
-            float r = dist;
-            if (a.extra) {
-              if (dg > eps) r = dg;
-              else if (dg < -eps) r = dist;
-              else amb = true;
-            }
-            if (!amb) {
-              float diff = h.width - th32 * r;
-              float tol = 4e-6f * (h.width + th32 * (dist + h.geo));
-              if (fabsf(diff) > tol) open = diff >= 0.f;
-              else amb = true;
-            }
-            if (amb) {
-              const WNode64 h64 = a.w64[node];
-              open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
-            }
-            if (!open) {
-              ev++;
-              evf++;
-              if (node != 0) {
-                const WPay32 &P = a.p32[node];
-                float rd = rsqrtf(d2);
-                float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
-                float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
-                float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
-                float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
-                float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
-                float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
-                float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
-                float wx = fmaf(v1, z2, -v2 * z1);
-                float wy = fmaf(v2, z0, -v0 * z2);
-                float wz = fmaf(v0, z1, -v1 * z0);
-                float t5 = 3.f * rd5;
-                float ox = fmaf(cx, rd3, wx * t5);
-                float oy = fmaf(cy, rd3, wy * t5);
-                float oz = fmaf(cz, rd3, wz * t5);
-                if (im < 0) k0.add(ox, oy, oz); else k1.add(ox, oy, oz);
-              }
-            }
-          }
-          unsigned om = __ballot_sync(0xffffffffu, open);
-          if (om) {
-            int nc = h.nchild;
-            if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+            if (sing) {
               bad = true;
-              nc = 0;
+            } else {
+              const WPay32 &P = a.p32[node];
+              float r2x = (P.a[0] - th[0]) + (P.b[0] - tl[0]);
+              float r2y = (P.a[1] - th[1]) + (P.b[1] - tl[1]);
+              float r2z = (P.a[2] - th[2]) + (P.b[2] - tl[2]);
+              float ox, oy, oz;
+              qv_seg32(-v0, -v1, -v2, r2x, r2y, r2z, P.C[0], P.C[1], P.C[2], d2, ox, oy, oz);
+              k0.add(ox, oy, oz);
+              ev++;
             }
-            if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
-            top += nc;
           }
-          __syncwarp();
         }
+      } else {
+        bool open = false;
+        if (in) {
+          float dist = sqrtf(d2);
+          float dg = dist - h.geo;
+          float eps = 4e-6f * (dist + h.geo);
+          bool amb = false;
+          float r = dist;
+          if (a.extra) {
+            if (dg > eps) r = dg;
+            else if (dg < -eps) r = dist;
+            else amb = true;
+          }
+          if (!amb) {
+            float diff = h.width - th32 * r;
+            float tol = 4e-6f * (h.width + th32 * (dist + h.geo));
+            if (fabsf(diff) > tol) open = diff >= 0.f;
+            else amb = true;
+          }
+          if (amb) {
+            const WNode64 h64 = a.w64[node];
+            open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+          }
+          if (!open) {
+            ev++;
+            evf++;
+            if (node != 0) {
+              const WPay32 &P = a.p32[node];
+              float rd = rsqrtf(d2);
+              float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
+              float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
+              float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
+              float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
+              float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
+              float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
+              float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
+              float wx = fmaf(v1, z2, -v2 * z1);
+              float wy = fmaf(v2, z0, -v0 * z2);
+              float wz = fmaf(v0, z1, -v1 * z0);
+              float t5 = 3.f * rd5;
+              k0.add(fmaf(cx, rd3, wx * t5), fmaf(cy, rd3, wy * t5), fmaf(cz, rd3, wz * t5));
+            }
+          }
+        }
+        unsigned om = __ballot_sync(0xffffffffu, open);
+        if (om) {
+          int nc = h.nchild;
+          if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+            bad = true;
+            nc = 0;
+          }
+          if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+          top += nc;
+        }
+        __syncwarp();
       }
     }
     if (live) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        double b0 = k0.get(c) * a.gfac, b1 = k1.get(c) * a.gfac;
-        a.u_bs[3 * i + c] = b0 + b1;
-        a.u[3 * i + c] = (a.u_li[3 * i + c] + b0) + b1;
-      }
+      double *o = a.part + ((size_t)m * a.n_act + q) * 3;
+      o[0] = k0.get(0); o[1] = k0.get(1); o[2] = k0.get(2);
     }
     for (int o = 16; o > 0; o >>= 1) {
       ev += __shfl_down_sync(0xffffffffu, ev, o);
@@ -381,19 +359,46 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
   }
 }
 
+// u_bs = s0 + sum of images, u = (u_li + s0) + images; images in the
+// reference's loop order (src/timestep.f90:276-288).
+__global__ void k_walk_reduce(int n_act, int nimg, const int *__restrict__ perm,
+                              const double *__restrict__ part, double gfac,
+                              const double *__restrict__ u_li, double *u, double *u_bs) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n_act) return;
+  int i = perm[q];
+  double s0[3], s1[3] = {0., 0., 0.};
+  for (int c = 0; c < 3; c++) s0[c] = part[(size_t)q * 3 + c] * gfac;
+  for (int m = 1; m <= nimg; m++)
+    for (int c = 0; c < 3; c++) s1[c] += part[((size_t)m * n_act + q) * 3 + c];
+  for (int c = 0; c < 3; c++) {
+    double b1 = s1[c] * gfac;
+    u_bs[3 * i + c] = s0[c] + b1;
+    u[3 * i + c] = (u_li[3 * i + c] + s0[c]) + b1;
+  }
+}
+
 int qv_launch_walk(qv_ctx *c) {
   TreeBuf &t = c->tree;
   if (!t.valid) return qv_fail(c, QV_ERR_STATE, "tree walk without a built tree");
   if (t.n_act == 0) return QV_OK;
+  int nimg = qv_img_count(c->p.boundary);
+  size_t need = sizeof(double) * 3 * (size_t)(nimg + 1) * t.n_act;
+  if (need > c->walk_part_bytes) {
+    int rc = qv_grow(c, (void **)&c->walk_part, need);
+    if (rc) return rc;
+    c->walk_part_bytes = need;
+  }
   WalkArgs a;
   a.n_act = t.n_act; a.perm = t.perm; a.x = c->x; a.inf = c->infront; a.beh = c->behind;
   a.w64 = t.w64; a.p64 = t.p64; a.w32 = t.w32; a.p32 = t.p32;
-  a.u_li = c->u_li; a.u = c->u; a.u_bs = c->u_bs;
+  a.u_li = c->u_li; a.u = c->u; a.u_bs = c->u_bs; a.part = c->walk_part;
   a.L = c->p.box_size; a.theta = c->p.tree_theta; a.gfac = c->p.quant_circ / 4. / QV_PI;
   a.extra = c->p.tree_extra_correction; a.evals = c->evals; a.evals_far = c->evals_far;
   a.status = c->dstatus;
-  int nwarps = (t.n_act + 31) / 32;
-  int nb = (nwarps + WW - 1) / WW;
+  a.ngroups = (t.n_act + 31) / 32;
+  long items = (long)a.ngroups * (nimg + 1);
+  int nb = (int)std::min<long>((items + WW - 1) / WW, 64L * c->sm_count);
   bool mixed = c->p.precision == QV_PREC_MIXED;
   switch (c->p.boundary) {
 #define QV_WALK_CASE(BCV)                                                        \
@@ -410,6 +415,9 @@ int qv_launch_walk(qv_ctx *c) {
       return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
   }
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 1);
+  k_walk_reduce<<<(t.n_act + 255) / 256, 256, 0, c->stream>>>(t.n_act, nimg, t.perm, c->walk_part,
+                                                                a.gfac, c->u_li, c->u, c->u_bs);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
   return QV_OK;
 }

@@ -84,6 +84,7 @@ _SIGS = {
     "qv_get_history": [_P, _P, _P, _P],
     "qv_set_closest": [_P, _P],
     "qv_get_points": [_P, _P, _P],
+    "qv_get_closest": [_P, _P, _P],
     "qv_device_arrays": [_P, _P, _P, _P, _P],
     "qv_ghosts": [_P],
     "qv_get_ghosts": [_P, _P, _P, _P, _P],
@@ -204,8 +205,8 @@ class Context:
         arrs = [None if u is None else _f64(u, self.n) for u in (u1, u2, u3)]
         self._check(_lib.qv_set_history(self._h, *[_ptr(a) for a in arrs]))
 
-    def get_history(self):
-        out = [np.empty((self.n, 3)) for _ in range(3)]
+    def get_history(self, *bufs):
+        out = list(bufs) if bufs else [np.empty((self.n, 3)) for _ in range(3)]
         self._check(_lib.qv_get_history(self._h, *[_ptr(a) for a in out]))
         return out
 
@@ -213,11 +214,17 @@ class Context:
         c = _i32(closest)
         self._check(_lib.qv_set_closest(self._h, _ptr(c)))
 
-    def get_points(self):
-        x = np.empty((self.n, 3))
-        u = np.empty((self.n, 3))
+    def get_points(self, x=None, u=None):
+        x = np.empty((self.n, 3)) if x is None else x
+        u = np.empty((self.n, 3)) if u is None else u
         self._check(_lib.qv_get_points(self._h, _ptr(x), _ptr(u)))
         return x, u
+
+    def get_closest(self, closest=None, closestd=None):
+        cl = np.empty(self.n, np.int32) if closest is None else closest
+        cd = np.empty(self.n) if closestd is None else closestd
+        self._check(_lib.qv_get_closest(self._h, _ptr(cl), _ptr(cd)))
+        return cl, cd
 
     def device_arrays(self):
         px, pu, pi, pb = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
