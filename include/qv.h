@@ -31,6 +31,7 @@ extern "C" {
 #define QV_ERR_NOMEM (-6)      /* device allocation failed */
 #define QV_ERR_UNSUPPORTED (-7)/* a run.in option outside this path (mirror, forcing, ...) */
 #define QV_ERR_NAN (-8)        /* NaN in positions (NAN_finder, src/general.f90:253-280) */
+#define QV_ERR_NOALLOC_LIMIT (-9) /* more slots than QV_NOALLOC_MAX_POINTS */
 
 #define QV_MAX_DEPTH 64
 
@@ -155,6 +156,26 @@ int qv_counters(qv_ctx *ctx, long long *launches, long long *leaf_evals, long lo
 /* Measured FP32 FMA throughput of the current device (TFLOP/s), the
  * denominator of the FP32-pipe roofline. */
 int qv_probe_fp32(void *stream, double *tflops);
+
+/* Non-local direct Biot-Savart velocity without any device allocation.
+ * No counterpart in the reference: it exists for hosts that cannot call
+ * cudaMalloc/cudaFree on their hot path -- drivers that reserve their whole
+ * device memory budget up front, codes embedded in a framework that owns the
+ * allocator, loops that cannot afford the device synchronisation of
+ * cudaMalloc/cudaFree.  It computes what qv_velocity returns in u_bs for
+ * velocity BS (the direct sum with the periodic images of p->boundary, in
+ * p->precision) from device pointers x (3n), infront, behind (n) into the
+ * device array u_bs (3n), on stream (NULL = legacy default stream), and
+ * returns when the result is complete.  Temporaries live in one file-scope
+ * device array sized for QV_NOALLOC_MAX_POINTS slots (about 9 MB, held by
+ * every GPU that loads the library until exit); n above that returns
+ * QV_ERR_NOALLOC_LIMIT.  The first call on a device looks up that array's
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+#define QV_NOALLOC_MAX_POINTS 16384
+int qv_velocity_direct_noalloc(const qv_params *p, int n, const double *x, const int *infront,
+                               const int *behind, double *u_bs, void *stream);
 
 #ifdef __cplusplus
 }

@@ -349,3 +349,66 @@ int qv_launch_direct(qv_ctx *c) {
   QV_CUDA(c, cudaFreeAsync(part, c->stream));
   return QV_OK;
 }
+
+// ------------------------------------------------------ caller-owned scratch
+// The same direct sum with every temporary placed in memory the caller
+// provides (no allocation): act (n ints), blk (n/256+2 ints), src64 (8n
+// doubles), src32 (16n floats), part (max_chunks * 6n doubles).  Writes only
+// u_bs (the non-local velocity, f(:)%u_s_BS of src/timestep.f90:229-240).
+__global__ void k_direct_reduce_bs(int na, int nchunk, const int *__restrict__ act,
+                                   const double *__restrict__ part, double scale, double *u_bs) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= na) return;
+  int i = act[q];
+  double s0[3] = {0., 0., 0.}, s1[3] = {0., 0., 0.};
+  for (int k = 0; k < nchunk; k++) {
+    const double *o = part + ((size_t)k * na + q) * 6;
+    for (int c = 0; c < 3; c++) { s0[c] += o[c]; s1[c] += o[3 + c]; }
+  }
+  for (int c = 0; c < 3; c++) u_bs[3 * i + c] = s0[c] * scale + s1[c] * scale;
+}
+
+int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, const double *x,
+                      const int *inf, const int *beh, const double *gi, int *act, int *blk,
+                      double *src64, float *src32, double *part, int max_chunks, double *u_bs) {
+  int nb = nblk(n, 256);
+  k_count_active<<<nb, 256, 0, s>>>(n, inf, blk);
+  k_scan_small<<<1, 1024, 0, s>>>(nb, blk, blk + nb);
+  k_scatter_active<<<nb, 256, 0, s>>>(n, inf, blk, act);
+  int na = 0;
+  if (cudaMemcpyAsync(&na, blk + nb, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return QV_ERR_CUDA;
+  if (cudaMemsetAsync(u_bs, 0, sizeof(double) * 3 * (size_t)n, s) != cudaSuccess) return QV_ERR_CUDA;
+  if (na == 0) return QV_OK;
+  int tb = nblk(na, 256);
+  bool mixed = p->precision == QV_PREC_MIXED;
+  k_pack_sources<<<tb, 256, 0, s>>>(na, act, x, gi, src64, src32);
+  int bx = nblk(na, DTILE);
+  int want = (4 * sm_count + bx - 1) / bx;
+  int maxch = max(1, na / (4 * DTILE));
+  int nchunk = max(1, min(min(want, maxch), max_chunks));
+  int chunk_len = ((nblk(na, nchunk) + DTILE - 1) / DTILE) * DTILE;
+  nchunk = nblk(na, chunk_len);
+  dim3 grid(bx, nchunk);
+  double L = p->box_size;
+  switch (p->boundary) {
+#define QV_DIRECT_SCRATCH_CASE(BCV)                                                      \
+  case BCV:                                                                              \
+    if (mixed)                                                                           \
+      k_direct32<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src32, chunk_len, L, part); \
+    else                                                                                 \
+      k_direct64<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src64, chunk_len, L, part); \
+    break;
+    QV_DIRECT_SCRATCH_CASE(QV_BC_OPEN)
+    QV_DIRECT_SCRATCH_CASE(QV_BC_PERIODIC)
+    QV_DIRECT_SCRATCH_CASE(QV_BC_OPENX)
+    QV_DIRECT_SCRATCH_CASE(QV_BC_OPENXY)
+#undef QV_DIRECT_SCRATCH_CASE
+    default:
+      return QV_ERR_UNSUPPORTED;
+  }
+  double scale = mixed ? p->quant_circ / (4. * QV_PI) : p->quant_circ / (2. * QV_PI);
+  k_direct_reduce_bs<<<tb, 256, 0, s>>>(na, nchunk, act, part, scale, u_bs);
+  return cudaGetLastError() == cudaSuccess ? QV_OK : QV_ERR_CUDA;
+}

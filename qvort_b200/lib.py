@@ -28,6 +28,8 @@ QV_ERR_STATE = -5
 QV_ERR_NOMEM = -6
 QV_ERR_UNSUPPORTED = -7
 QV_ERR_NAN = -8
+QV_ERR_NOALLOC_LIMIT = -9
+QV_NOALLOC_MAX_POINTS = 16384
 QV_MAX_DEPTH = 64
 
 BC = {"open": 0, "periodic": 1, "openx": 2, "openxy": 3}
@@ -104,6 +106,7 @@ _SIGS = {
     "qv_counters": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                     C.POINTER(C.c_longlong)],
     "qv_probe_fp32": [_P, _D],
+    "qv_velocity_direct_noalloc": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, _P],
 }
 for _name, _args in _SIGS.items():
     _f = getattr(_lib, _name)
