@@ -63,9 +63,11 @@ def dist_env():
 
 
 class Clocks:
-    """nvidia-smi clock/throttle sampler for the timed region."""
+    """nvidia-smi clock/throttle sampler.  It is started before the warm-up
+    (its start-up must not land in the timed region) and only the samples
+    stamped inside the timed window are kept."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -83,18 +85,29 @@ class Clocks:
         except Exception:
             self.p = None
 
-    def stop(self) -> dict:
+    def stop(self, t0: float, t1: float) -> dict:
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
         self.p.terminate()
         self.p.wait(timeout=5)
         self.f.flush()
-        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        import datetime as _dt
+
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            r = [x.strip() for x in line.split(",")]
+            try:
+                ts = _dt.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except (ValueError, IndexError):
+                continue
+            rows.append((ts, r))
+        inside = [r for ts, r in rows if t0 - 0.25 <= ts <= t1 + 0.25]
+        if not inside:  # window shorter than the sampling period: nearest samples
+            inside = [r for ts, r in sorted(rows, key=lambda z: abs(z[0] - (t0 + t1) / 2))[:2]]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
+        for r in inside:
             try:
                 sm.append(float(r[1]))
                 mx = float(r[2])
@@ -216,6 +229,8 @@ def our_arm(args):
     ctx.set_points(w.x, w.infront, w.behind)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
+    clocks = Clocks(local)
+    clocks.start()
     itime = 0
     for _ in range(max(3, args.warmup)):
         itime += 1
@@ -224,10 +239,9 @@ def our_arm(args):
     if ws > 1:
         torch.distributed.barrier()
     launches0 = ctx.counters()["launches"]
-    clocks = Clocks(local)
-    clocks.start()
     evs = []
     torch.cuda.synchronize()
+    t_wall0 = time.time()
     for k in range(args.steps):
         with torch.cuda.stream(stream):
             flush.fill_(k & 0xFF)       # L2 flush between timed steps (outside the events)
@@ -239,7 +253,7 @@ def our_arm(args):
             e1.record(stream)
         evs.append((e0, e1))
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop(t_wall0, time.time())
     launches = ctx.counters()["launches"] - launches0
     ms_total = sum(a.elapsed_time(b) for a, b in evs)
     if ws > 1:

@@ -14,27 +14,35 @@
 #include "qv_internal.cuh"
 
 #define CW 4
-#define CSTK (7 * QV_MAX_DEPTH + 16)
 
 __device__ __forceinline__ double dist_exact(const double *a, double b0, double b1, double b2) {
   double d0 = __dsub_rn(a[0], b0), d1 = __dsub_rn(a[1], b1), d2 = __dsub_rn(a[2], b2);
   return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
 }
 
-// Every comparison is first taken in FP32 from (hi, lo) float pairs of the
-// FP64 coordinates; only when it falls within a relative 1e-5 of its
-// threshold (or a distance must be stored) is the FP64 expression of the
-// reference evaluated, so the outcome is always the FP64 outcome.
+// Every comparison is first taken in FP32 on squared distances from (hi, lo)
+// float pairs of the FP64 coordinates; only when it falls within a relative
+// 4e-6 of its threshold (or a distance must be stored) is the FP64 expression
+// of the reference evaluated, so the outcome is always the FP64 outcome.
+// Children's headers are fetched when they are pushed (stack entries carry
+// them), so popping a node costs a shared-memory read.
+struct __align__(16) CStkEnt {
+  WNode32 h;
+  int node;
+  unsigned mask;
+  int pad[2];
+};
+
 __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *__restrict__ x,
                                                          const int *__restrict__ inf,
                                                          const int *__restrict__ beh,
                                                          const WNode64 *__restrict__ w64,
                                                          const WNode32 *__restrict__ w32,
-                                                         int *closest, double *closestd,
-                                                         int *status) {
-  __shared__ int2 stk[CW][CSTK];
+                                                         int stk_cap, int *closest,
+                                                         double *closestd, int *status) {
+  extern __shared__ CStkEnt cstk[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int2 *st = stk[wid];
+  CStkEnt *st = cstk + wid * stk_cap;
   const int nwarps = (n + 31) / 32;
   for (int w = blockIdx.x * CW + wid; w < nwarps; w += gridDim.x * CW) {
     int i = w * 32 + lane;
@@ -42,7 +50,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
     double xi[3] = {0., 0., 0.};
     int ii = i + 1, fi = -1, bi = -1, cl = 0;
     double cd = 100.;
-    float cd32 = 100.f;
+    float cd2 = 1e4f;
     float xh[3] = {0.f, 0.f, 0.f}, xl[3] = {0.f, 0.f, 0.f};
     if (live) {
       xi[0] = x[3 * i]; xi[1] = x[3 * i + 1]; xi[2] = x[3 * i + 2];
@@ -56,31 +64,34 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
     bool bad = false;
     int top = 0;
-    if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+    if (lane == 0) {
+      st[0].h = w32[0];
+      st[0].node = 0;
+      st[0].mask = live_mask;
+    }
     top = live_mask ? 1 : 0;
     __syncwarp();
     while (top > 0) {
       top--;
-      int2 e = st[top];
+      const WNode32 h = st[top].h;
+      const int node = st[top].node;
+      const bool in = (st[top].mask >> lane) & 1u;
       __syncwarp();
-      const int node = e.x;
-      const bool in = (((unsigned)e.y) >> lane) & 1u;
-      const WNode32 h = w32[node];
       bool open = false;
       if (in && h.count > 0) {
         float v0 = (xh[0] - h.ch[0]) + (xl[0] - h.cl[0]);
         float v1 = (xh[1] - h.ch[1]) + (xl[1] - h.cl[1]);
         float v2 = (xh[2] - h.ch[2]) + (xl[2] - h.cl[2]);
-        float d32 = sqrtf(fmaf(v0, v0, fmaf(v1, v1, v2 * v2)));
-        bool tiny = d32 < 1e-10f;
+        float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+        bool tiny = d2 < 1e-20f;
         double d64 = -1.;  // exact distance, computed on demand
         bool pass;
         if (h.count == 1) {
           pass = true;
         } else {
-          // theta = width/dist < 0.5  (src/tree.f90:248-249)
-          float diff = 0.5f * d32 - h.width;
-          if (!tiny && fabsf(diff) > 1e-5f * h.width) {
+          // theta = width/dist < 0.5  (src/tree.f90:248-249)  <=>  dist^2 > (2 width)^2
+          float diff = d2 - h.w4;
+          if (!tiny && fabsf(diff) > 4e-6f * h.w4) {
             pass = diff > 0.f;
           } else {
             const WNode64 hh = w64[node];
@@ -91,8 +102,8 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
         if (pass) {
           // dist < closestd
           bool closer;
-          float dc = d32 - cd32;
-          if (!tiny && fabsf(dc) > 1e-5f * cd32 && d64 < 0.) {
+          float dc = d2 - cd2;
+          if (!tiny && d64 < 0. && fabsf(dc) > 4e-6f * cd2) {
             closer = dc < 0.f;
           } else {
             if (d64 < 0.) {
@@ -111,7 +122,8 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
                 if (d64 < 0.) d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
                 cl = j;
                 cd = d64;
-                cd32 = __double2float_rn(cd);
+                float c32 = __double2float_rn(cd);
+                cd2 = c32 * c32;
               }
             }
           }
@@ -122,11 +134,17 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
       unsigned om = __ballot_sync(0xffffffffu, open);
       if (om) {
         int nc = h.nchild;
-        if (top + nc > CSTK) {
+        if (top + nc > stk_cap) {  // unreachable: the cap follows the tree depth
           bad = true;
           nc = 0;
         }
-        if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+        if (lane < nc) {
+          int ch = h.child_first + nc - 1 - lane;
+          CStkEnt &E = st[top + lane];
+          E.h = w32[ch];
+          E.node = ch;
+          E.mask = om;
+        }
         top += nc;
       }
       __syncwarp();
@@ -189,9 +207,18 @@ int qv_launch_closest(qv_ctx *c) {
   if (c->p.tree_theta > 0) {
     if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
     int nwarps = (c->n + 31) / 32;
-    k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, 0, c->stream>>>(
-        c->n, c->x, c->infront, c->behind, c->tree.w64, c->tree.w32, c->closest, c->closestd,
-        c->dstatus);
+    int cap = 7 * (c->tree.depth + 1) + 8;
+    size_t smem = sizeof(CStkEnt) * cap * CW;
+    if (smem > 48 * 1024) {
+      static size_t opted = 0;
+      if (smem > opted) {
+        cudaFuncSetAttribute(k_closest_tree, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        opted = smem;
+      }
+    }
+    k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, smem, c->stream>>>(
+        c->n, c->x, c->infront, c->behind, c->tree.w64, c->tree.w32, cap, c->closest,
+        c->closestd, c->dstatus);
   } else {
     k_pclose<<<(c->n + PT - 1) / PT, PT, 0, c->stream>>>(c->n, c->x, c->infront, c->behind,
                                                          c->closest, c->closestd);

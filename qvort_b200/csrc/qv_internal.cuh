@@ -40,10 +40,13 @@ struct __align__(16) WPay64 {
 };
 
 // FP32 header (48 B): cent as a two-float (hi, lo) split of the FP64 value so
-// that target-source differences keep FP64-level information.
+// that target-source differences keep FP64-level information, and the two
+// opening radii squared: rc2 for the velocity walk and w4 for the candidate
+// search (see k_pack_nodes).
 struct __align__(16) WNode32 {
   float ch[3], cl[3];
-  float width, geo;
+  float rc2;  // (geo + width/theta)^2, or -1 when only the FP64 test is valid
+  float w4;   // (2 width)^2: theta = width/dist < 0.5 <=> dist^2 > w4
   int count, child_first, nchild, jb;
 };
 

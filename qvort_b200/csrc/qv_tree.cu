@@ -38,13 +38,12 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 // control block layout
 #define CTL_NNODES 0
-#define CTL_NSPLIT 1
-#define CTL_NSPLIT_NEXT 2
 #define CTL_OVERFLOW 3  // 1 = node capacity, 2 = level capacity
 #define CTL_DEPTH 4
 #define CTL_NBIG 5      // number of nodes handled by k_moments_big
 #define CTL_LVL 8       // lvl_start[0..QV_MAX_DEPTH+2]
-#define CTL_SIZE (CTL_LVL + QV_MAX_DEPTH + 4)
+#define CTL_NS (CTL_LVL + QV_MAX_DEPTH + 4)  // splitting nodes per level
+#define CTL_SIZE (CTL_NS + QV_MAX_DEPTH + 4)
 
 struct BuildArgs {
   int n_act, n_slots, cap_pts, cap_nodes, cap_levels, nchunks;
@@ -125,7 +124,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
   volatile int *ctl = a.ctl;
   int d = 0;
   for (;;) {
-    int nsplit = ctl[CTL_NSPLIT];
+    int nsplit = ctl[CTL_NS + d];
     if (nsplit == 0) break;
     if (d + 1 >= a.cap_levels || d + 1 > QV_MAX_DEPTH) {
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_OVERFLOW] = 2;
@@ -189,7 +188,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
         ctl[CTL_OVERFLOW] = 1;
         continue;
       }
-      if (nsp) atomicAdd((int *)&ctl[CTL_NSPLIT_NEXT], nsp);
+      if (nsp) atomicAdd((int *)&ctl[CTL_NS + d + 1], nsp);
       a.child_first[k] = base;
       a.nchild[k] = nc;
       a.cmask[k] = (unsigned char)mask;
@@ -306,11 +305,6 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
       }
     }
     for (int q = blockIdx.x * BT + threadIdx.x; q < (le2 - le) * 9; q += gridDim.x * BT) cntn[q] = 0;
-    grid.sync();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      ctl[CTL_NSPLIT] = ctl[CTL_NSPLIT_NEXT];
-      ctl[CTL_NSPLIT_NEXT] = 0;
-    }
     d++;
     grid.sync();
   }
@@ -519,7 +513,8 @@ __global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict_
                              const int *__restrict__ nchild, const int *__restrict__ first,
                              const double *__restrict__ x, const double *__restrict__ gi,
                              const int *__restrict__ inf, const int *__restrict__ beh,
-                             WNode64 *w64, WPay64 *p64, WNode32 *w32, WPay32 *p32) {
+                             double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
+                             WPay32 *p32) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_nodes) return;
   WNode64 h;
@@ -546,8 +541,21 @@ __global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict_
   split2(h.cx, h32.ch[0], h32.cl[0]);
   split2(h.cy, h32.ch[1], h32.cl[1]);
   split2(h.cz, h32.ch[2], h32.cl[2]);
-  h32.width = __double2float_rn(h.width);
-  h32.geo = __double2float_rn(h.geo);
+  // Opening test of src/tree.f90:354-365,394: theta = w/(d - geo) < tree_theta
+  // (extra correction) or w/d < tree_theta.  For d > geo it is d > geo + w/theta.
+  // The centroid lies in its cell, so geo <= (sqrt 3 / 2) w, and d <= geo then
+  // gives w/d >= 2/sqrt 3: the cell opens whenever theta < 2/sqrt 3.  Under that
+  // condition the test is d^2 > rc2 exactly; the walk compares in FP32 with a
+  // margin and falls back to the FP64 expression near the threshold.  The root
+  // (centroid anywhere, zero moments) always takes the FP64 path.
+  bool fast = theta > 0. && (!extra || theta < 1.15);
+  if (k == 0 || !fast) {
+    h32.rc2 = -1.f;
+  } else {
+    double rc = (extra ? h.geo : 0.) + h.width / theta;
+    h32.rc2 = __double2float_rn(rc * rc);
+  }
+  h32.w4 = __double2float_rn(4. * h.width * h.width);
   h32.count = cnt;
   h32.child_first = h.child_first;
   h32.nchild = h.nchild;
@@ -678,6 +686,15 @@ int qv_launch_tree_build(qv_ctx *c) {
     if ((rc = qv_launch_ghosts(c))) return rc;
   if ((rc = qv_compact_active(c))) return rc;
   int na = c->n_act;
+  // the root centroid chain needs only the active list: start it now on a side
+  // stream so that it overlaps the level-synchronous build
+  if ((rc = qv_aux_streams(c))) return rc;
+  QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+  QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
+  k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(na, c->act, c->x, c->dscalar);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
   int cap_nodes = std::max(t.cap_nodes, 4 * na + 64);
   int cap_levels = std::max(t.cap_levels, std::min(QV_MAX_DEPTH + 1, 40));
   for (int attempt = 0; attempt < 8; attempt++) {
@@ -692,7 +709,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaMemsetAsync(t.cnt9, 0, sizeof(int) * 9 * (size_t)(2 * t.cap_pts + 2), c->stream));
     int h[CTL_SIZE] = {0};
     h[CTL_NNODES] = 1;
-    h[CTL_NSPLIT] = (c->n > 1 && na > 0) ? 1 : 0;
+    h[CTL_NS + 0] = (c->n > 1 && na > 0) ? 1 : 0;
     h[CTL_LVL + 0] = 0;
     h[CTL_LVL + 1] = 1;
     QV_CUDA(c, cudaMemcpyAsync(t.ctl, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
@@ -725,14 +742,9 @@ int qv_launch_tree_build(qv_ctx *c) {
     t.n_act = na;
     t.lvl_start.assign(h + CTL_LVL, h + CTL_LVL + t.depth + 2);
     t.perm = t.ord + (size_t)t.depth * t.cap_pts;
-    // moments of all non-root nodes and the root centroid, on three streams
-    if ((rc = qv_aux_streams(c))) return rc;
+    // moments of all non-root nodes on two streams (big nodes get a block each)
     QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
     QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
-    QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
-    k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(na, c->act, c->x, t.cent);
-    QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 1);
     if (t.n_nodes > 1) {
       QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
       k_list_big<<<std::max(1, std::min(nblk(t.n_nodes, 256), 4 * c->sm_count)), 256, 0,
@@ -748,12 +760,14 @@ int qv_launch_tree_build(qv_ctx *c) {
       QV_COUNT(c, 3);
     }
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
-    QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
+    QV_CUDA(c, cudaMemcpyAsync(t.cent, c->dscalar, 3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
     k_pack_nodes<<<nblk(t.n_nodes, 128), 128, 0, c->stream>>>(
         t.n_nodes, c->n, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first, t.nchild,
-        t.first, c->x, c->gi, c->infront, c->behind, t.w64, t.p64, t.w32, t.p32);
+        t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta, c->p.tree_extra_correction,
+        t.w64, t.p64, t.w32, t.p32);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 2);
     t.valid = true;

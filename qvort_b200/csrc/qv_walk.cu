@@ -2,11 +2,12 @@
 // (tree_walk, src/tree.f90:336-421; image loop src/timestep.f90:276-307).
 //
 // Execution model: a warp task is (32 targets adjacent in the tree's
-// depth-first point order, one periodic image); a target's 27 image walks are
-// independent, so splitting them across warps gives the GPU 27x more warps to
-// hide latency with.  Each task writes per-target partial sums; a second
-// kernel adds them in the reference's image order (main image, then images
-// peri,perj,perk = -1..1), so results do not depend on scheduling.  The
+// depth-first point order, one periodic image, and for the unshifted image one
+// of the root's children); these walks are independent, so the split gives
+// the GPU enough warps to hide latency with and keeps the longest task short.
+// Each task writes per-target partial sums; a second kernel adds them in the
+// reference's order (main image by root child, then images peri,perj,perk =
+// -1..1), so results do not depend on scheduling.  The
 // warp keeps one explicit stack of (node, lane mask) in shared memory: at each
 // node every lane in the mask takes its own decision exactly as the reference
 // does (leaf -> exact segment, theta < tree_theta -> far-field multipole,
@@ -28,7 +29,8 @@
 #include "qv_internal.cuh"
 
 #define WW 4                           // warps per block
-#define STK (7 * QV_MAX_DEPTH + 16)    // stack entries per warp
+#define STK (7 * QV_MAX_DEPTH + 16)    // stack entries per warp (FP64 walk)
+#define NSPLIT 8                       // tasks per target group for the main image
 
 struct WalkArgs {
   int n_act;
@@ -41,9 +43,9 @@ struct WalkArgs {
   const WPay32 *p32;
   const double *u_li;
   double *u, *u_bs;
-  double *part;  // (NIMG+1) x n_act x 3 partial sums, image-major
+  double *part;  // (NSPLIT+NIMG) x n_act x 3 partial sums, slot-major
   double L, theta, gfac;
-  int extra, ngroups;
+  int extra, ngroups, stk_cap;
   unsigned long long *evals, *evals_far;
   int *status;
 };
@@ -98,6 +100,12 @@ struct Kahan3w {
   __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
 };
 
+// Task slot s: s < NSPLIT -> unshifted image, root child s; else image s-NSPLIT.
+__device__ __forceinline__ void slot_image(int bc, int s, int &ma, int &mb, int &mc) {
+  ma = mb = mc = 0;
+  if (s >= NSPLIT) qv_img_shift(bc, s - NSPLIT, &ma, &mb, &mc);
+}
+
 // ---------------------------------------------------------------- FP64 walk
 template <int BC>
 __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
@@ -105,9 +113,9 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
   __shared__ int2 stk[WW][STK];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int2 *st = stk[wid];
-  const int items = a.ngroups * (NIMG + 1);
+  const int items = a.ngroups * (NSPLIT + NIMG);
   for (int item = blockIdx.x * WW + wid; item < items; item += gridDim.x * WW) {
-    const int m = item / a.ngroups, g = item - m * a.ngroups;
+    const int sl = item / a.ngroups, g = item - sl * a.ngroups;
     int q = g * 32 + lane;
     bool live = q < a.n_act;
     int i = live ? a.perm[q] : 0;
@@ -117,16 +125,37 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
       xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
       bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
     }
-    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
     double acc[3] = {0., 0., 0.};
     unsigned long long ev = 0, evf = 0;
     bool bad = false;
-    int ma = 0, mb = 0, mc = 0;
-    if (m > 0) qv_img_shift(BC, m - 1, &ma, &mb, &mc);
+    int ma, mb, mc;
+    slot_image(BC, sl, ma, mb, mc);
     const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
     int top = 0;
-    if (lane == 0) st[0] = make_int2(0, (int)live_mask);
-    top = live_mask ? 1 : 0;
+    if (sl >= NSPLIT) {
+      const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+      if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+      top = live_mask ? 1 : 0;
+    } else {
+      // unshifted image: the root's own decision, then only root child sl
+      const WNode64 r = a.w64[0];
+      bool ropen = false;
+      if (r.count == 1) {
+        const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+        if (sl == 0 && lane == 0) st[0] = make_int2(0, (int)live_mask);
+        top = (sl == 0 && live_mask) ? 1 : 0;
+      } else {
+        if (live) {
+          ropen = exact_open(exact_dist(xi, r, s), r, a.theta, a.extra);
+          if (!ropen && sl == 0) { ev++; evf++; }  // root far field: zero moments
+        }
+        const unsigned om = __ballot_sync(0xffffffffu, ropen);
+        if (om && sl < r.nchild) {
+          if (lane == 0) st[0] = make_int2(r.child_first + sl, (int)om);
+          top = 1;
+        }
+      }
+    }
     __syncwarp();
     while (top > 0) {
       top--;
@@ -200,7 +229,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
       }
     }
     if (live) {
-      double *o = a.part + ((size_t)m * a.n_act + q) * 3;
+      double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
       o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2];
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -214,16 +243,24 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
 }
 
 // ---------------------------------------------------------------- mixed walk
+// Stack entry: the child's FP32 header, fetched when the child is pushed so
+// that popping it costs a shared-memory read instead of a dependent global load.
+struct __align__(16) StkEnt {
+  WNode32 h;
+  int node;
+  unsigned mask;
+  int pad[2];
+};
+
 template <int BC>
 __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
-  __shared__ int2 stk[WW][STK];
+  extern __shared__ StkEnt stk_dyn[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int2 *st = stk[wid];
-  const float th32 = (float)a.theta;
-  const int items = a.ngroups * (NIMG + 1);
+  StkEnt *st = stk_dyn + wid * a.stk_cap;
+  const int items = a.ngroups * (NSPLIT + NIMG);
   for (int item = blockIdx.x * WW + wid; item < items; item += gridDim.x * WW) {
-    const int m = item / a.ngroups, g = item - m * a.ngroups;
+    const int sl = item / a.ngroups, g = item - sl * a.ngroups;
     int q = g * 32 + lane;
     bool live = q < a.n_act;
     int i = live ? a.perm[q] : 0;
@@ -233,13 +270,12 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
       xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
       bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
     }
-    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
     Kahan3w k0;
     k0.zero();
     unsigned long long ev = 0, evf = 0;
     bool bad = false;
-    int ma = 0, mb = 0, mc = 0;
-    if (m > 0) qv_img_shift(BC, m - 1, &ma, &mb, &mc);
+    int ma, mb, mc;
+    slot_image(BC, sl, ma, mb, mc);
     const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
     // target recentred for this image, t = x_i - shift as (hi, lo) floats
     float th[3], tl[3];
@@ -250,16 +286,49 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
       tl[c] = __double2float_rn(t - (double)th[c]);
     }
     int top = 0;
-    if (lane == 0) st[0] = make_int2(0, (int)live_mask);
-    top = live_mask ? 1 : 0;
+    if (sl >= NSPLIT) {
+      const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+      if (lane == 0) {
+        st[0].h = a.w32[0];
+        st[0].node = 0;
+        st[0].mask = live_mask;
+      }
+      top = live_mask ? 1 : 0;
+    } else {
+      // unshifted image: the root's own decision, then only root child sl
+      const WNode64 r = a.w64[0];
+      bool ropen = false;
+      if (r.count == 1) {
+        const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+        if (sl == 0 && lane == 0) {
+          st[0].h = a.w32[0];
+          st[0].node = 0;
+          st[0].mask = live_mask;
+        }
+        top = (sl == 0 && live_mask) ? 1 : 0;
+      } else {
+        if (live) {
+          ropen = exact_open(exact_dist(xi, r, s), r, a.theta, a.extra);
+          if (!ropen && sl == 0) { ev++; evf++; }  // root far field: zero moments
+        }
+        const unsigned om = __ballot_sync(0xffffffffu, ropen);
+        if (om && sl < r.nchild) {
+          if (lane == 0) {
+            st[0].h = a.w32[r.child_first + sl];
+            st[0].node = r.child_first + sl;
+            st[0].mask = om;
+          }
+          top = 1;
+        }
+      }
+    }
     __syncwarp();
     while (top > 0) {
       top--;
-      int2 e = st[top];
+      const WNode32 h = st[top].h;
+      const int node = st[top].node;
+      const bool in = (st[top].mask >> lane) & 1u;
       __syncwarp();
-      const int node = e.x;
-      const bool in = (((unsigned)e.y) >> lane) & 1u;
-      const WNode32 h = a.w32[node];
       // v = t - cent  (= x_i - (cent + shift))
       float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
       float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
@@ -291,23 +360,12 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
       } else {
         bool open = false;
         if (in) {
-          float dist = sqrtf(d2);
-          float dg = dist - h.geo;
-          float eps = 4e-6f * (dist + h.geo);
-          bool amb = false;
-          float r = dist;
-          if (a.extra) {
-            if (dg > eps) r = dg;
-            else if (dg < -eps) r = dist;
-            else amb = true;
-          }
-          if (!amb) {
-            float diff = h.width - th32 * r;
-            float tol = 4e-6f * (h.width + th32 * (dist + h.geo));
-            if (fabsf(diff) > tol) open = diff >= 0.f;
-            else amb = true;
-          }
-          if (amb) {
+          // accept (far field) iff d^2 > rc2, decided in FP32 outside a
+          // relative margin of 4e-6 and by the reference's FP64 test inside it
+          float diff = d2 - h.rc2;
+          if (h.rc2 > 0.f && fabsf(diff) > 4e-6f * h.rc2) {
+            open = diff <= 0.f;
+          } else {
             const WNode64 h64 = a.w64[node];
             open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
           }
@@ -335,18 +393,24 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
         unsigned om = __ballot_sync(0xffffffffu, open);
         if (om) {
           int nc = h.nchild;
-          if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+          if (top + nc > a.stk_cap) {  // unreachable: the cap follows the tree depth
             bad = true;
             nc = 0;
           }
-          if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+          if (lane < nc) {
+            int ch = h.child_first + nc - 1 - lane;
+            StkEnt &E = st[top + lane];
+            E.h = a.w32[ch];
+            E.node = ch;
+            E.mask = om;
+          }
           top += nc;
         }
         __syncwarp();
       }
     }
     if (live) {
-      double *o = a.part + ((size_t)m * a.n_act + q) * 3;
+      double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
       o[0] = k0.get(0); o[1] = k0.get(1); o[2] = k0.get(2);
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -359,22 +423,24 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
   }
 }
 
-// u_bs = s0 + sum of images, u = (u_li + s0) + images; images in the
-// reference's loop order (src/timestep.f90:276-288).
+// u_bs = main + images, u = (u_li + main) + images, with the main image summed
+// over the root's children in child order and the images in the reference's
+// loop order (src/timestep.f90:276-288).
 __global__ void k_walk_reduce(int n_act, int nimg, const int *__restrict__ perm,
                               const double *__restrict__ part, double gfac,
                               const double *__restrict__ u_li, double *u, double *u_bs) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_act) return;
   int i = perm[q];
-  double s0[3], s1[3] = {0., 0., 0.};
-  for (int c = 0; c < 3; c++) s0[c] = part[(size_t)q * 3 + c] * gfac;
-  for (int m = 1; m <= nimg; m++)
+  double s0[3] = {0., 0., 0.}, s1[3] = {0., 0., 0.};
+  for (int m = 0; m < NSPLIT; m++)
+    for (int c = 0; c < 3; c++) s0[c] += part[((size_t)m * n_act + q) * 3 + c];
+  for (int m = NSPLIT; m < NSPLIT + nimg; m++)
     for (int c = 0; c < 3; c++) s1[c] += part[((size_t)m * n_act + q) * 3 + c];
   for (int c = 0; c < 3; c++) {
-    double b1 = s1[c] * gfac;
-    u_bs[3 * i + c] = s0[c] + b1;
-    u[3 * i + c] = (u_li[3 * i + c] + s0[c]) + b1;
+    double b0 = s0[c] * gfac, b1 = s1[c] * gfac;
+    u_bs[3 * i + c] = b0 + b1;
+    u[3 * i + c] = (u_li[3 * i + c] + b0) + b1;
   }
 }
 
@@ -383,7 +449,7 @@ int qv_launch_walk(qv_ctx *c) {
   if (!t.valid) return qv_fail(c, QV_ERR_STATE, "tree walk without a built tree");
   if (t.n_act == 0) return QV_OK;
   int nimg = qv_img_count(c->p.boundary);
-  size_t need = sizeof(double) * 3 * (size_t)(nimg + 1) * t.n_act;
+  size_t need = sizeof(double) * 3 * (size_t)(NSPLIT + nimg) * t.n_act;
   if (need > c->walk_part_bytes) {
     int rc = qv_grow(c, (void **)&c->walk_part, need);
     if (rc) return rc;
@@ -397,13 +463,27 @@ int qv_launch_walk(qv_ctx *c) {
   a.extra = c->p.tree_extra_correction; a.evals = c->evals; a.evals_far = c->evals_far;
   a.status = c->dstatus;
   a.ngroups = (t.n_act + 31) / 32;
-  long items = (long)a.ngroups * (nimg + 1);
+  // a depth-first stack over a tree of depth D never holds more than 7 D + 1
+  // entries (each open pushes at most 8 and pops 1)
+  a.stk_cap = 7 * (t.depth + 1) + 8;
+  size_t smem = sizeof(StkEnt) * a.stk_cap * WW;
+  long items = (long)a.ngroups * (NSPLIT + nimg);
   int nb = (int)std::min<long>((items + WW - 1) / WW, 64L * c->sm_count);
   bool mixed = c->p.precision == QV_PREC_MIXED;
+  if (mixed && smem > 48 * 1024) {
+    static size_t opted = 0;
+    if (smem > opted) {
+      cudaFuncSetAttribute(k_walk32<QV_BC_OPEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_walk32<QV_BC_PERIODIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_walk32<QV_BC_OPENX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k_walk32<QV_BC_OPENXY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      opted = smem;
+    }
+  }
   switch (c->p.boundary) {
 #define QV_WALK_CASE(BCV)                                                        \
   case BCV:                                                                      \
-    if (mixed) k_walk32<BCV><<<nb, WW * 32, 0, c->stream>>>(a);                  \
+    if (mixed) k_walk32<BCV><<<nb, WW * 32, smem, c->stream>>>(a);               \
     else k_walk64<BCV><<<nb, WW * 32, 0, c->stream>>>(a);                        \
     break;
     QV_WALK_CASE(QV_BC_OPEN)
