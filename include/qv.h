@@ -140,6 +140,28 @@ int qv_energy(qv_ctx *ctx, double *energy);
  * itime % recon_shots == 0, ghostp, boundary wrap.  Device-resident. */
 int qv_step(qv_ctx *ctx, int itime);
 
+/* ---------------------------------------------------------------- host side
+ * The parts of the reference's driver that feed this path, for a host that
+ * runs without the Fortran code (qvort_run) or a test. */
+typedef struct qv_run {
+  qv_params p;          /* the path's parameters (gpu_precision selects FP64/mixed) */
+  int nsteps, shots, pcount, readin_var_file, switch_off_recon;
+  char initf[32];
+} qv_run;
+/* read_run_file (src/cdata.f90:420-807) for the keys of this path; unknown
+ * labels are ignored and a value that fails to read ends the file, as there. */
+int qv_read_run_file(const char *path, qv_run *out);
+/* read_var_file (src/initial.f90:463-496): t, pcount, x, y, z, infront;
+ * behind reconstructed as there.  With x == NULL only *n and *t are set. */
+int qv_read_var_file(const char *path, int cap, int *n, double *t, double *x, int *infront,
+                     int *behind);
+/* printf (src/output.f90:116-143): the var%04d.log stream snapshot. */
+int qv_write_var_file(const char *path, int n, double t, const double *x, const int *infront,
+                      const double *u);
+/* setup_single_loop / setup_leap_frog (src/initial_loop.f90:11-38, 206-245). */
+int qv_setup_loops(const char *initf, int pcount, double delta, double *x, int *infront,
+                   int *behind);
+
 /* Block until the context's stream is idle. */
 int qv_sync(qv_ctx *ctx);
 
@@ -147,7 +169,9 @@ int qv_sync(qv_ctx *ctx);
  * src/run.f90:31-166, and eval_counter, src/tree.f90:40).  With profiling on,
  * the phases below are bracketed by CUDA events on the context's stream and
  * their device times accumulate into ms[QV_NPHASES]. */
-#define QV_NPHASES 7 /* ghosts, tree build, local term, non-local sum, update, search, wrap */
+/* ghosts, tree build, local term, non-local sum, update, search, wrap, and two
+ * parts of the tree build: the level-synchronous construction and the moments */
+#define QV_NPHASES 9
 int qv_profile(qv_ctx *ctx, int enable);
 int qv_phase_times(qv_ctx *ctx, double *ms, int reset);
 /* Kernel launches issued by this context so far, and the leaf / far-field

@@ -39,11 +39,29 @@ FILE_FLAGS = {"qv_points.cu": ["--fmad=false"]}
 
 
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+
+
+RUNNER_SRC = HERE / "host" / "qvort_run.cpp"
+RUNNER = HERE / "qvort_run"
+
+
+def build_runner() -> Path:
+    """The C++ driver executable, linked against the library (rpath = its folder)."""
+    if RUNNER.exists() and RUNNER.stat().st_mtime >= max(RUNNER_SRC.stat().st_mtime,
+                                                        OUT.stat().st_mtime):
+        return RUNNER
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-I", str(HERE.parent / "include"), str(RUNNER_SRC),
+           "-L", str(HERE), "-lqvort_b200", "-Wl,-rpath,$ORIGIN", "-o", str(RUNNER)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"qvort_run build failed:\n{r.stdout}\n{r.stderr}")
+    return RUNNER
 
 
 def _compile(src: Path, verbose: bool) -> Path:
-    obj = BUILD / (src.stem + ".o")
+    obj = BUILD / (src.name.replace(".", "_") + ".o")
     deps = [src] + sorted(CSRC.glob("*.cuh")) + [HERE.parent / "include" / "qv.h"]
     if obj.exists() and obj.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return obj
@@ -80,6 +98,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, OUT)
     stamp.write_text(flags)
+    build_runner()
     return OUT
 
 

@@ -82,7 +82,8 @@ extern "C" int qv_create(const qv_params *p, void *stream, qv_ctx **out) {
   if (cudaMalloc(&c->evals, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->evals_far, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&c->dstatus, sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c->dscalar, 16 * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&c->dscalar, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_nact, 4 * sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     delete c;
     return QV_ERR_NOMEM;
@@ -92,6 +93,8 @@ extern "C" int qv_create(const qv_params *p, void *stream, qv_ctx **out) {
 }
 
 static void free_tree(TreeBuf &t) {
+  if (t.h_ctl) cudaFreeHost(t.h_ctl);
+  if (t.ev_ctl) cudaEventDestroy(t.ev_ctl);
   void *ps[] = {t.pos, t.width, t.cent, t.circ, t.C, t.count, t.start, t.parent, t.child_first,
                 t.nchild, t.first, t.level, t.digit, t.cmask, t.w64, t.p64, t.w32, t.p32,
                 t.ord, t.nodeA, t.nodeB, t.dig, t.rnk, t.cnt9, t.rs9, t.chunk9, t.ctl};
@@ -103,9 +106,12 @@ static void free_tree(TreeBuf &t) {
 static void free_points(qv_ctx *c) {
   void *ps[] = {c->x, c->u, c->u1, c->u2, c->u3, c->gi, c->gb, c->gii, c->gbb, c->u_li,
                 c->u_bs, c->closestd, c->infront, c->behind, c->closest, c->act, c->src64,
-                c->src32};
+                c->src32, c->blkcnt, c->dpart};
   for (void *q : ps)
     if (q) cudaFree(q);
+  c->blkcnt = nullptr;
+  c->dpart = nullptr;
+  c->dpart_bytes = 0;
   c->x = c->u = c->u1 = c->u2 = c->u3 = c->gi = c->gb = c->gii = c->gbb = c->u_li = c->u_bs =
       c->closestd = nullptr;
   c->infront = c->behind = c->closest = c->act = nullptr;
@@ -127,6 +133,7 @@ extern "C" int qv_destroy(qv_ctx *c) {
   }
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->dscalar) cudaFree(c->dscalar);
+  if (c->d_nact) cudaFree(c->d_nact);
   if (c->walk_part) cudaFree(c->walk_part);
   for (int k = 0; k < 2; k++) {
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -165,6 +172,7 @@ static int reserve_points(qv_ctx *c, int n) {
   if ((rc = qv_grow(c, (void **)&c->act, sizeof(int) * n))) return rc;
   if ((rc = qv_grow(c, (void **)&c->src64, sizeof(double) * 8 * (size_t)n))) return rc;
   if ((rc = qv_grow(c, (void **)&c->src32, sizeof(float) * 16 * (size_t)n))) return rc;
+  if ((rc = qv_grow(c, (void **)&c->blkcnt, sizeof(int) * ((size_t)n / 256 + 4)))) return rc;
   c->cap = n;
   return QV_OK;
 }
@@ -349,13 +357,10 @@ extern "C" int qv_tree_export(qv_ctx *c, int cap, int *parent, int *digit, int *
   return m;
 }
 
-static long long count_active_host(qv_ctx *c) {
-  return c->n_act;
-}
-
-extern "C" int qv_velocity(qv_ctx *c, double *u, double *u_li, double *u_bs, long long *eval_count) {
-  QV_CHECK_CTX(c);
-  if (c->n == 0) return QV_OK;
+// Launch the local term and the non-local sum (calc_velocity for every active
+// point).  The tree path issues no host synchronisation here; the counters
+// and the status word are read by velocity_collect.
+static int velocity_launch(qv_ctx *c) {
   int rc;
   if (!c->ghosts_valid)
     if ((rc = qv_launch_ghosts(c))) return rc;
@@ -365,14 +370,11 @@ extern "C" int qv_velocity(qv_ctx *c, double *u, double *u_li, double *u_bs, lon
   qv_phase_begin(c, PH_LIA);
   if ((rc = qv_launch_lia(c))) return rc;
   qv_phase_end(c, PH_LIA);
-  long long ev = 0;
   if (c->p.velocity == QV_VEL_BS) {
     if ((rc = qv_compact_active(c))) return rc;
     qv_phase_begin(c, PH_NONLOCAL);
     if ((rc = qv_launch_direct(c))) return rc;
     qv_phase_end(c, PH_NONLOCAL);
-    long long na = count_active_host(c);
-    ev = na * na * (1 + qv_img_count(c->p.boundary));
   } else if (c->p.velocity == QV_VEL_TREE) {
     if (!c->tree.valid) {
       qv_phase_begin(c, PH_BUILD);
@@ -384,32 +386,49 @@ extern "C" int qv_velocity(qv_ctx *c, double *u, double *u_li, double *u_bs, lon
     qv_phase_end(c, PH_NONLOCAL);
   } else if (c->p.velocity == QV_VEL_LIA) {
     if ((rc = qv_compact_active(c))) return rc;
-    ev = c->n_act;
   }
-  size_t v = sizeof(double) * 3 * (size_t)c->n;
-  if (u) QV_CUDA(c, cudaMemcpyAsync(u, c->u, v, cudaMemcpyDeviceToHost, c->stream));
-  if (u_li) QV_CUDA(c, cudaMemcpyAsync(u_li, c->u_li, v, cudaMemcpyDeviceToHost, c->stream));
-  if (u_bs) QV_CUDA(c, cudaMemcpyAsync(u_bs, c->u_bs, v, cudaMemcpyDeviceToHost, c->stream));
+  return QV_OK;
+}
+
+// Wait for the stream, read the evaluation counters and the status word.
+static int velocity_collect(qv_ctx *c, long long *eval_count) {
   unsigned long long dev_ev = 0, dev_far = 0;
   int st = 0;
   QV_CUDA(c, cudaMemcpyAsync(&dev_ev, c->evals, sizeof(dev_ev), cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaMemcpyAsync(&dev_far, c->evals_far, sizeof(dev_far), cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaMemcpyAsync(&st, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  long long ev = 0;
   if (c->p.velocity == QV_VEL_TREE) {
     ev = 2LL * c->tree.n_act + (long long)dev_ev;
     c->last_far = (long long)dev_far;
     c->last_leaf = (long long)(dev_ev - dev_far);
   } else if (c->p.velocity == QV_VEL_BS) {
+    long long na = c->n_act;
+    ev = na * na * (1 + qv_img_count(c->p.boundary));
     c->last_far = 0;
     c->last_leaf = ev;
+  } else if (c->p.velocity == QV_VEL_LIA) {
+    ev = c->n_act;
   }
   if (eval_count) *eval_count = ev;
   if (st & 1)
     return qv_fail(c, QV_ERR_SINGULAR, "singularity in BS (tree) velocity field - this is normally "
                    "caused by having recon_shots too large");
-  if (st & 2) return qv_fail(c, QV_ERR_TREE_DEPTH, "walk stack overflow");
+  if (st & 2) return qv_fail(c, QV_ERR_TREE_DEPTH, "walk or search stack overflow");
   return QV_OK;
+}
+
+extern "C" int qv_velocity(qv_ctx *c, double *u, double *u_li, double *u_bs, long long *eval_count) {
+  QV_CHECK_CTX(c);
+  if (c->n == 0) return QV_OK;
+  int rc = velocity_launch(c);
+  if (rc) return rc;
+  size_t v = sizeof(double) * 3 * (size_t)c->n;
+  if (u) QV_CUDA(c, cudaMemcpyAsync(u, c->u, v, cudaMemcpyDeviceToHost, c->stream));
+  if (u_li) QV_CUDA(c, cudaMemcpyAsync(u_li, c->u_li, v, cudaMemcpyDeviceToHost, c->stream));
+  if (u_bs) QV_CUDA(c, cudaMemcpyAsync(u_bs, c->u_bs, v, cudaMemcpyDeviceToHost, c->stream));
+  return velocity_collect(c, eval_count);
 }
 
 extern "C" int qv_step_ab(qv_ctx *c) {
@@ -421,13 +440,7 @@ extern "C" int qv_step_ab(qv_ctx *c) {
   return QV_OK;
 }
 
-// velocity evaluation on the current state without host copies
-static int velocity_device(qv_ctx *c) {
-  return qv_velocity(c, nullptr, nullptr, nullptr, nullptr);
-}
-
-extern "C" int qv_step_rk3(qv_ctx *c) {
-  QV_CHECK_CTX(c);
+static int rk3_stages(qv_ctx *c) {
   int rc;
   for (int stage = 0; stage < 3; stage++) {
     if (stage > 0) {
@@ -435,12 +448,20 @@ extern "C" int qv_step_rk3(qv_ctx *c) {
       if (c->p.tree_theta > 0)
         if ((rc = qv_launch_tree_build(c))) return rc;
     }
-    if ((rc = velocity_device(c))) return rc;
+    if ((rc = velocity_launch(c))) return rc;
+    if ((rc = velocity_collect(c, nullptr))) return rc;
     qv_phase_begin(c, PH_UPDATE);
     if ((rc = qv_launch_rk3_stage(c, stage))) return rc;
     qv_phase_end(c, PH_UPDATE);
     c->ghosts_valid = false;
   }
+  return QV_OK;
+}
+
+extern "C" int qv_step_rk3(qv_ctx *c) {
+  QV_CHECK_CTX(c);
+  int rc = rk3_stages(c);
+  if (rc) return rc;
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
   return QV_OK;
 }
@@ -491,16 +512,15 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
     qv_phase_end(c, PH_BUILD);
   }
   if (c->p.runge_kutta) {                                        // run.f90:50-54
-    if ((rc = qv_step_rk3(c))) return rc;
+    if ((rc = rk3_stages(c))) return rc;
   } else {
-    if ((rc = velocity_device(c))) return rc;
+    if ((rc = velocity_launch(c))) return rc;
     qv_phase_begin(c, PH_UPDATE);
     if ((rc = qv_launch_ab(c))) return rc;
     qv_phase_end(c, PH_UPDATE);
     c->ghosts_valid = false;
   }
   if (itime % c->p.recon_shots == 0) {                           // run.f90:63-69
-    QV_CUDA(c, cudaMemsetAsync(c->dstatus, 0, sizeof(int), c->stream));
     qv_phase_begin(c, PH_CLOSEST);
     if ((rc = qv_launch_closest(c))) return rc;
     qv_phase_end(c, PH_CLOSEST);
@@ -510,8 +530,7 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
   if ((rc = qv_launch_wrap(c))) return rc;                       // run.f90:82-93
   qv_phase_end(c, PH_WRAP);
   c->ghosts_valid = false;
-  QV_CUDA(c, cudaStreamSynchronize(c->stream));
-  return QV_OK;
+  return velocity_collect(c, nullptr);  // one wait per step; reports any status
 }
 
 extern "C" int qv_sync(qv_ctx *c) {
@@ -521,22 +540,39 @@ extern "C" int qv_sync(qv_ctx *c) {
 }
 
 // ------------------------------------------------------------ instrumentation
+static void phase_collect_one(qv_ctx *c, int ph) {
+  if (!c->ev_pending[ph]) return;
+  cudaEventSynchronize(c->ev_end[ph]);
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, c->ev_beg[ph], c->ev_end[ph]) == cudaSuccess) c->phase_ms[ph] += ms;
+  cudaGetLastError();
+  c->ev_pending[ph] = false;
+}
+
 void qv_phase_begin(qv_ctx *c, int ph) {
   if (!c->profile) return;
   if (!c->ev_beg[ph]) {
     cudaEventCreate(&c->ev_beg[ph]);
     cudaEventCreate(&c->ev_end[ph]);
   }
+  phase_collect_one(c, ph);
   cudaEventRecord(c->ev_beg[ph], c->stream);
 }
 
-void qv_phase_end(qv_ctx *c, int ph) {
+// Record the end of a phase without waiting for it (collected later).
+void qv_phase_end_async(qv_ctx *c, int ph) {
   if (!c->profile || !c->ev_beg[ph]) return;
   cudaEventRecord(c->ev_end[ph], c->stream);
-  cudaEventSynchronize(c->ev_end[ph]);
-  float ms = 0.f;
-  if (cudaEventElapsedTime(&ms, c->ev_beg[ph], c->ev_end[ph]) == cudaSuccess) c->phase_ms[ph] += ms;
-  cudaGetLastError();
+  c->ev_pending[ph] = true;
+}
+
+void qv_phase_end(qv_ctx *c, int ph) {
+  qv_phase_end_async(c, ph);
+  phase_collect_one(c, ph);
+}
+
+void qv_phase_collect(qv_ctx *c) {
+  for (int k = 0; k < PH_N; k++) phase_collect_one(c, k);
 }
 
 extern "C" int qv_profile(qv_ctx *c, int enable) {
@@ -547,6 +583,7 @@ extern "C" int qv_profile(qv_ctx *c, int enable) {
 
 extern "C" int qv_phase_times(qv_ctx *c, double *ms, int reset) {
   QV_CHECK_CTX(c);
+  qv_phase_collect(c);
   for (int k = 0; k < PH_N; k++) {
     if (ms) ms[k] = c->phase_ms[k];
     if (reset) c->phase_ms[k] = 0.;

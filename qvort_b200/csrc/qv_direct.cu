@@ -81,16 +81,26 @@ __global__ void k_scatter_active(int n, const int *__restrict__ inf, const int *
 // Stable compaction of the active slots (ascending index) into c->act.
 int qv_compact_active(qv_ctx *c) {
   int nb = nblk(c->n, 256);
-  int *tmp = nullptr;
-  QV_CUDA(c, cudaMallocAsync((void **)&tmp, sizeof(int) * (nb + 1), c->stream));
+  int *tmp = c->blkcnt;
   k_count_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp);
   k_scan_small<<<1, 1024, 0, c->stream>>>(nb, tmp, tmp + nb);
   k_scatter_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp, c->act);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 3);
   QV_CUDA(c, cudaMemcpyAsync(&c->n_act, tmp + nb, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  QV_CUDA(c, cudaFreeAsync(tmp, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+// The same compaction without waiting for it: the count goes to c->d_nact.
+int qv_compact_active_async(qv_ctx *c) {
+  int nb = nblk(c->n, 256);
+  int *tmp = c->blkcnt;
+  k_count_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp);
+  k_scan_small<<<1, 1024, 0, c->stream>>>(nb, tmp, c->d_nact);
+  k_scatter_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp, c->act);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 3);
   return QV_OK;
 }
 
@@ -316,8 +326,13 @@ int qv_launch_direct(qv_ctx *c) {
   int nchunk = max(1, min(want, maxch));
   int chunk_len = ((nblk(na, nchunk) + DTILE - 1) / DTILE) * DTILE;
   nchunk = nblk(na, chunk_len);
-  double *part = nullptr;
-  QV_CUDA(c, cudaMallocAsync((void **)&part, sizeof(double) * 6 * (size_t)na * nchunk, c->stream));
+  size_t need = sizeof(double) * 6 * (size_t)na * nchunk;
+  if (need > c->dpart_bytes) {
+    int rc = qv_grow(c, (void **)&c->dpart, need);
+    if (rc) return rc;
+    c->dpart_bytes = need;
+  }
+  double *part = c->dpart;
   dim3 grid(bx, nchunk);
   double L = c->p.box_size;
   bool mixed = c->p.precision == QV_PREC_MIXED;
@@ -337,7 +352,6 @@ int qv_launch_direct(qv_ctx *c) {
     QV_DIRECT_CASE(QV_BC_OPENXY)
 #undef QV_DIRECT_CASE
     default:
-      cudaFreeAsync(part, c->stream);
       return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
   }
   QV_LAUNCH_CHECK(c);
@@ -346,7 +360,6 @@ int qv_launch_direct(qv_ctx *c) {
                                              c->u_bs);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 2);
-  QV_CUDA(c, cudaFreeAsync(part, c->stream));
   return QV_OK;
 }
 

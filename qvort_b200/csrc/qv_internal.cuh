@@ -84,11 +84,18 @@ struct TreeBuf {
   int *chunk9 = nullptr;                   // per chunk of positions
   int *ctl = nullptr;                      // device control block
   int *perm = nullptr;                     // final (DFS) order of active points
+  int *h_ctl = nullptr;                    // pinned copy of the control block
+  cudaEvent_t ev_ctl = nullptr;
   std::vector<int> lvl_start;
 };
 
 // Phases timed with CUDA events when profiling is on (qv_profile).
-enum { PH_GHOSTS = 0, PH_BUILD, PH_LIA, PH_NONLOCAL, PH_UPDATE, PH_CLOSEST, PH_WRAP, PH_N };
+enum {
+  PH_GHOSTS = 0, PH_BUILD, PH_LIA, PH_NONLOCAL, PH_UPDATE, PH_CLOSEST, PH_WRAP,
+  PH_BUILD_LEVELS,   // inside PH_BUILD: init + the level-synchronous kernel
+  PH_BUILD_MOMENTS,  // inside PH_BUILD: moment chains, root centroid join, packs
+  PH_N
+};
 
 struct qv_ctx {
   qv_params p;
@@ -101,6 +108,10 @@ struct qv_ctx {
   int *infront = nullptr, *behind = nullptr, *closest = nullptr;
   int *act = nullptr;  // compacted active slots (direct sums)
   int n_act = 0;
+  int *d_nact = nullptr;  // device copy of n_act (tree path)
+  int *blkcnt = nullptr;  // per-256-slot block counts of the compaction (n/256+2)
+  double *dpart = nullptr;  // direct-sum partial sums, grown on demand
+  size_t dpart_bytes = 0;
   double *src64 = nullptr;  // direct-sum source pack (FP64)
   float *src32 = nullptr;   // direct-sum source pack (FP32 hi/lo)
   unsigned long long *evals = nullptr;  // device eval counter
@@ -114,7 +125,7 @@ struct qv_ctx {
   // instrumentation
   bool profile = false;
   cudaEvent_t ev_beg[PH_N] = {}, ev_end[PH_N] = {};
-  bool ev_open[PH_N] = {};
+  bool ev_pending[PH_N] = {};
   double phase_ms[PH_N] = {};
   long long launches = 0;
   unsigned long long *evals_far = nullptr;
@@ -138,6 +149,7 @@ int qv_fail(qv_ctx *c, int code, const char *fmt, ...);
 int qv_grow(qv_ctx *c, void **ptr, size_t bytes);
 void qv_phase_begin(qv_ctx *c, int ph);
 void qv_phase_end(qv_ctx *c, int ph);
+void qv_phase_end_async(qv_ctx *c, int ph);
 void qv_phase_collect(qv_ctx *c);
 #define QV_COUNT(c, k) ((c)->launches += (k))
 
@@ -153,6 +165,7 @@ int qv_launch_wrap(qv_ctx *c);
 int qv_launch_closest(qv_ctx *c);
 int qv_launch_energy(qv_ctx *c, double *out_host);
 int qv_compact_active(qv_ctx *c);
+int qv_compact_active_async(qv_ctx *c);
 int qv_aux_streams(qv_ctx *c);
 
 // ---------------------------------------------------------------- helpers

@@ -347,15 +347,15 @@ __global__ void k_energy_final(int nb, const double *blk, double *out, double qu
 
 int qv_launch_energy(qv_ctx *c, double *out_host) {
   int nb = nblk(c->n, 256);
-  double *blk = nullptr;
-  QV_CUDA(c, cudaMallocAsync((void **)&blk, sizeof(double) * (nb + 1), c->stream));
+  double *blk = nullptr;  // energy is a diagnostic, off the step path
+  QV_CUDA(c, cudaMalloc((void **)&blk, sizeof(double) * (nb + 1)));
   k_energy_terms<<<nb, 256, 0, c->stream>>>(c->n, c->x, c->u, c->infront, c->gi, c->gb, c->gii,
                                             c->gbb, c->p.deriv_order, blk);
   k_energy_final<<<1, 256, 0, c->stream>>>(nb, blk, blk + nb, c->p.quant_circ);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 2);
   QV_CUDA(c, cudaMemcpyAsync(out_host, blk + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  QV_CUDA(c, cudaFreeAsync(blk, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  QV_CUDA(c, cudaFree(blk));
   return QV_OK;
 }

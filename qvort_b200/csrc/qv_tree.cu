@@ -41,12 +41,14 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 #define CTL_OVERFLOW 3  // 1 = node capacity, 2 = level capacity
 #define CTL_DEPTH 4
 #define CTL_NBIG 5      // number of nodes handled by k_moments_big
+#define CTL_NACT 6      // active points of this build
 #define CTL_LVL 8       // lvl_start[0..QV_MAX_DEPTH+2]
 #define CTL_NS (CTL_LVL + QV_MAX_DEPTH + 4)  // splitting nodes per level
 #define CTL_SIZE (CTL_NS + QV_MAX_DEPTH + 4)
 
 struct BuildArgs {
-  int n_act, n_slots, cap_pts, cap_nodes, cap_levels, nchunks;
+  const int *d_nact;  // active points (device-resident count of the compaction)
+  int n_slots, cap_pts, cap_nodes, cap_levels, nchunks;
   const double *x, *gi;
   double *pos, *width;
   int *count, *start, *parent, *child_first, *nchild, *level;
@@ -122,10 +124,12 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
   __shared__ Pack2 sh[BT / 32 + 1];
   __shared__ int s9[BT / 32][9];
   volatile int *ctl = a.ctl;
+  const int n_act = *a.d_nact;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_NACT] = n_act;
   int d = 0;
   for (;;) {
     int nsplit = ctl[CTL_NS + d];
-    if (nsplit == 0) break;
+    if (nsplit == 0 || n_act == 0) break;
     if (d + 1 >= a.cap_levels || d + 1 > QV_MAX_DEPTH) {
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_OVERFLOW] = 2;
       break;
@@ -145,7 +149,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
       for (int j = 0; j < PPT; j++) {
         int p = ch * CH + threadIdx.x * PPT + j;
         int g = NOD, key = -1;
-        if (p < a.n_act) {
+        if (p < n_act) {
           int k = nodc[p];
           if (k >= 0 && a.count[k] >= 2) {
             int s = ordc[p];
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
 #pragma unroll
       for (int j = 0; j < PPT; j++) {
         int p = ch * CH + threadIdx.x * PPT + j;
-        gs[j] = p < a.n_act ? a.dig[p] : NOD;
+        gs[j] = p < n_act ? a.dig[p] : NOD;
         if (gs[j] != NOD) { Pack2 o = pk_one(gs[j]); loc.lo += o.lo; loc.hi += o.hi; }
       }
       Pack2 tot;
@@ -290,7 +294,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
 
     // ---- P4: scatter into the next level's order; reset counters
     const int le2 = ctl[CTL_LVL + d + 2];
-    for (int p = blockIdx.x * BT + threadIdx.x; p < a.n_act; p += gridDim.x * BT) {
+    for (int p = blockIdx.x * BT + threadIdx.x; p < n_act; p += gridDim.x * BT) {
       int g = a.dig[p];
       if (g == NOD) {
         ordn[p] = ordc[p];
@@ -321,7 +325,8 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
 #define MC 256    // points per shared-memory chunk in the block kernel
 
 // One warp per node with at most BIGN points.
-__global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__restrict__ level,
+__global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl, int cap_nodes,
+                                                     const int *__restrict__ level,
                                                      const int *__restrict__ start,
                                                      const int *__restrict__ count,
                                                      const int *__restrict__ ord, int cap_pts,
@@ -330,6 +335,8 @@ __global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__r
                                                      double *circ, double *C, int *first) {
   __shared__ double buf[MW][32][15];
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (ctl[CTL_OVERFLOW]) return;
+  const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   for (int k = 1 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
     int s = start[k], n = count[k];
     if (n > BIGN) continue;
@@ -374,7 +381,10 @@ __global__ void __launch_bounds__(MW * 32) k_moments(int n_nodes, const int *__r
 }
 
 // List the nodes with more than BIGN points (order irrelevant).
-__global__ void k_list_big(int n_nodes, const int *__restrict__ count, int *list, int *nlist) {
+__global__ void k_list_big(const int *__restrict__ ctl, int cap_nodes,
+                           const int *__restrict__ count, int *list, int *nlist) {
+  if (ctl[CTL_OVERFLOW]) return;
+  const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   for (int k = 1 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
     if (count[k] > BIGN) list[atomicAdd(nlist, 1)] = k;
 }
@@ -461,10 +471,12 @@ __global__ void __launch_bounds__(256) k_moments_big(const int *__restrict__ lis
 // Warps 1.. stage chunks of positions in shared memory (double buffered);
 // lanes 0..2 of warp 0 run the three chains.
 #define RC 2048
-__global__ void __launch_bounds__(512) k_root_cent(int n_act, const int *__restrict__ act,
+__global__ void __launch_bounds__(512) k_root_cent(const int *__restrict__ d_nact,
+                                                   const int *__restrict__ act,
                                                    const double *__restrict__ x, double *cent) {
   extern __shared__ double rb[];  // [2][RC][3]
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int n_act = *d_nact;
   const int nch = (n_act + RC - 1) / RC;
   auto produce = [&](int ch, double *dst) {
     int base = ch * RC, m = min(RC, n_act - base);
@@ -506,7 +518,18 @@ __device__ __forceinline__ void split2(double v, float &h, float &l) {
   l = __double2float_rn(v - (double)h);
 }
 
-__global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict__ pos,
+__device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
+                          const double *__restrict__ width, const double *__restrict__ cent,
+                          const double *__restrict__ circ, const double *__restrict__ C,
+                          const int *__restrict__ count, const int *__restrict__ child_first,
+                          const int *__restrict__ nchild, const int *__restrict__ first,
+                          const double *__restrict__ x, const double *__restrict__ gi,
+                          const int *__restrict__ inf, const int *__restrict__ beh,
+                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
+                          WPay32 *p32);
+
+__global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int n_slots,
+                             const double *__restrict__ pos,
                              const double *__restrict__ width, const double *__restrict__ cent,
                              const double *__restrict__ circ, const double *__restrict__ C,
                              const int *__restrict__ count, const int *__restrict__ child_first,
@@ -515,8 +538,22 @@ __global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict_
                              const int *__restrict__ inf, const int *__restrict__ beh,
                              double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
                              WPay32 *p32) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_nodes) return;
+  if (ctl[CTL_OVERFLOW]) return;
+  const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
+    pack_node(k, n_slots, pos, width, cent, circ, C, count, child_first, nchild, first, x, gi, inf,
+              beh, theta, extra, w64, p64, w32, p32);
+}
+
+__device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
+                          const double *__restrict__ width, const double *__restrict__ cent,
+                          const double *__restrict__ circ, const double *__restrict__ C,
+                          const int *__restrict__ count, const int *__restrict__ child_first,
+                          const int *__restrict__ nchild, const int *__restrict__ first,
+                          const double *__restrict__ x, const double *__restrict__ gi,
+                          const int *__restrict__ inf, const int *__restrict__ beh,
+                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
+                          WPay32 *p32) {
   WNode64 h;
   h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
   h.width = width[k];
@@ -590,20 +627,42 @@ __global__ void k_pack_nodes(int n_nodes, int n_slots, const double *__restrict_
   p32[k] = r;
 }
 
-__global__ void k_root_record(double *pos, double *width, int *count, int *start, int *parent,
-                              int *child_first, int *nchild, int *level, unsigned char *digit,
-                              unsigned char *cmask, int *first, double L, int n_slots) {
-  pos[0] = -L / 2.; pos[1] = -L / 2.; pos[2] = -L / 2.;
-  width[0] = L;
-  count[0] = n_slots;
-  start[0] = 0;
-  parent[0] = -1;
-  child_first[0] = -1;
-  nchild[0] = 0;
-  level[0] = 0;
-  digit[0] = 0xFF;
-  cmask[0] = 0;
-  first[0] = n_slots > 0 ? 0 : -1;
+// Everything a build starts from, in one launch: the root record
+// (src/tree.f90:49-58: corner -L/2, width L, pcount = all slots, parray(1) =
+// slot 1), the control block, the level-0 order (the active slots in
+// ascending order), node ids of level 0 and zeroed digit counters.
+__global__ void k_build_init(double *pos, double *width, int *count, int *start, int *parent,
+                             int *child_first, int *nchild, int *level, unsigned char *digit,
+                             unsigned char *cmask, int *first, double L, int n_slots, int *ctl,
+                             int *ord, const int *__restrict__ act, int *nodeA, int *cnt9,
+                             size_t ncnt9) {
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  if (tid == 0) {
+    pos[0] = -L / 2.; pos[1] = -L / 2.; pos[2] = -L / 2.;
+    width[0] = L;
+    count[0] = n_slots;
+    start[0] = 0;
+    parent[0] = -1;
+    child_first[0] = -1;
+    nchild[0] = 0;
+    level[0] = 0;
+    digit[0] = 0xFF;
+    cmask[0] = 0;
+    first[0] = n_slots > 0 ? 0 : -1;
+  }
+  for (size_t q = tid; q < CTL_SIZE; q += stride) {
+    int v = 0;
+    if (q == CTL_NNODES) v = 1;
+    else if (q == CTL_NS) v = n_slots > 1 ? 1 : 0;
+    else if (q == CTL_LVL + 1) v = 1;
+    ctl[q] = v;
+  }
+  for (size_t q = tid; q < (size_t)n_slots; q += stride) {
+    ord[q] = act[q];
+    nodeA[q] = 0;
+  }
+  for (size_t q = tid; q < ncnt9; q += stride) cnt9[q] = 0;
 }
 
 // --------------------------------------------------------------- host side
@@ -684,38 +743,37 @@ int qv_launch_tree_build(qv_ctx *c) {
   int rc;
   if (!c->ghosts_valid)
     if ((rc = qv_launch_ghosts(c))) return rc;
-  if ((rc = qv_compact_active(c))) return rc;
-  int na = c->n_act;
+  // The active count stays on the device (c->d_nact); every launch below is
+  // sized by the slot count n, so the host does not wait for the compaction.
+  if ((rc = qv_compact_active_async(c))) return rc;
+  const int n = c->n;
   // the root centroid chain needs only the active list: start it now on a side
   // stream so that it overlaps the level-synchronous build
   if ((rc = qv_aux_streams(c))) return rc;
   QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
   QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
-  k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(na, c->act, c->x, c->dscalar);
+  k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(c->d_nact, c->act, c->x,
+                                                                   c->dscalar);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
   QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
-  int cap_nodes = std::max(t.cap_nodes, 4 * na + 64);
+  if (!t.h_ctl) {
+    QV_CUDA(c, cudaMallocHost((void **)&t.h_ctl, sizeof(int) * CTL_SIZE));
+    QV_CUDA(c, cudaEventCreateWithFlags(&t.ev_ctl, cudaEventDisableTiming));
+  }
+  int cap_nodes = std::max(t.cap_nodes, 4 * n + 64);
   int cap_levels = std::max(t.cap_levels, std::min(QV_MAX_DEPTH + 1, 40));
   for (int attempt = 0; attempt < 8; attempt++) {
-    if ((rc = tree_reserve(c, na, cap_nodes, cap_levels))) return rc;
-    k_root_record<<<1, 1, 0, c->stream>>>(t.pos, t.width, t.count, t.start, t.parent,
-                                          t.child_first, t.nchild, t.level, t.digit, t.cmask,
-                                          t.first, c->p.box_size, c->n);
+    if ((rc = tree_reserve(c, n, cap_nodes, cap_levels))) return rc;
+    qv_phase_begin(c, PH_BUILD_LEVELS);
+    k_build_init<<<2 * c->sm_count, 256, 0, c->stream>>>(
+        t.pos, t.width, t.count, t.start, t.parent, t.child_first, t.nchild, t.level, t.digit,
+        t.cmask, t.first, c->p.box_size, n, t.ctl, t.ord, c->act, t.nodeA, t.cnt9,
+        9 * (size_t)(2 * t.cap_pts + 2));
     QV_LAUNCH_CHECK(c);
-    if (na > 0)
-      QV_CUDA(c, cudaMemcpyAsync(t.ord, c->act, sizeof(int) * na, cudaMemcpyDeviceToDevice, c->stream));
-    QV_CUDA(c, cudaMemsetAsync(t.nodeA, 0, sizeof(int) * std::max(na, 1), c->stream));
-    QV_CUDA(c, cudaMemsetAsync(t.cnt9, 0, sizeof(int) * 9 * (size_t)(2 * t.cap_pts + 2), c->stream));
-    int h[CTL_SIZE] = {0};
-    h[CTL_NNODES] = 1;
-    h[CTL_NS + 0] = (c->n > 1 && na > 0) ? 1 : 0;
-    h[CTL_LVL + 0] = 0;
-    h[CTL_LVL + 1] = 1;
-    QV_CUDA(c, cudaMemcpyAsync(t.ctl, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
     BuildArgs a;
-    a.n_act = na; a.n_slots = c->n; a.cap_pts = t.cap_pts; a.cap_nodes = t.cap_nodes;
-    a.cap_levels = t.cap_levels; a.nchunks = std::max(1, nblk(na, CH));
+    a.d_nact = c->d_nact; a.n_slots = n; a.cap_pts = t.cap_pts; a.cap_nodes = t.cap_nodes;
+    a.cap_levels = t.cap_levels; a.nchunks = std::max(1, nblk(n, CH));
     a.x = c->x; a.gi = c->gi; a.pos = t.pos; a.width = t.width; a.count = t.count;
     a.start = t.start; a.parent = t.parent; a.child_first = t.child_first; a.nchild = t.nchild;
     a.level = t.level; a.digit = t.digit; a.cmask = t.cmask; a.ord = t.ord; a.nodeA = t.nodeA;
@@ -726,10 +784,48 @@ int qv_launch_tree_build(qv_ctx *c) {
     void *args[] = {&a};
     QV_CUDA(c, cudaLaunchCooperativeKernel((void *)k_build, grid, BT, args, 0, c->stream));
     QV_COUNT(c, 2);
-    QV_CUDA(c, cudaMemcpyAsync(h, t.ctl, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-    QV_CUDA(c, cudaStreamSynchronize(c->stream));
-    if (h[CTL_OVERFLOW] == 1) { cap_nodes *= 2; continue; }
-    if (h[CTL_OVERFLOW] == 2) {
+    qv_phase_end_async(c, PH_BUILD_LEVELS);
+    // control block to the host, read once the moment kernels are queued
+    QV_CUDA(c, cudaMemcpyAsync(t.h_ctl, t.ctl, sizeof(int) * CTL_SIZE, cudaMemcpyDeviceToHost,
+                               c->stream));
+    QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->stream));
+    qv_phase_begin(c, PH_BUILD_MOMENTS);
+    // moments of all non-root nodes on two streams (big nodes get a block each);
+    // node counts and the overflow flag are read on the device
+    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
+    QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
+    k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, t.count, t.rnk,
+                                                        t.ctl + CTL_NBIG);
+    k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
+        t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
+        t.cent, t.circ, t.C, t.first);
+    k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, t.level, t.start,
+                                                           t.count, t.ord, t.cap_pts, c->x, c->gi,
+                                                           t.cent, t.circ, t.C, t.first);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 3);
+    QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
+    QV_CUDA(c, cudaMemcpyAsync(t.cent, c->dscalar, 3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
+    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
+        t.ctl, t.cap_nodes, n, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
+        t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
+        c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.p32);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 2);
+    qv_phase_end_async(c, PH_BUILD_MOMENTS);
+    QV_CUDA(c, cudaEventSynchronize(t.ev_ctl));
+    const int *hc = t.h_ctl;
+    if (hc[CTL_OVERFLOW]) {
+      // the queued moment/pack kernels saw the flag and did nothing
+      QV_CUDA(c, cudaStreamSynchronize(c->stream));
+      if (hc[CTL_OVERFLOW] == 1) {
+        cap_nodes *= 2;
+        continue;
+      }
       if (cap_levels >= QV_MAX_DEPTH + 1)
         return qv_fail(c, QV_ERR_TREE_DEPTH,
                        "octree deeper than %d levels (coincident or nearly coincident points)",
@@ -737,39 +833,12 @@ int qv_launch_tree_build(qv_ctx *c) {
       cap_levels = QV_MAX_DEPTH + 1;
       continue;
     }
-    t.n_nodes = h[CTL_NNODES];
-    t.depth = h[CTL_DEPTH];
-    t.n_act = na;
-    t.lvl_start.assign(h + CTL_LVL, h + CTL_LVL + t.depth + 2);
+    t.n_nodes = hc[CTL_NNODES];
+    t.depth = hc[CTL_DEPTH];
+    t.n_act = hc[CTL_NACT];
+    c->n_act = t.n_act;
+    t.lvl_start.assign(hc + CTL_LVL, hc + CTL_LVL + t.depth + 2);
     t.perm = t.ord + (size_t)t.depth * t.cap_pts;
-    // moments of all non-root nodes on two streams (big nodes get a block each)
-    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
-    QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
-    if (t.n_nodes > 1) {
-      QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
-      k_list_big<<<std::max(1, std::min(nblk(t.n_nodes, 256), 4 * c->sm_count)), 256, 0,
-                   c->aux[0]>>>(t.n_nodes, t.count, t.rnk, t.ctl + CTL_NBIG);
-      k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
-          t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
-          t.cent, t.circ, t.C, t.first);
-      int nb = std::min(nblk(t.n_nodes - 1, MW), 16 * c->sm_count);
-      k_moments<<<nb, MW * 32, 0, c->stream>>>(t.n_nodes, t.level, t.start, t.count, t.ord,
-                                               t.cap_pts, c->x, c->gi, t.cent, t.circ, t.C,
-                                               t.first);
-      QV_LAUNCH_CHECK(c);
-      QV_COUNT(c, 3);
-    }
-    QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
-    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
-    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
-    QV_CUDA(c, cudaMemcpyAsync(t.cent, c->dscalar, 3 * sizeof(double), cudaMemcpyDeviceToDevice,
-                               c->stream));
-    k_pack_nodes<<<nblk(t.n_nodes, 128), 128, 0, c->stream>>>(
-        t.n_nodes, c->n, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first, t.nchild,
-        t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta, c->p.tree_extra_correction,
-        t.w64, t.p64, t.w32, t.p32);
-    QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 2);
     t.valid = true;
     return QV_OK;
   }

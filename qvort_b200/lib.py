@@ -56,6 +56,18 @@ class QvParams(C.Structure):
     ]
 
 
+class QvRun(C.Structure):
+    _fields_ = [
+        ("p", QvParams),
+        ("nsteps", C.c_int),
+        ("shots", C.c_int),
+        ("pcount", C.c_int),
+        ("readin_var_file", C.c_int),
+        ("switch_off_recon", C.c_int),
+        ("initf", C.c_char * 32),
+    ]
+
+
 class QvError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"qv error {code}: {msg}")
@@ -107,6 +119,10 @@ _SIGS = {
                     C.POINTER(C.c_longlong)],
     "qv_probe_fp32": [_P, _D],
     "qv_velocity_direct_noalloc": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, _P],
+    "qv_read_run_file": [C.c_char_p, C.POINTER(QvRun)],
+    "qv_read_var_file": [C.c_char_p, C.c_int, _I, _D, _P, _P, _P],
+    "qv_write_var_file": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
+    "qv_setup_loops": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
 }
 for _name, _args in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -304,7 +320,8 @@ class Context:
         self._check(_lib.qv_sync(self._h))
 
     # ---- instrumentation
-    PHASES = ("ghosts", "build", "local", "nonlocal", "update", "search", "wrap")
+    PHASES = ("ghosts", "build", "local", "nonlocal", "update", "search", "wrap",
+              "build_levels", "build_moments")
 
     def profile(self, enable: bool = True):
         self._check(_lib.qv_profile(self._h, int(enable)))
@@ -318,6 +335,48 @@ class Context:
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
         self._check(_lib.qv_counters(self._h, C.byref(a), C.byref(b), C.byref(c)))
         return dict(launches=a.value, leaf_evals=b.value, far_evals=c.value)
+
+
+def read_run_file(path) -> QvRun:
+    r = QvRun()
+    rc = _lib.qv_read_run_file(str(path).encode(), C.byref(r))
+    if rc < 0:
+        raise QvError(rc, f"cannot read {path}")
+    return r
+
+
+def read_var_file(path):
+    n, t = C.c_int(), C.c_double()
+    rc = _lib.qv_read_var_file(str(path).encode(), 0, C.byref(n), C.byref(t), None, None, None)
+    if rc < 0:
+        raise QvError(rc, f"cannot read {path}")
+    x = np.empty((n.value, 3))
+    inf = np.empty(n.value, np.int32)
+    beh = np.empty(n.value, np.int32)
+    rc = _lib.qv_read_var_file(str(path).encode(), n.value, C.byref(n), C.byref(t), _ptr(x),
+                               _ptr(inf), _ptr(beh))
+    if rc < 0:
+        raise QvError(rc, f"cannot read {path}")
+    return t.value, x, inf, beh
+
+
+def write_var_file(path, t, x, infront, u=None):
+    x = _f64(x)
+    inf = _i32(infront)
+    uu = None if u is None else _f64(u)
+    rc = _lib.qv_write_var_file(str(path).encode(), x.shape[0], t, _ptr(x), _ptr(inf), _ptr(uu))
+    if rc < 0:
+        raise QvError(rc, f"cannot write {path}")
+
+
+def setup_loops(initf: str, pcount: int, delta: float):
+    x = np.empty((pcount, 3))
+    inf = np.empty(pcount, np.int32)
+    beh = np.empty(pcount, np.int32)
+    rc = _lib.qv_setup_loops(initf.encode(), pcount, delta, _ptr(x), _ptr(inf), _ptr(beh))
+    if rc < 0:
+        raise QvError(rc, f"initf {initf} is outside this path")
+    return x, inf, beh
 
 
 def probe_fp32(stream: int | None = None) -> float:
