@@ -140,6 +140,26 @@ int qv_energy(qv_ctx *ctx, double *energy);
  * itime % recon_shots == 0, ghostp, boundary wrap.  Device-resident. */
 int qv_step(qv_ctx *ctx, int itime);
 
+/* ------------------------------------------------------------- derivatives
+ * Hand-written derivatives of the path (no counterpart in the reference, which
+ * has no adjoint; they serve gradient-based studies and the stiff solver). */
+/* calc_velocity for every active point into a device array u (3n). */
+int qv_velocity_device(qv_ctx *ctx, double *u);
+/* x_bar = J^T u_bar of calc_velocity (src/timestep.f90:180-309) at the
+ * context's positions, through LIA, the direct sum or the tree walk (topology
+ * of the current tree frozen) and the ghost gather.  Device pointers (3n). */
+int qv_velocity_vjp(qv_ctx *ctx, const double *u_bar, double *x_bar);
+/* energy_info (src/diagnostic.f90:259-280) for the context's positions and the
+ * device velocities u, with dE/dx (explicit, through s' and the segment
+ * lengths) and dE/du, device pointers (3n); energy on the host. */
+int qv_energy_grad(qv_ctx *ctx, const double *u, double *energy, double *x_bar, double *u_bar);
+/* biot_savart_general(_shift) (src/timestep.f90:516-563) at m host points and
+ * the exact gradient du_i/dx_k (9 per point, row-major) -- the derivative that
+ * velocity_quasip takes by central differences (src/hamiltonian.f90:65-89).
+ * grad_images = 0 differentiates the unshifted sum as the reference does. */
+int qv_field_velocity(qv_ctx *ctx, int m, const double *pts, int grad_images, double *u,
+                      double *dudx);
+
 /* ---------------------------------------------------------------- host side
  * The parts of the reference's driver that feed this path, for a host that
  * runs without the Fortran code (qvort_run) or a test. */

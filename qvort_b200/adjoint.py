@@ -1,0 +1,157 @@
+"""Differentiable filament dynamics on top of the C ABI's hand-written derivatives.
+
+The velocity u = calc_velocity(x) (src/timestep.f90:180-309) and the energy
+E = energy_info(x, u) (src/diagnostic.f90:259-280) are torch.autograd.Functions
+whose backward passes call qv_velocity_vjp and qv_energy_grad (CUDA).  The
+Adams-Bashforth ladder of pmotion (src/timestep.f90:48-71) and the periodic
+wrap (src/periodic.f90:188-214) are a few lines of torch, so autograd chains
+them; torch.utils.checkpoint keeps one state every `checkpoint_every` steps
+and recomputes the steps in between during the backward pass.
+
+With velocity Tree the topology of each step's octree is frozen in its
+derivative (the opening decisions are piecewise constant in x).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+from torch.utils.checkpoint import checkpoint
+
+from . import lib as L
+
+
+class FilamentSystem:
+    """A fixed set of links (infront/behind) and run parameters on one GPU."""
+
+    def __init__(self, params: L.QvParams, infront, behind, device="cuda"):
+        self.params = params
+        self.device = torch.device(device)
+        self.inf = torch.as_tensor(np.asarray(infront, np.int32), device=self.device)
+        self.beh = torch.as_tensor(np.asarray(behind, np.int32), device=self.device)
+        self.n = int(self.inf.shape[0])
+        self.stream = torch.cuda.current_stream(self.device)
+        self.ctx = L.Context(params, stream=self.stream.cuda_stream)
+
+    def load(self, x: torch.Tensor):
+        assert x.dtype == torch.float64 and x.is_cuda and x.shape == (self.n, 3)
+        x = x.contiguous()
+        self.ctx.set_points_device(self.n, x.data_ptr(), self.inf.data_ptr(), self.beh.data_ptr())
+        return x
+
+    def close(self):
+        self.ctx.close()
+
+
+class VelocityFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, system: FilamentSystem):
+        x = system.load(x.detach())
+        u = torch.empty_like(x)
+        system.ctx.velocity_device(u.data_ptr())
+        ctx.save_for_backward(x)
+        ctx.system = system
+        return u
+
+    @staticmethod
+    def backward(ctx, ubar):
+        (x,) = ctx.saved_tensors
+        system = ctx.system
+        system.load(x)
+        xbar = torch.empty_like(x)
+        system.ctx.velocity_vjp(ubar.contiguous().data_ptr(), xbar.data_ptr())
+        return xbar, None
+
+
+class EnergyFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, u, system: FilamentSystem):
+        x = system.load(x.detach())
+        u = u.detach().contiguous()
+        xbar = torch.empty_like(x)
+        ubar = torch.empty_like(u)
+        e = system.ctx.energy_grad(u.data_ptr(), xbar.data_ptr(), ubar.data_ptr())
+        ctx.save_for_backward(xbar, ubar)
+        return torch.tensor(e, dtype=torch.float64, device=x.device)
+
+    @staticmethod
+    def backward(ctx, ebar):
+        xbar, ubar = ctx.saved_tensors
+        return ebar * xbar, ebar * ubar, None
+
+
+def velocity(x: torch.Tensor, system: FilamentSystem) -> torch.Tensor:
+    return VelocityFn.apply(x, system)
+
+
+def energy(x: torch.Tensor, u: torch.Tensor, system: FilamentSystem) -> torch.Tensor:
+    return EnergyFn.apply(x, u, system)
+
+
+def _allzero(h):
+    return (h == 0).all(dim=1, keepdim=True)
+
+
+def ab_step(x, u, u1, u2, u3, dt: float):
+    """One rung of the Adams-Bashforth ladder per point (exact-zero history tests)."""
+    z1, z2, z3 = _allzero(u1), _allzero(u2), _allzero(u3)
+    ab4 = dt * (55.0 * u - 59.0 * u1 + 37.0 * u2 - 9.0 * u3) / 24.0
+    ab3 = (23.0 / 12.0) * dt * u - (4.0 / 3.0) * dt * u1 + (5.0 / 12.0) * dt * u2
+    ab2 = 1.5 * dt * u - 0.5 * dt * u1
+    dx = torch.where(z1, dt * u, torch.where(z2, ab2, torch.where(z3, ab3, ab4)))
+    return x + dx
+
+
+def wrap(x, system: FilamentSystem):
+    bc, L_ = system.params.boundary, system.params.box_size
+    lo = {1: 0, 2: 1, 3: 2}.get(bc)
+    if lo is None:
+        return x
+    h = L_ / 2.0
+    cols = torch.arange(3, device=x.device) >= lo
+    shift = (x.detach() > h).double() - (x.detach() < -h).double()
+    return x - L_ * shift * cols
+
+
+def run(x0: torch.Tensor, system: FilamentSystem, nsteps: int, checkpoint_every: int = 16):
+    """x_K after nsteps Adams-Bashforth steps from x0 with zero history."""
+    dt = system.params.dt
+    zero = torch.zeros_like(x0)
+
+    def segment(x, u1, u2, u3, k):
+        for _ in range(k):
+            u = velocity(x, system)
+            x = wrap(ab_step(x, u, u1, u2, u3, dt), system)
+            u1, u2, u3 = u, u1, u2
+        return x, u1, u2, u3
+
+    x, u1, u2, u3 = x0, zero, zero, zero
+    for s in range(0, nsteps, checkpoint_every):
+        k = min(checkpoint_every, nsteps - s)
+        if checkpoint_every and torch.is_grad_enabled():
+            x, u1, u2, u3 = checkpoint(segment, x, u1, u2, u3, k, use_reentrant=False)
+        else:
+            x, u1, u2, u3 = segment(x, u1, u2, u3, k)
+    return x
+
+
+def min_image(d: torch.Tensor, system: FilamentSystem):
+    if system.params.boundary != 1:
+        return d
+    L_ = system.params.box_size
+    return d - L_ * torch.round(d.detach() / L_)
+
+
+def loss(x0: torch.Tensor, system: FilamentSystem, nsteps: int, checkpoint_every: int = 16):
+    """Filament kinetic energy (energy_info) of the final state plus the squared
+    displacement of the points: E(x_K) + sum |x_K - x_0|^2."""
+    xk = run(x0, system, nsteps, checkpoint_every)
+    uk = velocity(xk, system)
+    return energy(xk, uk, system) + (min_image(xk - x0, system) ** 2).sum()
+
+
+def gradient(x0: np.ndarray, system: FilamentSystem, nsteps: int, checkpoint_every: int = 16):
+    """(loss, dloss/dx0) for initial positions x0 (n, 3)."""
+    x = torch.tensor(np.asarray(x0, np.float64), device=system.device, requires_grad=True)
+    val = loss(x, system, nsteps, checkpoint_every)
+    (g,) = torch.autograd.grad(val, x)
+    return float(val.item()), g.detach().cpu().numpy()

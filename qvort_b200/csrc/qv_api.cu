@@ -134,6 +134,11 @@ extern "C" int qv_destroy(qv_ctx *c) {
   if (c->dstatus) cudaFree(c->dstatus);
   if (c->dscalar) cudaFree(c->dscalar);
   if (c->d_nact) cudaFree(c->d_nact);
+  {
+    void *adj[] = {c->adj_xb, c->adj_gib, c->adj_gbb, c->adj_giib, c->adj_gbbb, c->adj_nb};
+    for (void *q : adj)
+      if (q) cudaFree(q);
+  }
   if (c->walk_part) cudaFree(c->walk_part);
   for (int k = 0; k < 2; k++) {
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);

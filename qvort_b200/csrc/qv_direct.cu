@@ -312,6 +312,16 @@ __global__ void k_direct_reduce(int na, int nchunk, const int *__restrict__ act,
   }
 }
 
+// Source packs of the compacted active list (c->act, c->n_act).
+int qv_pack_sources64(qv_ctx *c) {
+  if (c->n_act == 0) return QV_OK;
+  k_pack_sources<<<nblk(c->n_act, 256), 256, 0, c->stream>>>(c->n_act, c->act, c->x, c->gi,
+                                                             c->src64, c->src32);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
 int qv_launch_direct(qv_ctx *c) {
   int na = c->n_act;
   if (na == 0) return QV_OK;

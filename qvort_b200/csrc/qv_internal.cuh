@@ -112,6 +112,12 @@ struct qv_ctx {
   int *blkcnt = nullptr;  // per-256-slot block counts of the compaction (n/256+2)
   double *dpart = nullptr;  // direct-sum partial sums, grown on demand
   size_t dpart_bytes = 0;
+  // adjoint scratch: per-point adjoints of x and the four ghosts, per-node
+  // adjoints of (cent, circ, Cij)
+  double *adj_xb = nullptr, *adj_gib = nullptr, *adj_gbb = nullptr, *adj_giib = nullptr,
+         *adj_gbbb = nullptr, *adj_nb = nullptr;
+  int adj_n = 0;
+  size_t adj_nb_bytes = 0;
   double *src64 = nullptr;  // direct-sum source pack (FP64)
   float *src32 = nullptr;   // direct-sum source pack (FP32 hi/lo)
   unsigned long long *evals = nullptr;  // device eval counter

@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "qv_internal.cuh"
+#include "qv_lia.cuh"
 
 int qv_fail(qv_ctx *c, int code, const char *fmt, ...) {
   if (c) {
@@ -80,47 +81,12 @@ int qv_launch_ghosts(qv_ctx *c) {
 }
 
 // ---------------------------------------------------------------- LIA
-__device__ __forceinline__ double ddist(const double *a, const double *b) {
-  double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
-  return sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-}
+__device__ __forceinline__ double ddist(const double *a, const double *b) { return lia_dist(a, b); }
 
-// get_deriv_1 / get_deriv_2, src/derivatives.f90:11-75 (second and fourth
-// order non-uniform finite differences on the ghost stencil).
-__device__ void derivs(int order, const double *x, const double *gi, const double *gb,
-                       const double *gii, const double *gbb, double *s1, double *s2) {
-  double disti = ddist(x, gi), distb = ddist(x, gb);
-  if (order != 4) {
-    double den1 = 2. * distb * disti;
-    double q1 = disti * (disti + distb), q2 = disti * distb, q3 = distb * (disti + distb);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      s1[c] = (distb * gi[c] + (disti - distb) * x[c] - disti * gb[c]) / den1;
-      s2[c] = 2. * (gi[c] / q1 - x[c] / q2 + gb[c] / q3);
-    }
-    return;
-  }
-  double dii = ddist(gii, gi), dbb = ddist(gbb, gb);
-  double di2 = disti * disti, db2 = distb * distb;
-  double dA = dbb * (dbb + distb) * (dbb + distb + disti) * (dbb + distb + disti + dii);
-  double dB = dbb * distb * (distb + disti) * (distb + disti + dii);
-  double dD = disti * dii * (distb + disti) * (dbb + distb + disti);
-  double dE = dii * (disti + dii) * (distb + disti + dii) * (dbb + distb + disti + dii);
-  double A = (distb * di2 + distb * disti * dii) / dA;
-  double B = (-dbb * di2 - distb * di2 - dbb * disti * dii - distb * disti * dii) / dB;
-  double D = (dbb * distb * disti + db2 * disti + dbb * distb * dii + db2 * dii) / dD;
-  double E = (-disti * db2 - dbb * distb * disti) / dE;
-  double C = -(A + B + D + E);
-  double A2 = 2. * (-2. * distb * disti + di2 - distb * dii + disti * dii) / dA;
-  double B2 = 2. * (2. * dbb * disti + 2. * distb * disti - di2 + dbb * dii + distb * dii - disti * dii) / dB;
-  double D2 = 2. * (-dbb * distb - db2 + dbb * disti + 2. * distb * disti + dbb * dii + 2. * distb * dii) / dD;
-  double E2 = 2. * (dbb * distb + db2 - dbb * disti - 2. * distb * disti) / dE;
-  double C2 = -(A2 + B2 + D2 + E2);
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    s1[c] = A * gbb[c] + B * gb[c] + C * x[c] + D * gi[c] + E * gii[c];
-    s2[c] = A2 * gbb[c] + B2 * gb[c] + C2 * x[c] + D2 * gi[c] + E2 * gii[c];
-  }
+__device__ __forceinline__ void derivs(int order, const double *x, const double *gi,
+                                       const double *gb, const double *gii, const double *gbb,
+                                       double *s1, double *s2) {
+  lia_derivs(order, x, gi, gb, gii, gbb, s1, s2);
 }
 
 // Local term of calc_velocity: LIA arm (src/timestep.f90:196-217) or the
@@ -134,31 +100,14 @@ __global__ void k_lia(int n, const double *__restrict__ x, const int *__restrict
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (inf[i] == 0) return;
-  double X[3], GI[3], GB[3], GII[3], GBB[3], s1[3], s2[3];
+  double X[3], GI[3], GB[3], GII[3], GBB[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     X[c] = x[3 * i + c]; GI[c] = gi[3 * i + c]; GB[c] = gb[3 * i + c];
     GII[c] = gii[3 * i + c]; GBB[c] = gbb[3 * i + c];
   }
-  double out[3] = {0., 0., 0.};
-  if (velocity != QV_VEL_OFF) {
-    derivs(order, X, GI, GB, GII, GBB, s1, s2);
-    double beta;
-    if (velocity == QV_VEL_LIA) {
-      if (fixed_beta) {
-        beta = 1.3E-3;
-      } else {
-        double curv = sqrt(s2[0] * s2[0] + s2[1] * s2[1] + s2[2] * s2[2]);
-        curv = curv < QV_DEPS ? QV_DEPS : 1. / curv;
-        beta = (quant_circ / (4. * QV_PI)) * log(curv / corea);
-      }
-    } else {
-      beta = (quant_circ / (4. * QV_PI)) * log((1.21 / corea) * sqrt(ddist(X, GI) * ddist(X, GB)));
-    }
-    out[0] = beta * (s1[1] * s2[2] - s1[2] * s2[1]);
-    out[1] = beta * (s1[2] * s2[0] - s1[0] * s2[2]);
-    out[2] = beta * (s1[0] * s2[1] - s1[1] * s2[0]);
-  }
+  double out[3];
+  lia_term(velocity, order, fixed_beta, quant_circ, corea, X, GI, GB, GII, GBB, out);
 #pragma unroll
   for (int c = 0; c < 3; c++) u_li[3 * i + c] = out[c];
   if (velocity == QV_VEL_LIA || velocity == QV_VEL_OFF)

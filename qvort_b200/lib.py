@@ -119,6 +119,10 @@ _SIGS = {
                     C.POINTER(C.c_longlong)],
     "qv_probe_fp32": [_P, _D],
     "qv_velocity_direct_noalloc": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, _P],
+    "qv_velocity_device": [_P, _P],
+    "qv_velocity_vjp": [_P, _P, _P],
+    "qv_energy_grad": [_P, _P, _D, _P, _P],
+    "qv_field_velocity": [_P, C.c_int, _P, C.c_int, _P, _P],
     "qv_read_run_file": [C.c_char_p, C.POINTER(QvRun)],
     "qv_read_var_file": [C.c_char_p, C.c_int, _I, _D, _P, _P, _P],
     "qv_write_var_file": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
@@ -318,6 +322,27 @@ class Context:
 
     def sync(self):
         self._check(_lib.qv_sync(self._h))
+
+    # ---- derivatives (device pointers)
+    def velocity_device(self, u_ptr: int):
+        self._check(_lib.qv_velocity_device(self._h, u_ptr))
+
+    def velocity_vjp(self, ubar_ptr: int, xbar_ptr: int):
+        self._check(_lib.qv_velocity_vjp(self._h, ubar_ptr, xbar_ptr))
+
+    def energy_grad(self, u_ptr: int, xbar_ptr: int, ubar_ptr: int) -> float:
+        e = C.c_double()
+        self._check(_lib.qv_energy_grad(self._h, u_ptr, C.byref(e), xbar_ptr, ubar_ptr))
+        return e.value
+
+    def field_velocity(self, pts, grad_images: bool = False):
+        pts = _f64(pts).reshape(-1, 3)
+        m = pts.shape[0]
+        u = np.empty((m, 3))
+        du = np.empty((m, 3, 3))
+        self._check(_lib.qv_field_velocity(self._h, m, _ptr(pts), int(grad_images), _ptr(u),
+                                           _ptr(du)))
+        return u, du
 
     # ---- instrumentation
     PHASES = ("ghosts", "build", "local", "nonlocal", "update", "search", "wrap",

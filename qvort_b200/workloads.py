@@ -75,16 +75,18 @@ def ring(n: int = 200, radius: float = 0.01, perturb: float = 1e-5, seed: int = 
 
 def random_rings(n_rings: int, rmin: float, rmax: float, delta: float, box: float = 0.1,
                  seed: int = 0, spacing: float = 0.75, theta: float = 0.4,
-                 dt: float = 1e-7, name: str = "tangle") -> Workload:
-    """Rings with radius U(rmin, rmax), centres uniform in the box, normals uniform
-    on the sphere, point spacing spacing*delta, wrapped into the periodic box."""
+                 dt: float = 1e-7, name: str = "tangle", centre_box: float | None = None) -> Workload:
+    """Rings with radius U(rmin, rmax), centres uniform in the box (or in a cube
+    of side centre_box about the origin), normals uniform on the sphere, point
+    spacing spacing*delta, wrapped into the periodic box."""
     rng = np.random.default_rng(seed)
     xs, infs, behs = [], [], []
     start = 0
     for _ in range(n_rings):
         R = rng.uniform(rmin, rmax)
         m = max(5, int(round(2 * np.pi * R / (spacing * delta))))
-        c = rng.uniform(0.0, box, 3) - box / 2.0
+        cb = box if centre_box is None else centre_box
+        c = rng.uniform(0.0, cb, 3) - cb / 2.0
         nrm = rng.normal(size=3)
         e1, e2 = _basis(nrm)
         k = np.arange(1, m + 1)

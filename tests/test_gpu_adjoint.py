@@ -1,0 +1,158 @@
+"""GPU tests of the hand-written derivatives against central finite differences.
+
+Tolerance: 1e-5 relative on directional derivatives (the bar the adjoint is
+built to).  The FP64 forward maps are smooth between tree opening decisions;
+steps of 1e-7 (1e-8 with the tree, so that no decision flips) balance the
+truncation error against the rounding noise of the forward sums.  The rings
+are placed so that none crosses the box: with open boundaries a wrapped ring
+would contain a box-long segment, whose near-singular Biot-Savart terms make
+any difference quotient rounding-dominated.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _mods():
+    import torch
+
+    from qvort_b200 import adjoint as A
+    from qvort_b200 import lib as L
+    from qvort_b200 import workloads as W
+
+    return torch, A, L, W
+
+
+def _system(W, L, A, velocity="BS", boundary="open", theta=0.0, order=2, precision="fp64",
+            seed=4, n_rings=6):
+    w = W.random_rings(n_rings, 0.006, 0.01, 5e-4, 0.1, seed=seed, centre_box=0.05)
+    prm = dict(w.params, velocity=velocity, boundary=boundary, tree_theta=theta,
+               deriv_order=order, precision=precision)
+    return w, A.FilamentSystem(L.default_params(**prm), w.infront, w.behind)
+
+
+def _dirderiv_fd(f, x, d, h):
+    return (f(x + h * d) - f(x - h * d)) / (2 * h)
+
+
+@pytest.mark.parametrize("velocity,boundary,theta,order", [
+    ("BS", "open", 0.0, 2), ("BS", "periodic", 0.0, 2), ("BS", "open", 0.0, 4),
+    ("Tree", "periodic", 0.5, 2), ("LIA", "open", 0.0, 2)])
+def test_velocity_vjp_matches_fd(velocity, boundary, theta, order):
+    torch, A, L, W = _mods()
+    w, sysm = _system(W, L, A, velocity, boundary, theta, order)
+    rng = np.random.default_rng(1)
+    x = torch.tensor(w.x, device="cuda")
+    ub = torch.tensor(rng.normal(size=w.x.shape), device="cuda")
+    xr = x.clone().requires_grad_(True)
+    u = A.velocity(xr, sysm)
+    (xb,) = torch.autograd.grad((u * ub).sum(), xr)
+    worst = 0.0
+    for k in range(3):
+        d = torch.tensor(rng.normal(size=w.x.shape), device="cuda")
+        d /= d.norm()
+        f = lambda y: float((A.velocity(y, sysm) * ub).sum())
+        fd = _dirderiv_fd(f, x, d, 1e-7 if velocity != "Tree" else 1e-8)
+        an = float((xb * d).sum())
+        worst = max(worst, abs(fd - an) / abs(an))
+    sysm.close()
+    assert worst < 1e-5, worst
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_energy_grad_matches_fd(order):
+    torch, A, L, W = _mods()
+    w, sysm = _system(W, L, A, order=order)
+    rng = np.random.default_rng(2)
+    x = torch.tensor(w.x, device="cuda")
+    u = torch.tensor(rng.normal(size=w.x.shape) * 0.1, device="cuda")
+    xr, ur = x.clone().requires_grad_(True), u.clone().requires_grad_(True)
+    e = A.energy(xr, ur, sysm)
+    xb, ubar = torch.autograd.grad(e, (xr, ur))
+    for k in range(2):
+        d = torch.tensor(rng.normal(size=w.x.shape), device="cuda")
+        d /= d.norm()
+        fx = _dirderiv_fd(lambda y: float(A.energy(y, u, sysm)), x, d, 1e-7)
+        fu = _dirderiv_fd(lambda v: float(A.energy(x, v, sysm)), u, d, 1e-6)
+        assert abs(fx - float((xb * d).sum())) <= 1e-5 * abs(fx)
+        assert abs(fu - float((ubar * d).sum())) <= 1e-5 * abs(fu)
+    sysm.close()
+
+
+def test_energy_matches_the_path_energy():
+    torch, A, L, W = _mods()
+    w, sysm = _system(W, L, A)
+    c = L.Context(sysm.params)
+    c.set_points(w.x, w.infront, w.behind)
+    u, *_ = c.velocity()
+    e_ref = c.energy()
+    x = torch.tensor(w.x, device="cuda")
+    e = float(A.energy(x, torch.tensor(u, device="cuda"), sysm))
+    assert e == pytest.approx(e_ref, rel=1e-12)
+    sysm.close()
+
+
+def test_trajectory_loss_gradient_matches_fd():
+    """Gradient of E(x_K) + sum|x_K - x_0|^2 after K AB steps (checkpointed
+    every 4 steps) w.r.t. x_0, against central differences of the same loss."""
+    torch, A, L, W = _mods()
+    w, sysm = _system(W, L, A, boundary="periodic", n_rings=4)
+    K = 10
+    val, g = A.gradient(w.x, sysm, K, checkpoint_every=4)
+    rng = np.random.default_rng(3)
+    x = torch.tensor(w.x, device="cuda")
+    worst = 0.0
+    for k in range(4):
+        d = rng.normal(size=w.x.shape)
+        d /= np.linalg.norm(d)
+        dd = torch.tensor(d, device="cuda")
+        with torch.no_grad():
+            f = lambda y: float(A.loss(y, sysm, K, checkpoint_every=4))
+            fd = _dirderiv_fd(f, x, dd, 1e-7)
+        an = float((g * d).sum())
+        worst = max(worst, abs(fd - an) / abs(an))
+    sysm.close()
+    assert worst < 1e-5, worst
+
+
+def test_mixed_tree_gradient_matches_fp64_tree_gradient():
+    """The fast path's gradient (mixed-precision Barnes-Hut forward) against the
+    reference gradient from the FP64 velocity (same tree decisions)."""
+    torch, A, L, W = _mods()
+    grads = []
+    for prec in ("mixed", "fp64"):
+        w, sysm = _system(W, L, A, "Tree", "periodic", 0.5, precision=prec, n_rings=8)
+        grads.append(A.gradient(w.x, sysm, 8, checkpoint_every=4)[1])
+        sysm.close()
+    rel = np.linalg.norm(grads[0] - grads[1]) / np.linalg.norm(grads[1])
+    assert rel < 1e-5, rel
+
+
+@pytest.mark.parametrize("grad_images", [False, True])
+def test_field_velocity_and_exact_gradient(grad_images):
+    torch, A, L, W = _mods()
+    w, sysm = _system(W, L, A, boundary="periodic")
+    c = L.Context(sysm.params)
+    c.set_points(w.x, w.infront, w.behind)
+    rng = np.random.default_rng(5)
+    pts = rng.uniform(-0.04, 0.04, (5, 3))
+    u, du = c.field_velocity(pts, grad_images)
+    h = 1e-7
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = h
+        up, _ = c.field_velocity(pts + e, grad_images)
+        um, _ = c.field_velocity(pts - e, grad_images)
+        if not grad_images:
+            # velocity_quasip differentiates the unshifted sum only
+            q = L.default_params(**dict(w.params, boundary="open"))
+            c2 = L.Context(q)
+            c2.set_points(w.x, w.infront, w.behind)
+            up, _ = c2.field_velocity(pts + e)
+            um, _ = c2.field_velocity(pts - e)
+            c2.close()
+        fd = (up - um) / (2 * h)
+        np.testing.assert_allclose(du[:, :, k], fd, rtol=1e-5, atol=1e-9 * np.abs(du).max())
+    c.close()
+    sysm.close()
