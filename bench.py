@@ -404,11 +404,37 @@ def extras(ctx, w, stream, L, torch, itime):
                           "-> qv_get_points/qv_get_history/qv_get_closest (pinned host), "
                           "wall clock"}
 
+    # ---- gradients/s on the differentiation workload: 16 trefoil rings,
+    # N = 50,000, periodic, K = 256 Adams-Bashforth steps checkpointed every 16,
+    # mixed Barnes-Hut forward (theta 0.4) and the FP64 adjoint backward
+    out["gradient"] = gradient_rate(L, torch)
+
     # ---- CPU baseline (oracle port on this host's cores), bounded sample
     t, sample, cores = cpu_step_rate(w)
     out["cpu_baseline"] = {"value": pairs_step / t, "unit": UNIT, "cores": cores, "kind": "port",
                            "sample": sample, "ms_per_step": t * 1e3}
     return out
+
+
+def gradient_rate(L, torch, steps: int = 256, reps: int = 2) -> dict:
+    from qvort_b200 import adjoint as A
+    from qvort_b200 import workloads as W
+
+    w = W.trefoil_rings()
+    prm = dict(w.params, velocity="Tree", tree_theta=0.4, precision="mixed")
+    s = A.FilamentSystem(L.default_params(**prm), w.infront, w.behind)
+    A.gradient(w.x, s, 16, 16)          # warm-up: buffers, tree capacity
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        A.gradient(w.x, s, steps, 16)
+    torch.cuda.synchronize()
+    sec = (time.perf_counter() - t0) / reps
+    s.close()
+    return {"value": 1.0 / sec, "unit": "gradients/s", "s_per_gradient": sec,
+            "workload": f"16 trefoil rings, N={w.n}, periodic L=0.1, K={steps} AB steps, "
+                        "checkpoint every 16, Tree theta 0.4 mixed forward, FP64 adjoint; "
+                        "loss = E(x_K) + sum |x_K - x_0|^2; wall clock"}
 
 
 def main():

@@ -73,7 +73,11 @@ typedef struct qv_ctx qv_ctx;
 int qv_default_params(qv_params *p);
 
 /* Create / destroy a context.  Replaces nothing: the reference keeps state in
- * module variables (src/cdata.f90).  stream may be NULL (a private stream). */
+ * module variables (src/cdata.f90).  Every launch and copy of the context goes
+ * to `stream`; NULL makes the context create a private non-blocking stream,
+ * which is not ordered with any other stream, so a caller that hands the
+ * context device buffers written by work on the legacy default stream passes
+ * cudaStreamLegacy ((void *)0x1) instead of NULL. */
 int qv_create(const qv_params *p, void *stream, qv_ctx **out);
 int qv_destroy(qv_ctx *ctx);
 int qv_set_params(qv_ctx *ctx, const qv_params *p);

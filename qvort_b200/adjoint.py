@@ -30,7 +30,11 @@ class FilamentSystem:
         self.beh = torch.as_tensor(np.asarray(behind, np.int32), device=self.device)
         self.n = int(self.inf.shape[0])
         self.stream = torch.cuda.current_stream(self.device)
-        self.ctx = L.Context(params, stream=self.stream.cuda_stream)
+        # The context reads and writes torch-owned device memory, so it must
+        # run on torch's stream.  torch's default stream has handle 0, which
+        # qv_create takes as "make a private stream": pass cudaStreamLegacy
+        # (0x1), the same legacy default stream, instead.
+        self.ctx = L.Context(params, stream=self.stream.cuda_stream or 0x1)
 
     def load(self, x: torch.Tensor):
         assert x.dtype == torch.float64 and x.is_cuda and x.shape == (self.n, 3)

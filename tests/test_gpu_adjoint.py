@@ -156,3 +156,20 @@ def test_field_velocity_and_exact_gradient(grad_images):
         np.testing.assert_allclose(du[:, :, k], fd, rtol=1e-5, atol=1e-9 * np.abs(du).max())
     c.close()
     sysm.close()
+
+
+def test_trefoil_trajectory_gradient_fd_check():
+    """The differentiation configuration's check at reduced size: trefoil rings
+    (mode-3 perturbation, seeded 1e-5 cm displacement), periodic, FP64 direct
+    velocity, K=32 steps checkpointed every 16, central differences along
+    seeded unit directions.  The step is 1e-7 cm: at 1e-9 cm the rounding
+    noise of the loss (an energy summed over all points) divided by h reaches
+    1e-6..6e-5 of the directional derivative on this system."""
+    torch, A, L, W = _mods()
+    from qvort_b200 import gradcheck as G
+
+    w = W.trefoil_rings(seed=0, n_rings=4, pts_per_ring=64)
+    r = G.fd_check(w, steps=32, dirs=8, hs=(1e-7,), velocity="BS", tree_theta=0.0)
+    assert r["by_h"]["1e-07"]["rel_max"] < 1e-5, r["by_h"]
+    m = G.mixed_vs_fp64(w, steps=32, velocity="Tree", tree_theta=0.4)
+    assert m["rel"] < 1e-5, m
