@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--suite", default="tangle", choices=["tangle", "batch", "gradient"],
+                    help="tangle: the headline line; batch / gradient: only that workload's entry")
     ap.add_argument("--quick", action="store_true",
                     help="headline timing only (no comparators, e2e or CPU baseline)")
     return ap.parse_args()
@@ -409,6 +411,9 @@ def extras(ctx, w, stream, L, torch, itime):
     # mixed Barnes-Hut forward (theta 0.4) and the FP64 adjoint backward
     out["gradient"] = gradient_rate(L, torch)
 
+    # ---- batched ensemble: 512 independent open systems in one graph per step
+    out["batch"] = batch_rate(L, torch)
+
     # ---- CPU baseline (oracle port on this host's cores), bounded sample
     t, sample, cores = cpu_step_rate(w)
     out["cpu_baseline"] = {"value": pairs_step / t, "unit": UNIT, "cores": cores, "kind": "port",
@@ -437,10 +442,74 @@ def gradient_rate(L, torch, steps: int = 256, reps: int = 2) -> dict:
                         "loss = E(x_K) + sum |x_K - x_0|^2; wall clock"}
 
 
+def batch_rate(L, torch, steps: int = 20) -> dict:
+    """512 independent open systems (rings and leap-frogging pairs, N log-uniform
+    in [100, 8000], dt from {5e-8, 1e-7, 2e-7}, direct below 2000 points,
+    Barnes-Hut theta 0.4 above) advanced by qv_batch_step, against the same
+    systems stepped one after another through single-system contexts."""
+    from qvort_b200 import workloads as W
+
+    ws = W.batch_systems()
+    n_all = sum(w.n for w in ws)
+    pairs = float(sum(w.n * w.n for w in ws))
+    p = L.default_params(**dict(ws[0].params, boundary="open", velocity="Tree", tree_theta=0.4,
+                                precision="mixed"))
+    b = L.Batch(p, [(w.x, w.infront, w.behind) for w in ws], [w.params["velocity"] for w in ws],
+                [w.params["dt"] for w in ws])
+    tuned = b.tune(3)
+    u_batch = b.velocity()
+    b.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(steps)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    st = b.stats()
+    b.close()
+    # the same systems one at a time (the per-system launch sequence of qv_step's
+    # velocity + update), and the bitwise comparison of their velocities
+    ctxs, equal = [], True
+    for w, u in zip(ws, np.split(u_batch, np.cumsum([w.n for w in ws])[:-1])):
+        c = L.Context(L.default_params(**dict(w.params, precision="mixed")))
+        c.set_points(w.x, w.infront, w.behind)
+        equal = equal and bool(np.array_equal(c.velocity(False)[0], u))
+        ctxs.append((c, w.params["velocity"] == "Tree"))
+
+    def seq_step():
+        for c, tree in ctxs:
+            if tree:
+                c.build_tree()
+            c.velocity(False)
+            c.step_ab()
+
+    seq_step()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        seq_step()
+    seq_ms = (time.perf_counter() - t0) * 1e3 / 2
+    for c, _ in ctxs:
+        c.close()
+    return {"ms_per_step": ms, "system_steps_per_s": len(ws) * 1e3 / ms,
+            "pairs_per_s": pairs / (ms * 1e-3), "sequential_ms_per_step": seq_ms,
+            "speedup_vs_sequential": seq_ms / ms, "velocities_bitwise_equal_to_sequential": equal,
+            "graph": st["graph"], "tuned": tuned, "leaf_evals": st["leaf_evals"],
+            "far_evals": st["far_evals"],
+            "workload": f"512 open systems, N={n_all} points ({sum(w.params['velocity'] == 'Tree' for w in ws)} "
+                        "Barnes-Hut theta 0.4, the rest direct), per-system dt; pairs = sum N_s^2 "
+                        "(direct-equivalent); wall clock over the graph replays"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.suite != "tangle":
+        import torch
+
+        from qvort_b200 import lib as L
+
+        r = batch_rate(L, torch, args.steps) if args.suite == "batch" else gradient_rate(L, torch)
+        print(json.dumps({"suite": args.suite, **r}), flush=True)
+        return 0
     return our_arm(args)
 
 

@@ -225,6 +225,43 @@ int qv_probe_fp32(void *stream, double *tflops);
 int qv_velocity_direct_noalloc(const qv_params *p, int n, const double *x, const int *infront,
                                const int *behind, double *u_bs, void *stream);
 
+/* ---------------------------------------------------------------- batches
+ * Many independent systems advanced together (no counterpart in the
+ * reference, which runs one system per process; each system is what one run
+ * of src/run.f90's loop would hold).  nsys systems occupy consecutive slot
+ * ranges [offsets[s], offsets[s+1]) of one point array; method[s] is
+ * QV_VEL_BS (direct sum) or QV_VEL_TREE (Barnes-Hut with p->tree_theta), dt[s]
+ * the system's time step.  Every system has open boundaries and its own box of
+ * side p->box_size centred on the origin of its coordinates; p->boundary must
+ * be QV_BC_OPEN and p->precision QV_PREC_MIXED (else QV_ERR_UNSUPPORTED).
+ * stream: as for qv_create; graph capture needs a stream other than the
+ * legacy default stream (NULL gives a private one). */
+typedef struct qv_batch qv_batch;
+int qv_batch_create(const qv_params *p, int nsys, const int *offsets, const int *method,
+                    const double *dt, void *stream, qv_batch **out);
+void qv_batch_destroy(qv_batch *b);
+const char *qv_batch_last_error(qv_batch *b);
+/* Positions x (3 per slot) and each system's own 1-based links (1..n_s; no
+ * empty slots); clears the Adams-Bashforth history. */
+int qv_batch_set_points(qv_batch *b, const double *x, const int *infront, const int *behind);
+/* calc_velocity of every system at the current positions (u: 3 per slot,
+ * host, may be NULL); positions and history unchanged. */
+int qv_batch_velocity(qv_batch *b, double *u);
+/* nsteps steps of velocity + pmotion for every system: one CUDA graph launch
+ * per step when capture succeeds, otherwise the same launches issued
+ * directly.  Returns when all steps are done. */
+int qv_batch_step(qv_batch *b, int nsteps);
+int qv_batch_get_points(qv_batch *b, double *x, double *u);
+/* Times the persistent work kernel under each launch shape and keeps the
+ * fastest; best_cfg = {warps per block, blocks per SM, order (1 = largest
+ * items first)}.  Results are identical under every shape. */
+int qv_batch_tune(qv_batch *b, int reps, int *best_cfg, float *best_ms);
+int qv_batch_set_config(qv_batch *b, int warps_per_block, int blocks_per_sm, int order);
+/* evals[0..1] = leaf and far-field evaluations of the last step; graph_used;
+ * config[0..7] = warps per block, blocks per SM, order, walk stack entries,
+ * work items, tree systems, forest depth, launches issued so far. */
+int qv_batch_stats(qv_batch *b, long long *evals, int *graph_used, int *config);
+
 #ifdef __cplusplus
 }
 #endif

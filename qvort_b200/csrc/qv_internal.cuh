@@ -174,6 +174,22 @@ int qv_compact_active(qv_ctx *c);
 int qv_compact_active_async(qv_ctx *c);
 int qv_aux_streams(qv_ctx *c);
 
+// A forest of independent trees (one root per system) in c->tree.
+// roots[r] = (first slot, slot count, first position in fact, active count);
+// fact = the forest's active slots, each system's contiguous and ascending;
+// froot[q] = root of position q; d_nfact = device copy of n_fact.
+struct ForestArgs {
+  int nroots = 0, n_fact = 0;
+  const int4 *roots = nullptr;
+  const int *fact = nullptr, *froot = nullptr, *d_nfact = nullptr;
+};
+int qv_forest_reserve(qv_ctx *c, int n_fact, int cap_nodes);
+int qv_forest_build(qv_ctx *c, const ForestArgs &f);
+// control-block words read by forest users on the device
+#define QV_CTL_OVERFLOW 3
+#define QV_CTL_DEPTH 4
+#define QV_CTL_NNODES 0
+
 // ---------------------------------------------------------------- helpers
 // Straight-segment Biot-Savart term in FP32, without the G/(4 pi) factor:
 //   (|R1|+|R2|) / (|R1||R2| (|R1||R2| + R1.R2)) * (R1 x R2)

@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
 #define MC 256    // points per shared-memory chunk in the block kernel
 
 // One warp per node with at most BIGN points.
-__global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl, int cap_nodes,
+__global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl, int cap_nodes, int k0,
                                                      const int *__restrict__ level,
                                                      const int *__restrict__ start,
                                                      const int *__restrict__ count,
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
-  for (int k = 1 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
+  for (int k = k0 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
     int s = start[k], n = count[k];
     if (n > BIGN) continue;
     const int *o = ord + (size_t)level[k] * cap_pts + s;
@@ -380,12 +380,12 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
   }
 }
 
-// List the nodes with more than BIGN points (order irrelevant).
-__global__ void k_list_big(const int *__restrict__ ctl, int cap_nodes,
+// List the non-root nodes (k >= k0) with more than BIGN points (order irrelevant).
+__global__ void k_list_big(const int *__restrict__ ctl, int cap_nodes, int k0,
                            const int *__restrict__ count, int *list, int *nlist) {
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
-  for (int k = 1 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
+  for (int k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
     if (count[k] > BIGN) list[atomicAdd(nlist, 1)] = k;
 }
 
@@ -471,12 +471,10 @@ __global__ void __launch_bounds__(256) k_moments_big(const int *__restrict__ lis
 // Warps 1.. stage chunks of positions in shared memory (double buffered);
 // lanes 0..2 of warp 0 run the three chains.
 #define RC 2048
-__global__ void __launch_bounds__(512) k_root_cent(const int *__restrict__ d_nact,
-                                                   const int *__restrict__ act,
-                                                   const double *__restrict__ x, double *cent) {
+__device__ __forceinline__ void root_cent_chain(const int n_act, const int *__restrict__ act,
+                                                const double *__restrict__ x, double *cent) {
   extern __shared__ double rb[];  // [2][RC][3]
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int n_act = *d_nact;
   const int nch = (n_act + RC - 1) / RC;
   auto produce = [&](int ch, double *dst) {
     int base = ch * RC, m = min(RC, n_act - base);
@@ -512,13 +510,34 @@ __global__ void __launch_bounds__(512) k_root_cent(const int *__restrict__ d_nac
   if (wid == 0 && lane < 3) cent[lane] = __ddiv_rn(acc, (double)n_act);
 }
 
+__global__ void __launch_bounds__(512) k_root_cent(const int *__restrict__ d_nact,
+                                                   const int *__restrict__ act,
+                                                   const double *__restrict__ x, double *cent) {
+  root_cent_chain(*d_nact, act, x, cent);
+}
+
+// The same centroid for every root of a forest: block r takes root r, whose
+// active slots are fact[roots[r].z .. roots[r].z + roots[r].w).
+__global__ void __launch_bounds__(512) k_forest_root_cent(int nroots, const int4 *__restrict__ roots,
+                                                          const int *__restrict__ fact,
+                                                          const double *__restrict__ x,
+                                                          const int *__restrict__ ctl,
+                                                          double *cent) {
+  if (ctl[CTL_OVERFLOW]) return;
+  for (int r = blockIdx.x; r < nroots; r += gridDim.x) {
+    const int4 R = roots[r];
+    if (R.w > 0) root_cent_chain(R.w, fact + R.z, x, cent + 3 * r);
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------ walk packs
 __device__ __forceinline__ void split2(double v, float &h, float &l) {
   h = __double2float_rn(v);
   l = __double2float_rn(v - (double)h);
 }
 
-__device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
+__device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
                           const double *__restrict__ circ, const double *__restrict__ C,
                           const int *__restrict__ count, const int *__restrict__ child_first,
@@ -528,7 +547,7 @@ __device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
                           WPay32 *p32);
 
-__global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int n_slots,
+__global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nroots,
                              const double *__restrict__ pos,
                              const double *__restrict__ width, const double *__restrict__ cent,
                              const double *__restrict__ circ, const double *__restrict__ C,
@@ -541,11 +560,11 @@ __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int n_s
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
-    pack_node(k, n_slots, pos, width, cent, circ, C, count, child_first, nchild, first, x, gi, inf,
+    pack_node(k, nroots, pos, width, cent, circ, C, count, child_first, nchild, first, x, gi, inf,
               beh, theta, extra, w64, p64, w32, p32);
 }
 
-__device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
+__device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
                           const double *__restrict__ circ, const double *__restrict__ C,
                           const int *__restrict__ count, const int *__restrict__ child_first,
@@ -563,7 +582,9 @@ __device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
   double g1 = __dsub_rn(h.cy, __dadd_rn(pos[3 * k + 1], hw));
   double g2 = __dsub_rn(h.cz, __dadd_rn(pos[3 * k + 2], hw));
   h.geo = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(g0, g0), __dmul_rn(g1, g1)), __dmul_rn(g2, g2)));
-  int cnt = k == 0 ? n_slots : count[k];
+  // a root's count is its system's slot count, empty slots included
+  const bool root = k < nroots;
+  int cnt = count[k];
   h.count = cnt;
   h.child_first = child_first[k];
   h.nchild = nchild[k];
@@ -586,7 +607,7 @@ __device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
   // margin and falls back to the FP64 expression near the threshold.  The root
   // (centroid anywhere, zero moments) always takes the FP64 path.
   bool fast = theta > 0. && (!extra || theta < 1.15);
-  if (k == 0 || !fast) {
+  if (root || !fast) {
     h32.rc2 = -1.f;
   } else {
     double rc = (extra ? h.geo : 0.) + h.width / theta;
@@ -608,8 +629,8 @@ __device__ void pack_node(int k, int n_slots, const double *__restrict__ pos,
     for (int c = 0; c < 3; c++) r.C[c] = __double2float_rn(q.b[c] - q.a[c]);
   } else {
     const double *M = C + 9 * k;
-    for (int c = 0; c < 3; c++) q.a[c] = k == 0 ? 0. : circ[3 * k + c];
-    if (k == 0) {
+    for (int c = 0; c < 3; c++) q.a[c] = root ? 0. : circ[3 * k + c];
+    if (root) {
       for (int c = 0; c < 9; c++) q.C[c] = 0.;
     } else {
       for (int c = 0; c < 9; c++) q.C[c] = M[c];
@@ -661,6 +682,51 @@ __global__ void k_build_init(double *pos, double *width, int *count, int *start,
   for (size_t q = tid; q < (size_t)n_slots; q += stride) {
     ord[q] = act[q];
     nodeA[q] = 0;
+  }
+  for (size_t q = tid; q < ncnt9; q += stride) cnt9[q] = 0;
+}
+
+// The same start for a forest of independent systems: root r is system r's
+// construct_tree root (corner -L/2, width L, pcount = the system's slots,
+// parray(1) = its first slot); the level-0 order is the forest's active slots
+// (each system's contiguous and ascending) and froot gives each position's root.
+__global__ void k_forest_init(int nroots, const int4 *__restrict__ roots, double *pos,
+                              double *width, int *count, int *start, int *parent,
+                              int *child_first, int *nchild, int *level, unsigned char *digit,
+                              unsigned char *cmask, int *first, double L, int n_fact, int *ctl,
+                              int *ord, const int *__restrict__ fact,
+                              const int *__restrict__ froot, int *nodeA, int *cnt9, size_t ncnt9) {
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t r = tid; r < (size_t)nroots; r += stride) {
+    const int4 R = roots[r];
+    pos[3 * r] = -L / 2.; pos[3 * r + 1] = -L / 2.; pos[3 * r + 2] = -L / 2.;
+    width[r] = L;
+    count[r] = R.y;
+    start[r] = R.z;
+    parent[r] = -1;
+    child_first[r] = -1;
+    nchild[r] = 0;
+    level[r] = 0;
+    digit[r] = 0xFF;
+    cmask[r] = 0;
+    first[r] = R.y > 0 ? R.x : -1;
+  }
+  if (tid == 0) {
+    int nsplit = 0;
+    for (int r = 0; r < nroots; r++) nsplit += roots[r].y > 1 ? 1 : 0;
+    ctl[CTL_NS] = nsplit;
+  }
+  for (size_t q = tid; q < CTL_SIZE; q += stride) {
+    if (q == CTL_NS) continue;
+    int v = 0;
+    if (q == CTL_NNODES) v = nroots;
+    else if (q == CTL_LVL + 1) v = nroots;
+    ctl[q] = v;
+  }
+  for (size_t q = tid; q < (size_t)n_fact; q += stride) {
+    ord[q] = fact[q];
+    nodeA[q] = froot[q];
   }
   for (size_t q = tid; q < ncnt9; q += stride) cnt9[q] = 0;
 }
@@ -795,12 +861,12 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
     QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
-    k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, t.count, t.rnk,
+    k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rnk,
                                                         t.ctl + CTL_NBIG);
     k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
         t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
         t.cent, t.circ, t.C, t.first);
-    k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, t.level, t.start,
+    k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, 1, t.level, t.start,
                                                            t.count, t.ord, t.cap_pts, c->x, c->gi,
                                                            t.cent, t.circ, t.C, t.first);
     QV_LAUNCH_CHECK(c);
@@ -811,7 +877,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaMemcpyAsync(t.cent, c->dscalar, 3 * sizeof(double), cudaMemcpyDeviceToDevice,
                                c->stream));
     k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
-        t.ctl, t.cap_nodes, n, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
+        t.ctl, t.cap_nodes, 1, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
         t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
         c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.p32);
     QV_LAUNCH_CHECK(c);
@@ -843,4 +909,69 @@ int qv_launch_tree_build(qv_ctx *c) {
     return QV_OK;
   }
   return qv_fail(c, QV_ERR_NOMEM, "tree build did not fit after repeated growth");
+}
+
+// ------------------------------------------------------------------ forest
+// Independent systems' trees built together: one root per system at level 0,
+// then the same level-synchronous kernel, moment chains and packs as a single
+// tree.  Nothing here waits for the host, so a step that contains the build can
+// be captured in a CUDA graph; capacities are reserved up front and an
+// overflow leaves CTL_OVERFLOW set for the caller to read.
+int qv_forest_reserve(qv_ctx *c, int n_fact, int cap_nodes) {
+  int rc;
+  if ((rc = qv_aux_streams(c))) return rc;
+  QV_CUDA(c, cudaFuncSetAttribute(k_forest_root_cent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  2 * RC * 3 * (int)sizeof(double)));
+  return tree_reserve(c, std::max(n_fact, 1), cap_nodes, QV_MAX_DEPTH + 1);
+}
+
+int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
+  TreeBuf &t = c->tree;
+  if (f.n_fact > t.cap_pts || t.cap_levels < QV_MAX_DEPTH + 1)
+    return qv_fail(c, QV_ERR_STATE, "forest build without reserved capacity");
+  k_forest_init<<<2 * c->sm_count, 256, 0, c->stream>>>(
+      f.nroots, f.roots, t.pos, t.width, t.count, t.start, t.parent, t.child_first, t.nchild,
+      t.level, t.digit, t.cmask, t.first, c->p.box_size, f.n_fact, t.ctl, t.ord, f.fact, f.froot,
+      t.nodeA, t.cnt9, 9 * (size_t)(2 * t.cap_pts + 2));
+  QV_LAUNCH_CHECK(c);
+  BuildArgs a;
+  a.d_nact = f.d_nfact; a.n_slots = f.n_fact; a.cap_pts = t.cap_pts; a.cap_nodes = t.cap_nodes;
+  a.cap_levels = t.cap_levels; a.nchunks = std::max(1, nblk(f.n_fact, CH));
+  a.x = c->x; a.gi = c->gi; a.pos = t.pos; a.width = t.width; a.count = t.count;
+  a.start = t.start; a.parent = t.parent; a.child_first = t.child_first; a.nchild = t.nchild;
+  a.level = t.level; a.digit = t.digit; a.cmask = t.cmask; a.ord = t.ord; a.nodeA = t.nodeA;
+  a.nodeB = t.nodeB; a.rnk = t.rnk; a.cnt9A = t.cnt9; a.cnt9B = t.cnt9 + 9 * (size_t)(t.cap_pts + 1);
+  a.rs9 = t.rs9; a.chunk9 = t.chunk9; a.ctl = t.ctl; a.dig = t.dig;
+  int grid = std::max(1, std::min(build_grid(c), std::max(1, a.nchunks) * 4));
+  // a cooperative launch written as a launch attribute, which stream capture
+  // records as a cooperative kernel node
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(BT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  QV_CUDA(c, cudaLaunchKernelEx(&cfg, k_build, a));
+  QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->stream));
+  k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
+                                                      t.ctl + CTL_NBIG);
+  k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->stream>>>(
+      t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
+      t.circ, t.C, t.first);
+  k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.level,
+                                                         t.start, t.count, t.ord, t.cap_pts, c->x,
+                                                         c->gi, t.cent, t.circ, t.C, t.first);
+  k_forest_root_cent<<<std::min(f.nroots, 2 * c->sm_count), 512, 2 * RC * 3 * sizeof(double),
+                       c->stream>>>(f.nroots, f.roots, f.fact, c->x, t.ctl, t.cent);
+  k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
+      t.ctl, t.cap_nodes, f.nroots, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
+      t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
+      c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.p32);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 7);
+  return QV_OK;
 }

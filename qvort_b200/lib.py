@@ -127,6 +127,14 @@ _SIGS = {
     "qv_read_var_file": [C.c_char_p, C.c_int, _I, _D, _P, _P, _P],
     "qv_write_var_file": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
     "qv_setup_loops": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
+    "qv_batch_create": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, C.POINTER(_P)],
+    "qv_batch_set_points": [_P, _P, _P, _P],
+    "qv_batch_velocity": [_P, _P],
+    "qv_batch_step": [_P, C.c_int],
+    "qv_batch_get_points": [_P, _P, _P],
+    "qv_batch_tune": [_P, C.c_int, _P, C.POINTER(C.c_float)],
+    "qv_batch_set_config": [_P, C.c_int, C.c_int, C.c_int],
+    "qv_batch_stats": [_P, _P, _I, _P],
 }
 for _name, _args in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -134,8 +142,12 @@ for _name, _args in _SIGS.items():
     _f.restype = C.c_int
 _lib.qv_last_error.argtypes = [_P]
 _lib.qv_last_error.restype = C.c_char_p
+_lib.qv_batch_last_error.argtypes = [_P]
+_lib.qv_batch_last_error.restype = C.c_char_p
+_lib.qv_batch_destroy.argtypes = [_P]
+_lib.qv_batch_destroy.restype = None
 
-EXPORTED = tuple(_SIGS) + ("qv_last_error",)
+EXPORTED = tuple(_SIGS) + ("qv_last_error", "qv_batch_last_error", "qv_batch_destroy")
 
 
 def lib() -> C.CDLL:
@@ -411,3 +423,81 @@ def probe_fp32(stream: int | None = None) -> float:
     if rc < 0:
         raise QvError(rc, "qv_probe_fp32 failed")
     return t.value
+
+
+class Batch:
+    """Independent open systems advanced together (a qv_batch).
+
+    systems: list of (x (n, 3), infront, behind) with each system's own 1-based
+    links; method[s] "BS" or "Tree"; dt[s] per system."""
+
+    def __init__(self, params: QvParams, systems, method, dt, stream: int | None = None):
+        self.params = params
+        self.sizes = [len(sx[0]) for sx in systems]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int32)
+        meth = np.array([VELOCITY[m] if isinstance(m, str) else int(m) for m in method], np.int32)
+        dts = np.asarray(dt, np.float64)
+        h = C.c_void_p()
+        rc = _lib.qv_batch_create(C.byref(params), len(systems), _ptr(self.offsets), _ptr(meth),
+                                  _ptr(dts), stream, C.byref(h))
+        if rc < 0:
+            raise QvError(rc, "qv_batch_create failed")
+        self._h = h
+        self.ntot = int(self.offsets[-1])
+        x = _f64(np.concatenate([sx[0] for sx in systems]))
+        inf = _i32(np.concatenate([sx[1] for sx in systems]))
+        beh = _i32(np.concatenate([sx[2] for sx in systems]))
+        self._check(_lib.qv_batch_set_points(self._h, _ptr(x), _ptr(inf), _ptr(beh)))
+
+    def _check(self, rc: int):
+        if rc < 0:
+            raise QvError(rc, _lib.qv_batch_last_error(self._h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.qv_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def split(self, a: np.ndarray):
+        return [a[self.offsets[s]:self.offsets[s + 1]] for s in range(len(self.sizes))]
+
+    def velocity(self) -> np.ndarray:
+        u = np.empty((self.ntot, 3))
+        self._check(_lib.qv_batch_velocity(self._h, _ptr(u)))
+        return u
+
+    def step(self, nsteps: int = 1):
+        self._check(_lib.qv_batch_step(self._h, int(nsteps)))
+
+    def get_points(self):
+        x = np.empty((self.ntot, 3))
+        u = np.empty((self.ntot, 3))
+        self._check(_lib.qv_batch_get_points(self._h, _ptr(x), _ptr(u)))
+        return x, u
+
+    def tune(self, reps: int = 3):
+        cfg = np.zeros(3, np.int32)
+        ms = C.c_float()
+        self._check(_lib.qv_batch_tune(self._h, reps, _ptr(cfg), C.byref(ms)))
+        return dict(warps_per_block=int(cfg[0]), blocks_per_sm=int(cfg[1]), order=int(cfg[2]),
+                    work_ms=ms.value)
+
+    def set_config(self, warps_per_block: int, blocks_per_sm: int, order: int):
+        self._check(_lib.qv_batch_set_config(self._h, warps_per_block, blocks_per_sm, order))
+
+    def stats(self) -> dict:
+        ev = np.zeros(2, np.int64)
+        g = C.c_int()
+        cfg = np.zeros(8, np.int32)
+        self._check(_lib.qv_batch_stats(self._h, _ptr(ev), C.byref(g), _ptr(cfg)))
+        keys = ("warps_per_block", "blocks_per_sm", "order", "stack", "items", "tree_systems",
+                "depth", "launches")
+        return dict(leaf_evals=int(ev[0]), far_evals=int(ev[1]), graph=bool(g.value),
+                    **{k: int(v) for k, v in zip(keys, cfg)})
