@@ -123,6 +123,25 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def job_time_ms(ms_local: float, ws: int, device="cuda") -> float:
+    """The job's time for the timed region: the maximum over ranks of each
+    rank's device-timed milliseconds (every rank calls this, in the same order)."""
+    if ws <= 1:
+        return ms_local
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(units_per_step: float, ms_per_step: float, ws: int) -> float:
+    """Whole-job throughput: every rank runs an independent replica of the
+    step, so the job processes ws times the units of one replica."""
+    return ws * units_per_step / (ms_per_step * 1e-3)
+
+
 def workload(seed: int):
     from qvort_b200 import workloads as W
 
@@ -257,14 +276,11 @@ def our_arm(args):
     torch.cuda.synchronize()
     clk = clocks.stop(t_wall0, time.time())
     launches = ctx.counters()["launches"] - launches0
-    ms_total = sum(a.elapsed_time(b) for a, b in evs)
+    ms_total = job_time_ms(sum(a.elapsed_time(b) for a, b in evs), ws)
     if ws > 1:
-        t = torch.tensor([ms_total], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
         torch.distributed.barrier()
     ms_step = ms_total / args.steps
-    value = ws * pairs_step / (ms_step * 1e-3)
+    value = job_value(pairs_step, ms_step, ws)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,

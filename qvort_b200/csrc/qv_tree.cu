@@ -179,20 +179,41 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
     grid.sync();
 
     // ---- P2: children (all blocks), chunk prefix scan (block 0)
-    for (int k = ls + blockIdx.x * BT + threadIdx.x; k < le; k += gridDim.x * BT) {
-      if (a.count[k] < 2) { a.nchild[k] = 0; a.cmask[k] = 0; continue; }
+    // Child slots are claimed with one atomic per warp (the warp's node counts
+    // prefix-summed with shuffles); ids within a level carry no meaning beyond
+    // contiguity, so their order does not matter.
+    for (int kb = ls + blockIdx.x * BT; kb < le; kb += gridDim.x * BT) {
+      const int k = kb + threadIdx.x;
+      const int lane = threadIdx.x & 31;
+      const bool split = k < le && a.count[k] >= 2;
+      if (k < le && !split) { a.nchild[k] = 0; a.cmask[k] = 0; }
       int c9[9];
       int nc = 0, nsp = 0;
       unsigned mask = 0;
-      for (int g = 0; g < 9; g++) c9[g] = cntc[(k - ls) * 9 + g];
-      for (int g = 0; g < 8; g++)
-        if (c9[g] > 0) { nc++; mask |= 1u << g; if (c9[g] >= 2) nsp++; }
-      int base = atomicAdd((int *)&ctl[CTL_NNODES], nc);
+      if (split) {
+        for (int g = 0; g < 9; g++) c9[g] = cntc[(k - ls) * 9 + g];
+        for (int g = 0; g < 8; g++)
+          if (c9[g] > 0) { nc++; mask |= 1u << g; if (c9[g] >= 2) nsp++; }
+      }
+      int inc = nc, isp = nsp;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, inc, o);
+        int u = __shfl_up_sync(0xffffffffu, isp, o);
+        if (lane >= o) { inc += t; isp += u; }
+      }
+      int wbase = 0;
+      if (lane == 31) {
+        if (inc) wbase = atomicAdd((int *)&ctl[CTL_NNODES], inc);
+        if (isp) atomicAdd((int *)&ctl[CTL_NS + d + 1], isp);
+      }
+      wbase = __shfl_sync(0xffffffffu, wbase, 31);
+      if (!split) continue;
+      const int base = wbase + inc - nc;
       if (base + nc > a.cap_nodes) {
         ctl[CTL_OVERFLOW] = 1;
         continue;
       }
-      if (nsp) atomicAdd((int *)&ctl[CTL_NS + d + 1], nsp);
       a.child_first[k] = base;
       a.nchild[k] = nc;
       a.cmask[k] = (unsigned char)mask;
@@ -337,9 +358,35 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
+  // one-point nodes (most of a tree): one thread each, the 15 chains of a
+  // single point with the same roundings as the warp path below
+  for (int kl = k0 + blockIdx.x * blockDim.x + threadIdx.x; kl < n_nodes;
+       kl += gridDim.x * blockDim.x) {
+    if (count[kl] != 1) continue;
+    const int idx = ord[(size_t)level[kl] * cap_pts + start[kl]];
+    double X[3], G[3], cm[3], ci[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      cm[c] = __ddiv_rn(__dadd_rn(0., X[c]), 1.);
+      ci[c] = __dsub_rn(__dadd_rn(0., G[c]), X[c]);
+      cent[3 * kl + c] = cm[c];
+      circ[3 * kl + c] = ci[c];
+    }
+#pragma unroll
+    for (int mm = 0; mm < 3; mm++)
+#pragma unroll
+      for (int kk = 0; kk < 3; kk++) {
+        double acc = __dadd_rn(0., __dmul_rn(X[mm], __dsub_rn(G[kk], X[kk])));
+        C[9 * kl + 3 * mm + kk] = __dsub_rn(acc, __dmul_rn(cm[mm], ci[kk]));
+      }
+    first[kl] = idx;
+  }
+  // nodes of 2..BIGN points: one warp per node
   for (int k = k0 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
     int s = start[k], n = count[k];
-    if (n > BIGN) continue;
+    if (n < 2 || n > BIGN) continue;
     const int *o = ord + (size_t)level[k] * cap_pts + s;
     double acc = 0.;
     for (int base = 0; base < n; base += 32) {
