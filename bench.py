@@ -50,8 +50,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--suite", default="tangle", choices=["tangle", "batch", "gradient"],
-                    help="tangle: the headline line; batch / gradient: only that workload's entry")
+    ap.add_argument("--suite", default="tangle", choices=["tangle", "batch", "gradient", "large"],
+                    help="tangle: the headline line; batch / gradient / large: only that "
+                         "workload's entry")
     ap.add_argument("--quick", action="store_true",
                     help="headline timing only (no comparators, e2e or CPU baseline)")
     return ap.parse_args()
@@ -458,6 +459,49 @@ def gradient_rate(L, torch, steps: int = 256, reps: int = 2) -> dict:
                         "loss = E(x_K) + sum |x_K - x_0|^2; wall clock"}
 
 
+def large_rate(L, torch, steps: int = 5, warmup: int = 3) -> dict:
+    """The large isotropic tangle: 3000 random rings, R ~ U(0.004, 0.015) cm,
+    delta 3e-4 cm, periodic L = 0.1, Barnes-Hut theta 0.5, candidate search every
+    step.  Mixed and FP64 steps timed with CUDA events (inputs far above L2), and
+    the mixed velocity's error against the FP64 velocity on every target."""
+    from qvort_b200 import workloads as W
+
+    w = W.large_tangle()
+    n = w.n
+    out = {"workload": f"3000 rings, N={n}, periodic L=0.1, Tree theta 0.5, AB, dt 1e-7",
+           "n_points": n}
+    stream = torch.cuda.Stream()
+    vel = {}
+    for prec in ("mixed", "fp64"):
+        c = L.Context(L.default_params(**dict(w.params, precision=prec)), stream=stream.cuda_stream)
+        c.set_points(w.x, w.infront, w.behind)
+        vel[prec] = c.velocity(False)[0]
+        it = 0
+        for _ in range(max(1, warmup)):
+            it += 1
+            c.step(it)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(steps):
+                it += 1
+                c.step(it)
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        cnt = c.counters()
+        out[prec] = {"ms_per_step": ms, "pairs_per_s": float(n) * n * 27 / (ms * 1e-3),
+                     "leaf_evals": cnt["leaf_evals"], "far_evals": cnt["far_evals"]}
+        c.close()
+    rms, mx = _rel(vel["mixed"], vel["fp64"])
+    out["error"] = {"mixed_vs_fp64_bh_rms_rel": rms, "mixed_vs_fp64_bh_max_rel": mx,
+                    "targets": n}
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
+
+
 def batch_rate(L, torch, steps: int = 20) -> dict:
     """512 independent open systems (rings and leap-frogging pairs, N log-uniform
     in [100, 8000], dt from {5e-8, 1e-7, 2e-7}, direct below 2000 points,
@@ -523,7 +567,12 @@ def main():
 
         from qvort_b200 import lib as L
 
-        r = batch_rate(L, torch, args.steps) if args.suite == "batch" else gradient_rate(L, torch)
+        if args.suite == "batch":
+            r = batch_rate(L, torch, args.steps)
+        elif args.suite == "large":
+            r = large_rate(L, torch, args.steps, args.warmup)
+        else:
+            r = gradient_rate(L, torch)
         print(json.dumps({"suite": args.suite, **r}), flush=True)
         return 0
     return our_arm(args)
