@@ -65,6 +65,10 @@ typedef struct qv_params {
   int precision;              /* QV_PREC_* */
   int runge_kutta;            /* runge_kutta */
   int recon_shots;            /* recon_shots, default 1 */
+  int line_ops;               /* 1: qv_step also runs pinsert after the update and premove
+                                 after the candidate search (the loop of src/run.f90:59-72
+                                 with switch_off_recon true); 0 (default): both left to
+                                 the caller (qv_pinsert, qv_premove) */
 } qv_params;
 
 typedef struct qv_ctx qv_ctx;
@@ -188,14 +192,32 @@ int qv_setup_loops(const char *initf, int pcount, double delta, double *x, int *
 
 /* Block until the context's stream is idle. */
 int qv_sync(qv_ctx *ctx);
+/* Line operations (replacing `call pinsert` / `call premove`, src/run.f90:59, 72).
+ * pinsert (src/line.f90:18-106; delta_adapt and mirror off): points inserted
+ * where the distance to the infront ghost exceeds delta, in the reference's
+ * slot order, on the stored ghosts (those of the last ghost gather, as after
+ * pmotion).  Empty slots are filled first (minloc), then slots are appended:
+ * the slot count can grow (qv_point_count).  *inserted may be NULL. */
+int qv_pinsert(qv_ctx *ctx, int *inserted);
+/* premove (src/line.f90:112-161; phonon emission and recon_info off) with
+ * loop_killer (src/reconnection.f90:421-461): the point infront of i goes when
+ * |x_i - x_infront(infront(i))| < 0.998 delta; loops left with fewer than 5
+ * points are cleared.  *removed (may be NULL) counts both. */
+int qv_premove(qv_ctx *ctx, int *removed);
+/* Current slot count (pcount), which pinsert can raise, and the links of all
+ * slots (1-based, 0 = empty slot; the f(:)%infront, f(:)%behind a host
+ * scatters back after insertion or removal). */
+int qv_point_count(qv_ctx *ctx, int *n);
+int qv_get_links(qv_ctx *ctx, int *infront, int *behind);
 
 /* Instrumentation (no reference counterpart beyond the seg_fault trace flags,
  * src/run.f90:31-166, and eval_counter, src/tree.f90:40).  With profiling on,
  * the phases below are bracketed by CUDA events on the context's stream and
  * their device times accumulate into ms[QV_NPHASES]. */
-/* ghosts, tree build, local term, non-local sum, update, search, wrap, and two
- * parts of the tree build: the level-synchronous construction and the moments */
-#define QV_NPHASES 9
+/* ghosts, tree build, local term, non-local sum, update, search, wrap, two
+ * parts of the tree build (the level-synchronous construction and the
+ * moments), and the line operations (pinsert, premove) */
+#define QV_NPHASES 10
 int qv_profile(qv_ctx *ctx, int enable);
 int qv_phase_times(qv_ctx *ctx, double *ms, int reset);
 /* Kernel launches issued by this context so far, and the leaf / far-field

@@ -85,6 +85,8 @@ def lib() -> C.CDLL:
         _lib.qo_dt_max.argtypes = [P]
         _lib.qo_dt_max.restype = C.c_double
         _lib.qo_set_depth_cap.argtypes = [C.c_int]
+        _lib.qo_pinsert.argtypes = [P, C.POINTER(C.c_int), C.c_int, C.POINTER(QoState)]
+        _lib.qo_premove.argtypes = [P, C.c_int, C.POINTER(QoState)]
     return _lib
 
 
@@ -210,6 +212,52 @@ class State:
                            _p(self.closestd) if search else None, C.byref(ev), nthreads)
         self.evals = ev.value
         return st
+
+
+class QoState(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("x", "u", "u1", "u2", "u3", "gi", "gb", "gii", "gbb",
+                                          "u_li", "u_bs", "closestd", "infront", "behind",
+                                          "closest")]
+
+
+LINE_FIELDS = {"x": 3, "u": 3, "u1": 3, "u2": 3, "u3": 3, "gi": 3, "gb": 3, "gii": 3, "gbb": 3,
+               "u_li": 3, "u_bs": 3, "closestd": 1, "infront": 0, "behind": 0, "closest": 0}
+
+
+def line_state(n: int, cap: int, **arrays):
+    """Arrays of cap slots for pinsert/premove, the first n filled from `arrays`
+    (missing fields zero)."""
+    st = {}
+    for k, w in LINE_FIELDS.items():
+        if w == 0:
+            a = np.zeros(cap, np.int32)
+        elif w == 1:
+            a = np.zeros(cap)
+        else:
+            a = np.zeros((cap, 3))
+        if k in arrays:
+            a[:n] = arrays[k]
+        st[k] = a
+    return st
+
+
+def _qostate(st) -> QoState:
+    return QoState(*[st[k].ctypes.data_as(C.c_void_p) for k in LINE_FIELDS])
+
+
+def pinsert(p: QoParams, n: int, st) -> tuple[int, int]:
+    """pinsert on the state dict in place; returns (new pcount, points inserted)."""
+    cap = st["x"].shape[0]
+    pc = C.c_int(n)
+    k = lib().qo_pinsert(C.byref(p), C.byref(pc), cap, C.byref(_qostate(st)))
+    if k < 0:
+        raise RuntimeError("pinsert needs more than cap slots")
+    return pc.value, k
+
+
+def premove(p: QoParams, n: int, st) -> int:
+    """premove on the state dict in place; returns the points removed."""
+    return lib().qo_premove(C.byref(p), n, C.byref(_qostate(st)))
 
 
 def dt_max(p: QoParams) -> float:

@@ -810,3 +810,139 @@ double qo_dt_max(const qo_params *p) {
 }
 
 void qo_set_depth_cap(int cap) { g_depth_cap = cap; }
+
+/* ------------------------------------------------ insertion and removal */
+/* The point state the line operations read and write (arrays of cap slots). */
+typedef struct {
+  double *x, *u, *u1, *u2, *u3, *gi, *gb, *gii, *gbb, *u_li, *u_bs, *closestd;
+  int *infront, *behind, *closest;
+} qo_state;
+
+/* get_ghost_p for one slot, src/periodic.f90:23-165 */
+static void ghost_one(const qo_params *p, int i, const qo_state *S) {
+  int a = S->infront[i] - 1, b = S->behind[i] - 1;
+  int aa = S->infront[a] - 1, bb = S->behind[b] - 1;
+  double *G[4] = {S->gi + 3 * i, S->gb + 3 * i, S->gii + 3 * i, S->gbb + 3 * i};
+  int src[4] = {a, b, aa, bb};
+  for (int k = 0; k < 4; k++)
+    for (int c = 0; c < 3; c++) G[k][c] = S->x[3 * src[k] + c];
+  int lo = 3;
+  if (p->boundary == 1) lo = 0;
+  else if (p->boundary == 2) lo = 1;
+  else if (p->boundary == 3) lo = 2;
+  for (int axis = lo; axis < 3; axis++)
+    for (int k = 0; k < 4; k++) unwrap(p, S->x + 3 * i, G[k], axis);
+}
+
+/* clear_particle, src/general.f90:11-22 (u3, delta and t_recon are kept) */
+static void clear_particle(qo_state *S, int i) {
+  for (int c = 0; c < 3; c++) {
+    S->x[3 * i + c] = 0.; S->u[3 * i + c] = 0.; S->u1[3 * i + c] = 0.; S->u2[3 * i + c] = 0.;
+    S->gi[3 * i + c] = 0.; S->gb[3 * i + c] = 0.; S->gii[3 * i + c] = 0.; S->gbb[3 * i + c] = 0.;
+    S->u_li[3 * i + c] = 0.; S->u_bs[3 * i + c] = 0.;
+  }
+  S->infront[i] = 0; S->behind[i] = 0;
+  S->closest[i] = 0; S->closestd[i] = 0.;
+}
+
+/* pinsert, src/line.f90:18-106 (delta_adapt, mirror and particles_only off).
+ * *pcount grows by the points appended past the last slot; returns the number
+ * of points inserted, or -1 when more than cap slots would be needed.  The
+ * ghosts read are the stored ones (computed before the move, refreshed only
+ * for the slots an insertion touches), as in the reference.  A slot appended
+ * to the array gets u3 = 0, closest = 0 and zero velocities (the reference
+ * leaves those components of a new array element undefined; none of them
+ * enters a result before it is overwritten). */
+int qo_pinsert(const qo_params *p, int *pcount, int cap, qo_state *S) {
+  int old_pcount = *pcount, inserted = 0;
+  for (int i = 0; i < old_pcount; i++) {
+    if (S->infront[i] == 0) continue;
+    double disti = dist_gen(S->x + 3 * i, S->gi + 3 * i);
+    if (disti > 1. * p->delta) {
+      int par_new = -1;
+      for (int k = 0; k < *pcount; k++)
+        if (S->infront[k] == 0) { par_new = k; break; }   /* minloc(f(:)%infront) */
+      if (par_new < 0) {
+        if (*pcount >= cap) return -1;
+        par_new = *pcount;
+        *pcount = *pcount + 1;
+        for (int c = 0; c < 3; c++) {
+          S->u3[3 * par_new + c] = 0.; S->u_li[3 * par_new + c] = 0.; S->u_bs[3 * par_new + c] = 0.;
+        }
+        S->closest[par_new] = 0; S->closestd[par_new] = 0.;
+      }
+      double fdd[3];
+      deriv2(p, S->x + 3 * i, S->gi + 3 * i, S->gb + 3 * i, S->gii + 3 * i, S->gbb + 3 * i, fdd);
+      double curv = sqrt(dot3(fdd, fdd));
+      double *xn = S->x + 3 * par_new;
+      const double *xi = S->x + 3 * i, *gi = S->gi + 3 * i;
+      if (curv > 1E-5) {
+        curv = 1. / curv;
+        if (curv * curv - 0.25 * (disti * disti) > 0.) {
+          double f = (sqrt(curv * curv - 0.25 * (disti * disti)) - curv) * curv;
+          for (int c = 0; c < 3; c++) xn[c] = 0.5 * (xi[c] + gi[c]) + f * fdd[c];
+        } else {
+          for (int c = 0; c < 3; c++) xn[c] = 0.5 * (xi[c] + gi[c]);
+        }
+      } else {
+        for (int c = 0; c < 3; c++) xn[c] = 0.5 * (xi[c] + gi[c]);
+      }
+      int a = S->infront[i] - 1;
+      for (int c = 0; c < 3; c++) {
+        S->u[3 * par_new + c] = 0.5 * (S->u[3 * i + c] + S->u[3 * a + c]);
+        S->u1[3 * par_new + c] = 0.;
+        S->u2[3 * par_new + c] = 0.;
+      }
+      S->behind[par_new] = i + 1;
+      S->infront[par_new] = S->infront[i];
+      ghost_one(p, par_new, S);
+      S->behind[a] = par_new + 1;
+      ghost_one(p, a, S);
+      S->infront[i] = par_new + 1;
+      ghost_one(p, i, S);
+      inserted++;
+    }
+  }
+  return inserted;
+}
+
+/* loop_killer, src/reconnection.f90:421-461: a loop of fewer than 5 points
+ * is cleared (the log of small loops is output only). */
+static int loop_killer(qo_state *S, int pcount, int particle) {
+  int counter = 1, next = particle;
+  for (int k = 0; k < pcount; k++) {
+    next = S->infront[next] - 1;
+    if (next == particle || next < 0) break;  /* next < 0: a cleared slot (a broken loop) */
+    counter++;
+  }
+  if (counter >= 5) return 0;
+  next = particle;
+  for (int k = 0; k < pcount; k++) {
+    int store_next = S->infront[next] - 1;
+    clear_particle(S, next);
+    next = store_next;
+    if (next == particle || next < 0) break;
+  }
+  return counter;
+}
+
+/* premove, src/line.f90:112-161 (mirror, phonon emission and recon_info off;
+ * every point's delta factor is 1, as pinsert leaves it).  distf is taken on
+ * raw positions, without periodic unwrapping, as in the reference.  Returns
+ * the number of points removed (loops cleared by loop_killer included). */
+int qo_premove(const qo_params *p, int pcount, qo_state *S) {
+  int removed = 0;
+  for (int i = 0; i < pcount; i++) {
+    if (S->infront[i] == 0) continue;
+    int a = S->infront[i] - 1, aa = S->infront[a] - 1;
+    const double *xi = S->x + 3 * i, *xj = S->x + 3 * aa;
+    double distii = sqrt(sq(xi[0] - xj[0]) + sq(xi[1] - xj[1]) + sq(xi[2] - xj[2]));
+    if (distii < .499 * p->delta * (1. + 1.)) {
+      S->behind[aa] = i + 1;
+      S->infront[i] = aa + 1;
+      clear_particle(S, a);
+      removed += 1 + loop_killer(S, pcount, i);
+    }
+  }
+  return removed;
+}

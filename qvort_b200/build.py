@@ -35,7 +35,7 @@ def _nvcc() -> str:
 # Per-file extra flags.  The per-point kernels (ghosts, LIA finite differences,
 # Adams-Bashforth, energy) follow the reference's FP64 operation order with one
 # rounding per operation, so FMA contraction is switched off there.
-FILE_FLAGS = {"qv_points.cu": ["--fmad=false"]}
+FILE_FLAGS = {"qv_points.cu": ["--fmad=false"], "qv_line.cu": ["--fmad=false"]}
 
 
 def sources() -> list[Path]:

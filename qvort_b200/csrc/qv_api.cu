@@ -34,6 +34,8 @@ static int validate(qv_ctx *c, const qv_params *p) {
   if (p->boundary != QV_BC_OPEN && !(p->box_size > 0))
     return qv_fail(c, QV_ERR_ARG, "periodic boundaries need a positive box size");
   if (p->recon_shots < 1) return qv_fail(c, QV_ERR_ARG, "recon_shots must be >= 1");
+  if (p->line_ops != 0 && p->line_ops != 1) return qv_fail(c, QV_ERR_ARG, "line_ops must be 0 or 1");
+  if (p->line_ops && !(p->delta > 0)) return qv_fail(c, QV_ERR_ARG, "line operations need delta > 0");
   return QV_OK;
 }
 
@@ -54,6 +56,7 @@ extern "C" int qv_default_params(qv_params *p) {
   p->precision = QV_PREC_FP64;
   p->runge_kutta = 0;
   p->recon_shots = 1;
+  p->line_ops = 0;
   return QV_OK;
 }
 
@@ -182,6 +185,52 @@ static int reserve_points(qv_ctx *c, int n) {
   return QV_OK;
 }
 
+// Grow the slot capacity to new_cap keeping the first n slots of every point
+// array (insertion appends slots past the last one, as pinsert's array
+// resize does, src/line.f90:56-66).
+int qv_grow_points(qv_ctx *c, int new_cap) {
+  if (new_cap <= c->cap) return QV_OK;
+  const size_t n = (size_t)c->n, m = (size_t)new_cap;
+  double **dv[] = {&c->x, &c->u, &c->u1, &c->u2, &c->u3, &c->gi, &c->gb, &c->gii, &c->gbb,
+                   &c->u_li, &c->u_bs};
+  int **iv[] = {&c->infront, &c->behind, &c->closest};
+  for (double **q : dv) {
+    double *d = nullptr;
+    QV_CUDA(c, cudaMalloc((void **)&d, sizeof(double) * 3 * m));
+    QV_CUDA(c, cudaMemsetAsync(d, 0, sizeof(double) * 3 * m, c->stream));
+    if (*q && n) QV_CUDA(c, cudaMemcpyAsync(d, *q, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, c->stream));
+    QV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*q) cudaFree(*q);
+    *q = d;
+  }
+  {
+    double *d = nullptr;
+    QV_CUDA(c, cudaMalloc((void **)&d, sizeof(double) * m));
+    QV_CUDA(c, cudaMemsetAsync(d, 0, sizeof(double) * m, c->stream));
+    if (c->closestd && n) QV_CUDA(c, cudaMemcpyAsync(d, c->closestd, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    QV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->closestd) cudaFree(c->closestd);
+    c->closestd = d;
+  }
+  for (int **q : iv) {
+    int *d = nullptr;
+    QV_CUDA(c, cudaMalloc((void **)&d, sizeof(int) * m));
+    QV_CUDA(c, cudaMemsetAsync(d, 0, sizeof(int) * m, c->stream));
+    if (*q && n) QV_CUDA(c, cudaMemcpyAsync(d, *q, sizeof(int) * n, cudaMemcpyDeviceToDevice, c->stream));
+    QV_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (*q) cudaFree(*q);
+    *q = d;
+  }
+  // scratch sized by the capacity (contents not kept)
+  int rc;
+  if ((rc = qv_grow(c, (void **)&c->act, sizeof(int) * m))) return rc;
+  if ((rc = qv_grow(c, (void **)&c->src64, sizeof(double) * 8 * m))) return rc;
+  if ((rc = qv_grow(c, (void **)&c->src32, sizeof(float) * 16 * m))) return rc;
+  if ((rc = qv_grow(c, (void **)&c->blkcnt, sizeof(int) * (m / 256 + 4)))) return rc;
+  c->cap = new_cap;
+  return QV_OK;
+}
+
 static int set_points_impl(qv_ctx *c, int n, const double *x, const int *inf, const int *beh,
                            cudaMemcpyKind kind) {
   if (n < 0 || (n > 0 && (!x || !inf || !beh))) return qv_fail(c, QV_ERR_ARG, "bad points");
@@ -199,6 +248,7 @@ static int set_points_impl(qv_ctx *c, int n, const double *x, const int *inf, co
     QV_CUDA(c, cudaMemsetAsync(c->closestd, 0, sizeof(double) * n, c->stream));
   }
   c->ghosts_valid = false;
+  c->ghosts_stored = false;
   c->tree.valid = false;
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
   return QV_OK;
@@ -525,10 +575,20 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
     qv_phase_end(c, PH_UPDATE);
     c->ghosts_valid = false;
   }
+  if (c->p.line_ops) {                                           // run.f90:59
+    qv_phase_begin(c, PH_LINE);
+    if ((rc = qv_line_insert(c, nullptr))) return rc;
+    qv_phase_end(c, PH_LINE);
+  }
   if (itime % c->p.recon_shots == 0) {                           // run.f90:63-69
     qv_phase_begin(c, PH_CLOSEST);
     if ((rc = qv_launch_closest(c))) return rc;
     qv_phase_end(c, PH_CLOSEST);
+    if (c->p.line_ops) {                                         // run.f90:72
+      qv_phase_begin(c, PH_LINE);
+      if ((rc = qv_line_remove(c, nullptr))) return rc;
+      qv_phase_end(c, PH_LINE);
+    }
   }
   qv_phase_begin(c, PH_WRAP);
   if ((rc = qv_launch_ghosts(c))) return rc;                     // run.f90:75
@@ -536,6 +596,34 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
   qv_phase_end(c, PH_WRAP);
   c->ghosts_valid = false;
   return velocity_collect(c, nullptr);  // one wait per step; reports any status
+}
+
+extern "C" int qv_pinsert(qv_ctx *c, int *inserted) {
+  QV_CHECK_CTX(c);
+  if (!(c->p.delta > 0)) return qv_fail(c, QV_ERR_ARG, "pinsert needs delta > 0");
+  return qv_line_insert(c, inserted);
+}
+
+extern "C" int qv_premove(qv_ctx *c, int *removed) {
+  QV_CHECK_CTX(c);
+  if (!(c->p.delta > 0)) return qv_fail(c, QV_ERR_ARG, "premove needs delta > 0");
+  return qv_line_remove(c, removed);
+}
+
+extern "C" int qv_get_links(qv_ctx *c, int *infront, int *behind) {
+  QV_CHECK_CTX(c);
+  size_t v = sizeof(int) * (size_t)c->n;
+  if (infront && v) QV_CUDA(c, cudaMemcpyAsync(infront, c->infront, v, cudaMemcpyDeviceToHost, c->stream));
+  if (behind && v) QV_CUDA(c, cudaMemcpyAsync(behind, c->behind, v, cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+extern "C" int qv_point_count(qv_ctx *c, int *n) {
+  QV_CHECK_CTX(c);
+  if (!n) return QV_ERR_ARG;
+  *n = c->n;
+  return QV_OK;
 }
 
 extern "C" int qv_sync(qv_ctx *c) {

@@ -94,6 +94,7 @@ enum {
   PH_GHOSTS = 0, PH_BUILD, PH_LIA, PH_NONLOCAL, PH_UPDATE, PH_CLOSEST, PH_WRAP,
   PH_BUILD_LEVELS,   // inside PH_BUILD: init + the level-synchronous kernel
   PH_BUILD_MOMENTS,  // inside PH_BUILD: moment chains, root centroid join, packs
+  PH_LINE,           // pinsert / premove
   PH_N
 };
 
@@ -126,6 +127,10 @@ struct qv_ctx {
   double *walk_part = nullptr;          // per-image partial sums of the walk
   size_t walk_part_bytes = 0;
   bool ghosts_valid = false;
+  bool ghosts_stored = false;  // ghost arrays hold values (possibly from before a move)
+  // line operations (pinsert / premove): flag and list scratch, sequential state
+  void *line_flags = nullptr, *line_st = nullptr;
+  size_t line_cap = 0;
   TreeBuf tree;
   int sm_count = 148;
   // instrumentation
@@ -171,6 +176,14 @@ int qv_launch_wrap(qv_ctx *c);
 int qv_launch_closest(qv_ctx *c);
 int qv_launch_energy(qv_ctx *c, double *out_host);
 int qv_compact_active(qv_ctx *c);
+int qv_grow_points(qv_ctx *c, int new_cap);
+int qv_line_insert(qv_ctx *c, int *inserted);
+int qv_line_remove(qv_ctx *c, int *removed);
+// ordered compaction kernels (qv_direct.cu): counts of nonzero flags per
+// 256-slot block, their exclusive scan (total to *total), the scatter
+__global__ void k_count_active(int n, const int *__restrict__ inf, int *blk_cnt);
+__global__ void k_scan_small(int m, int *v, int *total);
+__global__ void k_scatter_active(int n, const int *__restrict__ inf, const int *blk_off, int *act);
 int qv_compact_active_async(qv_ctx *c);
 int qv_aux_streams(qv_ctx *c);
 

@@ -1,0 +1,395 @@
+// qv_line.cu -- the line operations that keep the resolution: pinsert
+// (src/line.f90:18-106) and premove with loop_killer (src/line.f90:112-161,
+// src/reconnection.f90:421-461).
+//
+// Both are sequential scans over the slots in ascending order whose effects
+// feed later iterations: an insertion takes the first empty slot (or appends
+// one), relinks, and refreshes the stored ghosts of three slots (the new
+// point, i, and i's old infront), and a later test of a refreshed slot sees
+// the new ghosts; a removal relinks i past its infront, which changes the test
+// of i's behind.  Tests on unaffected slots only read state that nothing
+// earlier changed.  So:
+//   * one parallel pass evaluates every slot's test and compacts the
+//     candidates (ascending), plus the empty slots for pinsert;
+//   * one device thread then runs the reference's loop over the candidates
+//     and the slots an earlier iteration touched (a small min-heap), each
+//     re-tested on the current state, with the reference's arithmetic.
+// Candidates are few per step (the resolution is maintained every step), so
+// the sequential part is short; its state lives in device memory and a run
+// that needs more slots than are allocated stops before the insertion that
+// needs them, so that the host can grow the arrays and resume it.
+//
+// Compiled without FMA contraction: positions are computed in the reference's
+// order of roundings (gfortran -O2 does not contract either).
+#include <algorithm>
+
+#include "qv_internal.cuh"
+#include "qv_lia.cuh"
+
+static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+#define LHEAP 8192  // slots waiting for a re-test (min-heap)
+
+struct LineState {
+  int nc, ne;        // candidates, empty slots (written by the compaction)
+  int pc, epos;      // next candidate, next empty slot
+  int n_old, n_cur;  // slot count at the start (loop bound), current slot count
+  int last;          // last slot processed
+  int heap_n;
+  int status;        // 1: more slots needed, 2: heap overflow
+  int done;          // points inserted / removed so far
+  int pad[6];
+  int heap[LHEAP];
+};
+
+// ------------------------------------------------------------- per slot
+__device__ __forceinline__ void ghost_one(int i, const double *__restrict__ x, const int *inf,
+                                          const int *beh, double *gi, double *gb, double *gii,
+                                          double *gbb, int lo_axis, double L) {
+  int a = inf[i], b = beh[i];
+  int aa = inf[a - 1], bb = beh[b - 1];
+  int src[4] = {a - 1, b - 1, aa - 1, bb - 1};
+  double *dst[4] = {gi, gb, gii, gbb};
+  double xi[3] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+  double h = L / 2.;
+  for (int k = 0; k < 4; k++)
+    for (int c = 0; c < 3; c++) {
+      double g = x[3 * src[k] + c];
+      if (c >= lo_axis) {
+        if ((xi[c] - g) > h)
+          g = g + L;
+        else if ((xi[c] - g) < (-h))
+          g = g - L;
+      }
+      dst[k][3 * i + c] = g;
+    }
+}
+
+struct LineArgs {
+  double *x, *u, *u1, *u2, *u3, *gi, *gb, *gii, *gbb, *u_li, *u_bs, *closestd;
+  int *inf, *beh, *closest;
+  int cap, lo_axis, order;
+  double L, delta, thr;
+  const int *cand, *empt;
+  int *flag_a, *flag_b;
+  LineState *st;
+};
+
+// clear_particle, src/general.f90:11-22 (u3 is kept)
+__device__ __forceinline__ void clear_slot(const LineArgs &a, int i) {
+  for (int c = 0; c < 3; c++) {
+    a.x[3 * i + c] = 0.; a.u[3 * i + c] = 0.; a.u1[3 * i + c] = 0.; a.u2[3 * i + c] = 0.;
+    a.gi[3 * i + c] = 0.; a.gb[3 * i + c] = 0.; a.gii[3 * i + c] = 0.; a.gbb[3 * i + c] = 0.;
+    a.u_li[3 * i + c] = 0.; a.u_bs[3 * i + c] = 0.;
+  }
+  a.inf[i] = 0;
+  a.beh[i] = 0;
+  a.closest[i] = 0;
+  a.closestd[i] = 0.;
+}
+
+__device__ __forceinline__ double seg_len(const double *a, const double *b) {
+  return lia_dist(a, b);  // dist_gen, src/derivatives.f90:79-86
+}
+
+// ------------------------------------------------------------ detection
+// pinsert's test on the stored ghosts (src/line.f90:41,49) and the empty slots.
+__global__ void k_ins_flags(int n, LineArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int act = a.inf[i] != 0;
+  a.flag_b[i] = !act;
+  a.flag_a[i] = act && seg_len(a.x + 3 * i, a.gi + 3 * i) > 1. * a.delta;
+}
+
+// premove's test: |x_i - x_infront(infront(i))| on raw positions (src/line.f90:131-137).
+__device__ __forceinline__ bool remove_test(const LineArgs &a, int i) {
+  int j = a.inf[a.inf[i] - 1] - 1;
+  const double *xi = a.x + 3 * i, *xj = a.x + 3 * j;
+  double d0 = xi[0] - xj[0], d1 = xi[1] - xj[1], d2 = xi[2] - xj[2];
+  return sqrt(d0 * d0 + d1 * d1 + d2 * d2) < a.thr;
+}
+
+__global__ void k_rem_flags(int n, LineArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a.flag_a[i] = a.inf[i] != 0 && remove_test(a, i);
+}
+
+// ------------------------------------------------------------- worklist
+__device__ void heap_push(LineState *s, int v) {
+  if (s->heap_n >= LHEAP) {
+    s->status = 2;
+    return;
+  }
+  int k = s->heap_n++;
+  s->heap[k] = v;
+  while (k > 0) {
+    int p = (k - 1) / 2;
+    if (s->heap[p] <= s->heap[k]) break;
+    int t = s->heap[p]; s->heap[p] = s->heap[k]; s->heap[k] = t;
+    k = p;
+  }
+}
+
+__device__ void heap_pop(LineState *s) {
+  s->heap[0] = s->heap[--s->heap_n];
+  int k = 0;
+  for (;;) {
+    int l = 2 * k + 1, r = l + 1, m = k;
+    if (l < s->heap_n && s->heap[l] < s->heap[m]) m = l;
+    if (r < s->heap_n && s->heap[r] < s->heap[m]) m = r;
+    if (m == k) break;
+    int t = s->heap[m]; s->heap[m] = s->heap[k]; s->heap[k] = t;
+    k = m;
+  }
+}
+
+// The next slot above `last` from the candidates and the heap (-1: none).
+__device__ int next_slot(LineState *s, const int *cand) {
+  while (s->pc < s->nc && cand[s->pc] <= s->last) s->pc++;
+  while (s->heap_n > 0 && s->heap[0] <= s->last) heap_pop(s);
+  int c = s->pc < s->nc ? cand[s->pc] : -1;
+  int h = s->heap_n > 0 ? s->heap[0] : -1;
+  if (c < 0) return h;
+  if (h < 0) return c;
+  return min(c, h);
+}
+
+// ------------------------------------------------------------- pinsert
+__global__ void k_pinsert_seq(LineArgs a) {
+  LineState *s = a.st;
+  if (s->status) return;
+  for (;;) {
+    const int i = next_slot(s, a.cand);
+    if (i < 0) break;
+    if (a.inf[i] == 0) { s->last = i; continue; }
+    const double disti = seg_len(a.x + 3 * i, a.gi + 3 * i);
+    if (!(disti > 1. * a.delta)) { s->last = i; continue; }
+    int par;
+    if (s->epos < s->ne) {
+      par = a.empt[s->epos];
+    } else {
+      if (s->n_cur >= a.cap) {  // stop before this insertion; the host grows and resumes
+        s->status = 1;
+        return;
+      }
+      par = s->n_cur;
+      for (int c = 0; c < 3; c++) { a.u3[3 * par + c] = 0.; a.u_li[3 * par + c] = 0.; a.u_bs[3 * par + c] = 0.; }
+      a.closest[par] = 0;
+      a.closestd[par] = 0.;
+    }
+    s->last = i;
+    if (s->epos < s->ne) s->epos++;
+    else s->n_cur++;
+    // new position: midpoint moved onto the circle of the local curvature
+    // (src/line.f90:68-85)
+    double X[3], GI[3], GB[3], GII[3], GBB[3], s1[3], fdd[3];
+    for (int c = 0; c < 3; c++) {
+      X[c] = a.x[3 * i + c]; GI[c] = a.gi[3 * i + c]; GB[c] = a.gb[3 * i + c];
+      GII[c] = a.gii[3 * i + c]; GBB[c] = a.gbb[3 * i + c];
+    }
+    lia_derivs(a.order, X, GI, GB, GII, GBB, s1, fdd);  // get_deriv_2
+    double curv = sqrt(fdd[0] * fdd[0] + fdd[1] * fdd[1] + fdd[2] * fdd[2]);
+    double xn[3];
+    if (curv > 1E-5) {
+      curv = 1. / curv;
+      if (curv * curv - 0.25 * (disti * disti) > 0.) {
+        double f = (sqrt(curv * curv - 0.25 * (disti * disti)) - curv) * curv;
+        for (int c = 0; c < 3; c++) xn[c] = 0.5 * (X[c] + GI[c]) + f * fdd[c];
+      } else {
+        for (int c = 0; c < 3; c++) xn[c] = 0.5 * (X[c] + GI[c]);
+      }
+    } else {
+      for (int c = 0; c < 3; c++) xn[c] = 0.5 * (X[c] + GI[c]);
+    }
+    const int ao = a.inf[i] - 1;  // old infront
+    for (int c = 0; c < 3; c++) {
+      a.x[3 * par + c] = xn[c];
+      a.u[3 * par + c] = 0.5 * (a.u[3 * i + c] + a.u[3 * ao + c]);
+      a.u1[3 * par + c] = 0.;
+      a.u2[3 * par + c] = 0.;
+    }
+    a.beh[par] = i + 1;
+    a.inf[par] = a.inf[i];
+    ghost_one(par, a.x, a.inf, a.beh, a.gi, a.gb, a.gii, a.gbb, a.lo_axis, a.L);
+    a.beh[ao] = par + 1;
+    ghost_one(ao, a.x, a.inf, a.beh, a.gi, a.gb, a.gii, a.gbb, a.lo_axis, a.L);
+    a.inf[i] = par + 1;
+    ghost_one(i, a.x, a.inf, a.beh, a.gi, a.gb, a.gii, a.gbb, a.lo_axis, a.L);
+    s->done++;
+    // slots whose stored ghosts changed and that the loop still visits
+    if (ao > i && ao < s->n_old) heap_push(s, ao);
+    if (par > i && par < s->n_old) heap_push(s, par);
+    if (s->status) return;
+  }
+}
+
+// ------------------------------------------------------------- premove
+// loop_killer (src/reconnection.f90:421-461): only whether the loop has fewer
+// than 5 points matters, so the count stops at 5.
+__device__ int loop_killer(const LineArgs &a, int particle) {
+  int counter = 1, next = particle;
+  for (int k = 0; k < 5; k++) {
+    next = a.inf[next] - 1;
+    if (next == particle || next < 0) break;
+    counter++;
+  }
+  if (counter >= 5) return 0;
+  next = particle;
+  for (int k = 0; k < 5; k++) {
+    int store_next = a.inf[next] - 1;
+    clear_slot(a, next);
+    next = store_next;
+    if (next == particle || next < 0) break;
+  }
+  return counter;
+}
+
+__global__ void k_premove_seq(LineArgs a) {
+  LineState *s = a.st;
+  if (s->status) return;
+  for (;;) {
+    const int i = next_slot(s, a.cand);
+    if (i < 0) break;
+    s->last = i;
+    if (a.inf[i] == 0 || !remove_test(a, i)) continue;
+    const int r = a.inf[i] - 1, t = a.inf[r] - 1;  // removed point, its infront
+    a.beh[t] = i + 1;
+    a.inf[i] = t + 1;
+    clear_slot(a, r);
+    s->done += 1 + loop_killer(a, i);
+    // i's behind now reaches a different point two ahead
+    if (a.inf[i] != 0) {
+      const int b = a.beh[i] - 1;
+      if (b > i && b < s->n_old) heap_push(s, b);
+    }
+    if (s->status) return;
+  }
+}
+
+// --------------------------------------------------------------- host
+// Flag and list arrays for n slots (the slot count at the start of a scan).
+static int line_reserve(qv_ctx *c) {
+  size_t n = (size_t)std::max(c->n, 1);
+  if (c->line_cap >= n && c->line_st) return QV_OK;
+  int rc;
+  if ((rc = qv_grow(c, (void **)&c->line_flags, sizeof(int) * 4 * n))) return rc;
+  if (!c->line_st)
+    if ((rc = qv_grow(c, (void **)&c->line_st, sizeof(LineState)))) return rc;
+  c->line_cap = n;
+  return QV_OK;
+}
+
+static LineArgs line_args(qv_ctx *c) {
+  LineArgs a;
+  a.x = c->x; a.u = c->u; a.u1 = c->u1; a.u2 = c->u2; a.u3 = c->u3;
+  a.gi = c->gi; a.gb = c->gb; a.gii = c->gii; a.gbb = c->gbb;
+  a.u_li = c->u_li; a.u_bs = c->u_bs; a.closestd = c->closestd;
+  a.inf = c->infront; a.beh = c->behind; a.closest = c->closest;
+  a.cap = c->cap;
+  a.lo_axis = c->p.boundary == QV_BC_PERIODIC ? 0 : c->p.boundary == QV_BC_OPENX ? 1
+              : c->p.boundary == QV_BC_OPENXY ? 2 : 3;
+  a.order = c->p.deriv_order;
+  a.L = c->p.box_size;
+  a.delta = c->p.delta;
+  a.thr = .499 * c->p.delta * (1. + 1.);
+  int *f = (int *)c->line_flags;
+  size_t n = c->line_cap;
+  a.flag_a = f;
+  a.flag_b = f + n;
+  a.cand = f + 2 * n;
+  a.empt = f + 3 * n;
+  a.st = (LineState *)c->line_st;
+  return a;
+}
+
+// Ordered compaction of flag[0..n) into out (the active-slot compaction run
+// on a flag array); the count goes to *total on the device.
+static int compact_flags(qv_ctx *c, int n, const int *flag, int *out, int *total) {
+  int nb = nblk(n, 256);
+  int *tmp = c->blkcnt;
+  k_count_active<<<nb, 256, 0, c->stream>>>(n, flag, tmp);
+  k_scan_small<<<1, 1024, 0, c->stream>>>(nb, tmp, total);
+  k_scatter_active<<<nb, 256, 0, c->stream>>>(n, flag, tmp, out);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 3);
+  return QV_OK;
+}
+
+static int read_state(qv_ctx *c, LineState *h) {
+  QV_CUDA(c, cudaMemcpyAsync(h, c->line_st, offsetof(LineState, heap), cudaMemcpyDeviceToHost,
+                             c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+static __global__ void k_line_begin(LineState *s, int n) {
+  s->pc = 0; s->epos = 0; s->n_old = n; s->n_cur = n; s->last = -1; s->heap_n = 0;
+  s->status = 0; s->done = 0;
+}
+
+static __global__ void k_line_clear_status(LineState *s) { s->status = 0; }
+
+int qv_line_insert(qv_ctx *c, int *inserted) {
+  int rc;
+  if (c->n == 0) { if (inserted) *inserted = 0; return QV_OK; }
+  // pinsert reads the stored ghosts; compute them only if none exist yet
+  if (!c->ghosts_stored)
+    if ((rc = qv_launch_ghosts(c))) return rc;
+  // room for insertions past the last slot: grow (keeping the points) so that
+  // at least an eighth of the slots, or 4096, are free
+  int want = c->n + std::max(4096, c->n / 8);
+  if (c->cap < c->n + 1024)
+    if ((rc = qv_grow_points(c, want))) return rc;
+  if ((rc = line_reserve(c))) return rc;
+  LineArgs a = line_args(c);
+  const int n = c->n;
+  k_line_begin<<<1, 1, 0, c->stream>>>(a.st, n);
+  k_ins_flags<<<nblk(n, 256), 256, 0, c->stream>>>(n, a);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
+  if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
+  if ((rc = compact_flags(c, n, a.flag_b, (int *)a.empt, &a.st->ne))) return rc;
+  LineState h;
+  for (int attempt = 0; attempt < 16; attempt++) {
+    k_pinsert_seq<<<1, 1, 0, c->stream>>>(a);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    if ((rc = read_state(c, &h))) return rc;
+    if (h.status != 1) break;
+    // more slots than allocated: grow the point arrays, keeping every slot in
+    // use including those appended so far (the candidate and empty-slot lists
+    // keep their size), and resume where the scan stopped
+    c->n = h.n_cur;
+    if ((rc = qv_grow_points(c, c->cap + std::max(4096, c->cap / 4)))) return rc;
+    a = line_args(c);
+    k_line_clear_status<<<1, 1, 0, c->stream>>>(a.st);
+  }
+  if (h.status == 1) return qv_fail(c, QV_ERR_NOMEM, "pinsert: slot growth did not converge");
+  if (h.status == 2) return qv_fail(c, QV_ERR_STATE, "pinsert: more than %d re-tests pending", LHEAP);
+  c->n = h.n_cur;
+  if (inserted) *inserted = h.done;
+  return QV_OK;
+}
+
+int qv_line_remove(qv_ctx *c, int *removed) {
+  int rc;
+  if (c->n == 0) { if (removed) *removed = 0; return QV_OK; }
+  if ((rc = line_reserve(c))) return rc;
+  LineArgs a = line_args(c);
+  const int n = c->n;
+  k_line_begin<<<1, 1, 0, c->stream>>>(a.st, n);
+  k_rem_flags<<<nblk(n, 256), 256, 0, c->stream>>>(n, a);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
+  if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
+  k_premove_seq<<<1, 1, 0, c->stream>>>(a);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  LineState h;
+  if ((rc = read_state(c, &h))) return rc;
+  if (h.status == 2) return qv_fail(c, QV_ERR_STATE, "premove: more than %d re-tests pending", LHEAP);
+  if (removed) *removed = h.done;
+  return QV_OK;
+}

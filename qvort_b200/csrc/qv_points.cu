@@ -77,6 +77,7 @@ int qv_launch_ghosts(qv_ctx *c) {
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
   c->ghosts_valid = true;
+  c->ghosts_stored = true;
   return QV_OK;
 }
 

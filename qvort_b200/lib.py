@@ -53,6 +53,7 @@ class QvParams(C.Structure):
         ("precision", C.c_int),
         ("runge_kutta", C.c_int),
         ("recon_shots", C.c_int),
+        ("line_ops", C.c_int),
     ]
 
 
@@ -127,6 +128,10 @@ _SIGS = {
     "qv_read_var_file": [C.c_char_p, C.c_int, _I, _D, _P, _P, _P],
     "qv_write_var_file": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
     "qv_setup_loops": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
+    "qv_pinsert": [_P, _I],
+    "qv_premove": [_P, _I],
+    "qv_point_count": [_P, _I],
+    "qv_get_links": [_P, _P, _P],
     "qv_batch_create": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, C.POINTER(_P)],
     "qv_batch_set_points": [_P, _P, _P, _P],
     "qv_batch_velocity": [_P, _P],
@@ -329,8 +334,33 @@ class Context:
         self._check(_lib.qv_energy(self._h, C.byref(e)))
         return e.value
 
+    def pinsert(self) -> int:
+        k = C.c_int()
+        self._check(_lib.qv_pinsert(self._h, C.byref(k)))
+        self._sync_count()
+        return k.value
+
+    def premove(self) -> int:
+        k = C.c_int()
+        self._check(_lib.qv_premove(self._h, C.byref(k)))
+        return k.value
+
+    def get_links(self):
+        inf = np.empty(self.n, np.int32)
+        beh = np.empty(self.n, np.int32)
+        self._check(_lib.qv_get_links(self._h, _ptr(inf), _ptr(beh)))
+        return inf, beh
+
+    def _sync_count(self):
+        m = C.c_int()
+        self._check(_lib.qv_point_count(self._h, C.byref(m)))
+        self.n = m.value
+        return self.n
+
     def step(self, itime: int = 1):
         self._check(_lib.qv_step(self._h, itime))
+        if self.params.line_ops:
+            self._sync_count()
 
     def sync(self):
         self._check(_lib.qv_sync(self._h))
@@ -358,7 +388,7 @@ class Context:
 
     # ---- instrumentation
     PHASES = ("ghosts", "build", "local", "nonlocal", "update", "search", "wrap",
-              "build_levels", "build_moments")
+              "build_levels", "build_moments", "line")
 
     def profile(self, enable: bool = True):
         self._check(_lib.qv_profile(self._h, int(enable)))

@@ -21,6 +21,7 @@ module qv_iface
     real(c_double) :: quant_circ, corea, box_size, delta, dt, tree_theta
     integer(c_int) :: boundary, velocity, deriv_order, tree_extra_correction
     integer(c_int) :: fixed_lia_beta, precision, runge_kutta, recon_shots
+    integer(c_int) :: line_ops
   end type
 
   interface

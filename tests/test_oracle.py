@@ -191,3 +191,75 @@ def test_pclose_matches_bruteforce_numpy():
     j = d.argmin(axis=1)
     np.testing.assert_array_equal(cl, j + 1)
     np.testing.assert_allclose(cd, d[idx, j], rtol=1e-15)
+
+
+def _line_ring(n, radius, delta):
+    w = W.ring(n, radius, 0.0, seed=0)
+    p = O.params(**dict(w.params, delta=delta))
+    g = O.ghosts(p, w.x, w.infront, w.behind)
+    st = O.line_state(n, 3 * n, x=w.x, infront=w.infront, behind=w.behind, gi=g[0], gb=g[1],
+                      gii=g[2], gbb=g[3])
+    return p, st
+
+
+def test_pinsert_ring_splits_every_segment_onto_the_circle():
+    """Every segment of a coarse circle exceeds delta: one new point per segment,
+    appended after the last slot (no empty slot), each on the circle (the
+    insertion follows the local curvature radius, src/line.f90:68-85) and
+    linked between its neighbours."""
+    n, R = 40, 0.01
+    p, st = _line_ring(n, R, 5e-4)          # spacing 1.57e-3
+    n2, k = O.pinsert(p, n, st)
+    assert (n2, k) == (2 * n, n)
+    r = np.linalg.norm(st["x"][:n2], axis=1)
+    assert np.abs(r - R).max() < 1e-3 * R   # the discrete curvature radius of a 40-gon
+    inf = st["infront"][:n2]
+    assert sorted(inf) == list(range(1, n2 + 1))
+    for i in range(n):                       # i -> new point -> old infront
+        j = inf[i] - 1
+        assert j >= n and inf[j] == (i + 1) % n + 1
+
+
+def test_pinsert_resolution_kept_and_premove_undoes_crowding():
+    """After pinsert no segment is longer than delta on a circle whose spacing
+    was between delta and 2 delta; premove on a circle spaced at 0.3 delta
+    removes points until consecutive pairs are at least 0.998 delta apart (or
+    the scan has passed them)."""
+    p, st = _line_ring(60, 0.004, 3.5e-4)   # spacing 4.19e-4 in (delta, 2 delta)
+    n2, k = O.pinsert(p, 60, st)
+    assert k == 60
+    x, inf = st["x"][:n2], st["infront"][:n2]
+    seg = np.linalg.norm(x[inf - 1] - x, axis=1)
+    assert seg.max() <= 3.5e-4
+    p, st = _line_ring(200, 0.004, 4e-4)    # spacing 1.26e-4 = 0.31 delta
+    removed = O.premove(p, 200, st)
+    assert 0 < removed < 200
+    inf = st["infront"][:200]
+    act = np.nonzero(inf)[0]
+    assert len(act) == 200 - removed
+    # the loop is still closed: following infront from any point visits all
+    k, seen = act[0], 0
+    while True:
+        k = inf[k] - 1
+        seen += 1
+        if k == act[0]:
+            break
+    assert seen == len(act)
+
+
+def test_loop_killer_clears_loops_below_five_points():
+    """premove leaving a loop of 4 points clears it (src/reconnection.f90:441-458);
+    a loop left with 5 survives."""
+    for npts, survives in ((5, False), (6, True)):
+        b = np.array([0.0, 0.03, 0.06] + list(np.linspace(1.5, 5.0, npts - 3)))
+        x = np.stack([0.003 * np.cos(b), 0.003 * np.sin(b), np.zeros(npts)], 1)
+        inf = ((np.arange(npts) + 1) % npts + 1).astype(np.int32)
+        beh = ((np.arange(npts) - 1) % npts + 1).astype(np.int32)
+        p = O.params(**dict(W.ring(8).params, delta=3e-4))
+        st = O.line_state(npts, npts, x=x, infront=inf, behind=beh)
+        removed = O.premove(p, npts, st)
+        alive = int((st["infront"][:npts] != 0).sum())
+        if survives:
+            assert removed == 1 and alive == npts - 1
+        else:
+            assert removed == npts and alive == 0
