@@ -65,10 +65,12 @@ typedef struct qv_params {
   int precision;              /* QV_PREC_* */
   int runge_kutta;            /* runge_kutta */
   int recon_shots;            /* recon_shots, default 1 */
-  int line_ops;               /* 1: qv_step also runs pinsert after the update and premove
-                                 after the candidate search (the loop of src/run.f90:59-72
-                                 with switch_off_recon true); 0 (default): both left to
-                                 the caller (qv_pinsert, qv_premove) */
+  int line_ops;               /* 0 (default): qv_step leaves the line operations to the
+                                 caller (qv_pinsert, qv_precon, qv_premove); 1: qv_step
+                                 runs pinsert after the update and premove after the
+                                 candidate search (src/run.f90:59-72 with switch_off_recon
+                                 true); 2: also precon_original between the search and
+                                 premove (the reference's default loop) */
 } qv_params;
 
 typedef struct qv_ctx qv_ctx;
@@ -204,6 +206,12 @@ int qv_pinsert(qv_ctx *ctx, int *inserted);
  * |x_i - x_infront(infront(i))| < 0.998 delta; loops left with fewer than 5
  * points are cleared.  *removed (may be NULL) counts both. */
 int qv_premove(qv_ctx *ctx, int *removed);
+/* precon with recon_type 'original' (src/reconnection.f90:145-254; recon_info
+ * and recon_time_info off): reconnects each point whose last candidate search
+ * (qv_closest) found a partner closer than delta/2, unless the filaments are
+ * near parallel or the line would lengthen; loops left below 5 points are
+ * cleared.  Uses the stored ghosts.  *count (may be NULL) = reconnections. */
+int qv_precon(qv_ctx *ctx, int *count);
 /* Current slot count (pcount), which pinsert can raise, and the links of all
  * slots (1-based, 0 = empty slot; the f(:)%infront, f(:)%behind a host
  * scatters back after insertion or removal). */

@@ -87,6 +87,7 @@ def lib() -> C.CDLL:
         _lib.qo_set_depth_cap.argtypes = [C.c_int]
         _lib.qo_pinsert.argtypes = [P, C.POINTER(C.c_int), C.c_int, C.POINTER(QoState)]
         _lib.qo_premove.argtypes = [P, C.c_int, C.POINTER(QoState)]
+        _lib.qo_precon.argtypes = [P, C.c_int, C.POINTER(QoState)]
     return _lib
 
 
@@ -258,6 +259,11 @@ def pinsert(p: QoParams, n: int, st) -> tuple[int, int]:
 def premove(p: QoParams, n: int, st) -> int:
     """premove on the state dict in place; returns the points removed."""
     return lib().qo_premove(C.byref(p), n, C.byref(_qostate(st)))
+
+
+def precon(p: QoParams, n: int, st) -> int:
+    """precon_original on the state dict in place; returns the reconnections."""
+    return lib().qo_precon(C.byref(p), n, C.byref(_qostate(st)))
 
 
 def dt_max(p: QoParams) -> float:

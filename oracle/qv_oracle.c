@@ -946,3 +946,48 @@ int qo_premove(const qo_params *p, int pcount, qo_state *S) {
   }
   return removed;
 }
+
+/* norm_tanf, src/general.f90:94-107: get_deriv_1 on the stored ghosts, normalised */
+static void norm_tanf(const qo_params *p, const qo_state *S, int i, double *t) {
+  deriv1(p, S->x + 3 * i, S->gi + 3 * i, S->gb + 3 * i, S->gii + 3 * i, S->gbb + 3 * i, t);
+  double length = sqrt(sq(t[0]) + sq(t[1]) + sq(t[2]));
+  for (int c = 0; c < 3; c++) t[c] = t[c] / length;
+}
+
+/* precon_original, src/reconnection.f90:145-254 (recon_info and recon_time_info
+ * off).  Reads closest/closestd of the last candidate search and the stored
+ * ghosts; returns the number of reconnections. */
+int qo_precon(const qo_params *p, int pcount, qo_state *S) {
+  int count = 0;
+  for (int i = 0; i < pcount; i++) {
+    if (S->infront[i] == 0) continue;
+    int pari = S->infront[i] - 1, parb = S->behind[i] - 1;
+    if (!((S->closestd[i] < p->delta / 2.) && (S->closestd[i] > QO_EPS))) continue;
+    int j = S->closest[i] - 1;
+    if (j == pari) continue;
+    if (j == parb) continue;
+    if (j == -1) continue;
+    if (S->infront[j] == 0) continue;
+    int parjb = S->behind[j] - 1;
+    double t1[3], t2[3];
+    norm_tanf(p, S, i, t1);
+    norm_tanf(p, S, j, t2);
+    double dot_val = t1[0] * t2[0] + t1[1] * t2[1] + t1[2] * t2[2];
+    if (dot_val > 0.9) continue;
+    const double *xi = S->x + 3 * i, *xj = S->x + 3 * j;
+    double l_before = dist_gen(xi, S->gi + 3 * i) + dist_gen(xi, S->gb + 3 * i) +
+                      dist_gen(xj, S->gi + 3 * j) + dist_gen(xj, S->gb + 3 * j);
+    double l_after = dist_gen(xi, S->gb + 3 * i) + dist_gen(xi, xj) +
+                     dist_gen(xj, S->gi + 3 * j) + dist_gen(S->x + 3 * pari, S->x + 3 * parjb);
+    if (l_after <= l_before) {
+      count++;
+      S->infront[parjb] = pari + 1;
+      S->behind[pari] = parjb + 1;
+      S->infront[i] = j + 1;
+      S->behind[j] = i + 1;
+      loop_killer(S, pcount, pari);
+      loop_killer(S, pcount, i);
+    }
+  }
+  return count;
+}

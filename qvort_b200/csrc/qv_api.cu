@@ -34,7 +34,7 @@ static int validate(qv_ctx *c, const qv_params *p) {
   if (p->boundary != QV_BC_OPEN && !(p->box_size > 0))
     return qv_fail(c, QV_ERR_ARG, "periodic boundaries need a positive box size");
   if (p->recon_shots < 1) return qv_fail(c, QV_ERR_ARG, "recon_shots must be >= 1");
-  if (p->line_ops != 0 && p->line_ops != 1) return qv_fail(c, QV_ERR_ARG, "line_ops must be 0 or 1");
+  if (p->line_ops < 0 || p->line_ops > 2) return qv_fail(c, QV_ERR_ARG, "line_ops must be 0, 1 or 2");
   if (p->line_ops && !(p->delta > 0)) return qv_fail(c, QV_ERR_ARG, "line operations need delta > 0");
   return QV_OK;
 }
@@ -584,9 +584,11 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
     qv_phase_begin(c, PH_CLOSEST);
     if ((rc = qv_launch_closest(c))) return rc;
     qv_phase_end(c, PH_CLOSEST);
-    if (c->p.line_ops) {                                         // run.f90:72
+    if (c->p.line_ops) {
       qv_phase_begin(c, PH_LINE);
-      if ((rc = qv_line_remove(c, nullptr))) return rc;
+      if (c->p.line_ops == 2)                                    // run.f90:70
+        if ((rc = qv_line_reconnect(c, nullptr))) return rc;
+      if ((rc = qv_line_remove(c, nullptr))) return rc;          // run.f90:72
       qv_phase_end(c, PH_LINE);
     }
   }
@@ -617,6 +619,12 @@ extern "C" int qv_get_links(qv_ctx *c, int *infront, int *behind) {
   if (behind && v) QV_CUDA(c, cudaMemcpyAsync(behind, c->behind, v, cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
   return QV_OK;
+}
+
+extern "C" int qv_precon(qv_ctx *c, int *count) {
+  QV_CHECK_CTX(c);
+  if (!(c->p.delta > 0)) return qv_fail(c, QV_ERR_ARG, "precon needs delta > 0");
+  return qv_line_reconnect(c, count);
 }
 
 extern "C" int qv_point_count(qv_ctx *c, int *n) {

@@ -179,6 +179,7 @@ int qv_compact_active(qv_ctx *c);
 int qv_grow_points(qv_ctx *c, int new_cap);
 int qv_line_insert(qv_ctx *c, int *inserted);
 int qv_line_remove(qv_ctx *c, int *removed);
+int qv_line_reconnect(qv_ctx *c, int *count);
 // ordered compaction kernels (qv_direct.cu): counts of nonzero flags per
 // 256-slot block, their exclusive scan (total to *total), the scatter
 __global__ void k_count_active(int n, const int *__restrict__ inf, int *blk_cnt);

@@ -1,8 +1,8 @@
-// qv_line.cu -- the line operations that keep the resolution: pinsert
-// (src/line.f90:18-106) and premove with loop_killer (src/line.f90:112-161,
-// src/reconnection.f90:421-461).
+// qv_line.cu -- the line operations of the time loop: pinsert
+// (src/line.f90:18-106), precon_original (src/reconnection.f90:145-254) and
+// premove with loop_killer (src/line.f90:112-161, src/reconnection.f90:421-461).
 //
-// Both are sequential scans over the slots in ascending order whose effects
+// All three are sequential scans over the slots in ascending order whose effects
 // feed later iterations: an insertion takes the first empty slot (or appends
 // one), relinks, and refreshes the stored ghosts of three slots (the new
 // point, i, and i's old infront), and a later test of a refreshed slot sees
@@ -268,6 +268,62 @@ __global__ void k_premove_seq(LineArgs a) {
   }
 }
 
+// ------------------------------------------------------------- precon
+// precon_original (src/reconnection.f90:145-254): its candidates are the
+// active slots whose last search found a partner closer than delta/2 (and
+// farther than epsilon) -- closestd is not changed by the scan, so the list is
+// fixed before it runs; each candidate is then tested on the current links.
+__global__ void k_rec_flags(int n, LineArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double cd = a.closestd[i];
+  a.flag_a[i] = a.inf[i] != 0 && (cd < a.delta / 2.) && (cd > QV_DEPS);
+}
+
+// norm_tanf, src/general.f90:94-107: get_deriv_1 on the stored ghosts, normalised.
+__device__ void norm_tan(const LineArgs &a, int i, double *t) {
+  double X[3], GI[3], GB[3], GII[3], GBB[3], s2[3];
+  for (int c = 0; c < 3; c++) {
+    X[c] = a.x[3 * i + c]; GI[c] = a.gi[3 * i + c]; GB[c] = a.gb[3 * i + c];
+    GII[c] = a.gii[3 * i + c]; GBB[c] = a.gbb[3 * i + c];
+  }
+  lia_derivs(a.order, X, GI, GB, GII, GBB, t, s2);
+  double length = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  for (int c = 0; c < 3; c++) t[c] = t[c] / length;
+}
+
+__global__ void k_precon_seq(LineArgs a) {
+  LineState *s = a.st;
+  for (; s->pc < s->nc; s->pc++) {
+    const int i = a.cand[s->pc];
+    if (a.inf[i] == 0) continue;  // cleared by an earlier loop_killer
+    const int pari = a.inf[i] - 1, parb = a.beh[i] - 1;
+    const int j = a.closest[i] - 1;
+    if (j == pari || j == parb || j < 0) continue;
+    if (a.inf[j] == 0) continue;
+    const int parjb = a.beh[j] - 1;
+    double t1[3], t2[3];
+    norm_tan(a, i, t1);
+    norm_tan(a, j, t2);
+    const double dot_val = t1[0] * t2[0] + t1[1] * t2[1] + t1[2] * t2[2];
+    if (dot_val > 0.9) continue;  // parallel filaments do not reconnect
+    const double *xi = a.x + 3 * i, *xj = a.x + 3 * j;
+    const double l_before = seg_len(xi, a.gi + 3 * i) + seg_len(xi, a.gb + 3 * i) +
+                            seg_len(xj, a.gi + 3 * j) + seg_len(xj, a.gb + 3 * j);
+    const double l_after = seg_len(xi, a.gb + 3 * i) + seg_len(xi, xj) +
+                           seg_len(xj, a.gi + 3 * j) + seg_len(a.x + 3 * pari, a.x + 3 * parjb);
+    if (l_after <= l_before) {
+      a.inf[parjb] = pari + 1;
+      a.beh[pari] = parjb + 1;
+      a.inf[i] = j + 1;
+      a.beh[j] = i + 1;
+      loop_killer(a, pari);
+      loop_killer(a, i);
+      s->done++;
+    }
+  }
+}
+
 // --------------------------------------------------------------- host
 // Flag and list arrays for n slots (the slot count at the start of a scan).
 static int line_reserve(qv_ctx *c) {
@@ -370,6 +426,28 @@ int qv_line_insert(qv_ctx *c, int *inserted) {
   if (h.status == 2) return qv_fail(c, QV_ERR_STATE, "pinsert: more than %d re-tests pending", LHEAP);
   c->n = h.n_cur;
   if (inserted) *inserted = h.done;
+  return QV_OK;
+}
+
+int qv_line_reconnect(qv_ctx *c, int *count) {
+  int rc;
+  if (c->n == 0) { if (count) *count = 0; return QV_OK; }
+  if ((rc = line_reserve(c))) return rc;
+  LineArgs a = line_args(c);
+  const int n = c->n;
+  k_line_begin<<<1, 1, 0, c->stream>>>(a.st, n);
+  k_rec_flags<<<nblk(n, 256), 256, 0, c->stream>>>(n, a);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
+  if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
+  k_precon_seq<<<1, 1, 0, c->stream>>>(a);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  if (count) {
+    LineState h;
+    if ((rc = read_state(c, &h))) return rc;
+    *count = h.done;
+  }
   return QV_OK;
 }
 

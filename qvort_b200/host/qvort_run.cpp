@@ -2,9 +2,9 @@
 // runs the velocity-and-timestep path of this library from a run.in:
 //   read_run_file -> initial condition (var_file, single_loop, leap-frog) ->
 //   do itime = 1, nsteps: qv_step (ghostp, construct_tree, pmotion /
-//   pmotion_RK3, candidate search, ghostp, boundary wrap), t = t + dt;
+//   pmotion_RK3, pinsert, candidate search, precon unless switch_off_recon,
+//   premove, ghostp, boundary wrap), t = t + dt;
 //   every `shots` steps: data/var%04d.log and a one-line summary, STOP file.
-// Insertion, removal and reconnection are not part of the path and are not run.
 //
 //   usage: qvort_run [run.in]        (run from the run directory)
 #include <sys/stat.h>
@@ -57,6 +57,8 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "qvort_run: initf '%s' is outside this path (status %d)\n", r.initf, rc);
     return 2;
   }
+  // the line operations of src/run.f90:59-72 (they need a resolution delta)
+  r.p.line_ops = r.p.delta > 0 ? (r.switch_off_recon ? 1 : 2) : 0;
   qv_ctx *ctx = nullptr;
   if ((rc = qv_create(&r.p, nullptr, &ctx))) {
     std::fprintf(stderr, "qvort_run: qv_create failed (status %d)\n", rc);
@@ -77,7 +79,14 @@ int main(int argc, char **argv) {
     }
     t = t + r.p.dt;
     if (r.shots > 0 && itime % r.shots == 0) {
+      // insertion can raise the slot count and every line operation relinks
+      qv_point_count(ctx, &n);
+      x.resize(3 * (size_t)n);
+      u.resize(3 * (size_t)n);
+      inf.resize(n);
+      beh.resize(n);
       qv_get_points(ctx, x.data(), u.data());
+      qv_get_links(ctx, inf.data(), beh.data());
       char name[64];
       std::snprintf(name, sizeof name, "./data/var%04d.log", ++shot);
       qv_write_var_file(name, n, t, x.data(), inf.data(), u.data());

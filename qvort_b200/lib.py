@@ -131,6 +131,7 @@ _SIGS = {
     "qv_pinsert": [_P, _I],
     "qv_premove": [_P, _I],
     "qv_point_count": [_P, _I],
+    "qv_precon": [_P, _I],
     "qv_get_links": [_P, _P, _P],
     "qv_batch_create": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, C.POINTER(_P)],
     "qv_batch_set_points": [_P, _P, _P, _P],
@@ -338,6 +339,11 @@ class Context:
         k = C.c_int()
         self._check(_lib.qv_pinsert(self._h, C.byref(k)))
         self._sync_count()
+        return k.value
+
+    def precon(self) -> int:
+        k = C.c_int()
+        self._check(_lib.qv_precon(self._h, C.byref(k)))
         return k.value
 
     def premove(self) -> int:

@@ -183,3 +183,67 @@ def test_step_with_line_ops_equals_the_call_sequence():
     assert np.array_equal(xa[act], xb[act])
     a.close()
     b.close()
+
+
+def test_precon_matches_oracle():
+    L, W = _mods()
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).parent))
+    from test_oracle import _touching_rings
+
+    x, inf, beh = _touching_rings()
+    prm = dict(W.ring(8).params, delta=5e-4, box_size=0.1)
+    c = L.Context(L.default_params(**prm))
+    c.set_points(x, inf, beh)
+    c.ghosts()
+    cl, cd = c.closest()
+    st = _ctx_state(c)
+    n0, ref = _oracle_state(st, len(x))
+    ref["closest"][:] = cl
+    ref["closestd"][:] = cd
+    k_ref = O.precon(O.params(**prm), n0, ref)
+    k = c.precon()
+    assert k == k_ref == 2
+    _compare(c, n0, ref)
+    c.close()
+
+
+def test_step_with_reconnection_equals_the_call_sequence():
+    """line_ops = 2: pinsert, candidate search, precon, premove in qv_step."""
+    L, W = _mods()
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).parent))
+    from test_oracle import _touching_rings
+
+    x, inf, beh = _touching_rings(n=60, R=0.004, gap=4e-5)
+    prm = dict(W.ring(8).params, delta=4.5e-4, box_size=0.1, tree_theta=0.4, velocity="Tree",
+               precision="mixed", dt=1e-6)
+    a = L.Context(L.default_params(**prm, line_ops=2))
+    a.set_points(x, inf, beh)
+    b = L.Context(L.default_params(**prm))
+    b.set_points(x, inf, beh)
+    nrec = 0
+    for it in range(1, 4):
+        a.step(it)
+        b.ghosts()
+        b.build_tree()
+        b.velocity(False)
+        b.step_ab()
+        b.pinsert()
+        b.closest()
+        nrec += b.precon()
+        b.premove()
+        b.ghosts()
+        b.enforce_periodic()
+    assert nrec > 0 and a.n == b.n
+    ia, _ = a.get_links()
+    ib, _ = b.get_links()
+    assert np.array_equal(ia, ib)
+    xa, _ = a.get_points()
+    xb, _ = b.get_points()
+    act = ia != 0
+    assert np.array_equal(xa[act], xb[act])
+    a.close()
+    b.close()

@@ -263,3 +263,43 @@ def test_loop_killer_clears_loops_below_five_points():
             assert removed == 1 and alive == npts - 1
         else:
             assert removed == npts and alive == 0
+
+
+def _touching_rings(n=40, R=0.004, gap=1e-4):
+    """Two coplanar rings, both counter-clockwise, a gap apart at x = 0: their
+    tangents there are anti-parallel."""
+    a = 2 * np.pi * (np.arange(n) + 0.5) / n
+    r1 = np.stack([-R - gap / 2 + R * np.cos(a), R * np.sin(a), np.zeros(n)], 1)
+    r2 = np.stack([R + gap / 2 + R * np.cos(a + np.pi), R * np.sin(a + np.pi), np.zeros(n)], 1)
+    x = np.concatenate([r1, r2])
+    k = np.arange(n)
+    inf = np.concatenate([(k + 1) % n + 1, n + (k + 1) % n + 1]).astype(np.int32)
+    beh = np.concatenate([(k - 1) % n + 1, n + (k - 1) % n + 1]).astype(np.int32)
+    return x, inf, beh
+
+
+def test_precon_merges_two_touching_rings():
+    """Anti-parallel filaments closer than delta/2 reconnect (the line gets
+    shorter): two loops become one loop through all points."""
+    x, inf, beh = _touching_rings()
+    n = len(x)
+    p = O.params(**dict(W.ring(8).params, delta=5e-4))
+    g = O.ghosts(p, x, inf, beh)
+    cl, cd = O.pclose(x, inf, beh, np.zeros(n, np.int32))
+    st = O.line_state(n, n, x=x, infront=inf, behind=beh, gi=g[0], gb=g[1], gii=g[2], gbb=g[3],
+                      closest=cl, closestd=cd)
+    assert (cd < 2.5e-4).sum() >= 2
+    k = O.precon(p, n, st)
+    assert k >= 1
+    inf2 = st["infront"]
+    alive = np.nonzero(inf2)[0]
+    start = i = alive[0]
+    seen = 0
+    for _ in range(n):
+        i = inf2[i] - 1
+        seen += 1
+        if i == start or i < 0:
+            break
+    # one loop through every surviving point (the two-point loop the second
+    # reconnection cuts off goes to loop_killer)
+    assert i == start and seen == len(alive) >= n - 8
