@@ -183,11 +183,20 @@ def cpu_step_rate(w, seconds_budget: float = 12.0, nthreads: int | None = None):
     xn, *_ = O.pmotion_ab(p.dt, x, uf, *h, inf)
     t_ab = time.perf_counter() - t0
     t0 = time.perf_counter()
-    O.pclose_tree(tree, xn, inf, beh, np.zeros(w.n, np.int32), nthreads)
+    cl, cd = O.pclose_tree(tree, xn, inf, beh, np.zeros(w.n, np.int32), nthreads)
     t_c = time.perf_counter() - t0
-    t_step = t_g * 2 + t_b + t_v + t_ab + t_c
-    sample = (f"1 step of the same workload: ghosts, tree build, AB, candidate search on all "
-              f"{w.n} points; velocity on {m} evenly strided targets scaled by {w.n}/{m}")
+    # line operations (sequential in the reference): pinsert, precon, premove
+    st = O.line_state(w.n, 2 * w.n, x=xn, u=uf, infront=inf, behind=beh, gi=g[0], gb=g[1],
+                      gii=g[2], gbb=g[3], closest=cl, closestd=cd)
+    t0 = time.perf_counter()
+    n2, _ = O.pinsert(p, w.n, st)
+    O.precon(p, n2, st)
+    O.premove(p, n2, st)
+    t_l = time.perf_counter() - t0
+    t_step = t_g * 2 + t_b + t_v + t_ab + t_c + t_l
+    sample = (f"1 step of the same workload: ghosts, tree build, AB, candidate search, "
+              f"pinsert/precon/premove on all {w.n} points; velocity on {m} evenly strided "
+              f"targets scaled by {w.n}/{m}")
     return t_step, sample, nthreads
 
 
@@ -247,7 +256,8 @@ def our_arm(args):
     pairs_step = float(n) * n * 27
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
-    ctx = L.Context(L.default_params(**w.params, precision="mixed"), stream=sp)
+    # reconnections on (line_ops 2): pinsert, candidate search, precon, premove
+    ctx = L.Context(L.default_params(**w.params, precision="mixed", line_ops=2), stream=sp)
     ctx.set_points(w.x, w.infront, w.behind)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
@@ -290,8 +300,10 @@ def our_arm(args):
         "data": "synthetic (seeded random rings)",
         "config": {"workload": "tangle: 100 rings R~U(0.008,0.02) cm, delta 5e-4, N=%d, "
                                "periodic L=0.1 (26 images), Tree theta 0.4, mixed precision, "
-                               "AB ladder, dt 1e-7, candidate search every step" % n,
-                   "n_points": n, "l2": "flushed between timed steps (256 MiB write)",
+                               "AB ladder, dt 1e-7, reconnections on" % n,
+                   "n_points": n, "n_points_end": ctx.n,
+                   "line_ops": "pinsert, candidate search, precon (original), premove each step",
+                   "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{ws} (path does not shard)"},
         "steps_per_s": 1e3 / ms_step * ws,
         "clocks": clk,
@@ -386,42 +398,53 @@ def extras(ctx, w, stream, L, torch, itime):
     # ---- end to end through the C ABI with pinned host buffers (the Fortran
     # shim's per-step pattern: gather f(:) in, step, scatter f(:) out)
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
-    hx = pin((n, 3), torch.float64); hx[:] = w.x
-    hinf = pin((n,), torch.int32); hinf[:] = w.infront
-    hbeh = pin((n,), torch.int32); hbeh[:] = w.behind
-    hist = [pin((n, 3), torch.float64) for _ in range(3)]
+    cap = 2 * n  # room for insertions (the host grows f(:) when pcount grows)
+    hx = pin((cap, 3), torch.float64); hx[:n] = w.x
+    hinf = pin((cap,), torch.int32); hinf[:n] = w.infront
+    hbeh = pin((cap,), torch.int32); hbeh[:n] = w.behind
+    hist = [pin((cap, 3), torch.float64) for _ in range(3)]
     for h in hist:
         h[:] = 0
-    hcl = pin((n,), torch.int32); hcl[:] = 0
-    hu = pin((n, 3), torch.float64)
-    hcd = pin((n,), torch.float64)
-    c = L.Context(L.default_params(**w.params, precision="mixed"), stream=sp)
+    hcl = pin((cap,), torch.int32); hcl[:] = 0
+    hu = pin((cap, 3), torch.float64)
+    hcd = pin((cap,), torch.float64)
+    c = L.Context(L.default_params(**w.params, precision="mixed", line_ops=2), stream=sp)
+    cur = [n]
+    moved = [0, 0]
+
     def e2e_step(it):
-        c.set_points(hx, hinf, hbeh)
-        c.set_history(*hist)
-        c.set_closest(hcl)
+        m = cur[0]
+        c.set_points(hx[:m], hinf[:m], hbeh[:m])
+        c.set_history(*[h[:m] for h in hist])
+        c.set_closest(hcl[:m])
         c.step(it)
-        c.get_points(hx, hu)
-        c.get_history(*hist)
-        c.get_closest(hcl, hcd)
+        m = cur[0] = c.n
+        if m > cap:
+            raise RuntimeError("more insertions than the host buffers hold")
+        c.get_points(hx[:m], hu[:m])
+        c.get_history(*[h[:m] for h in hist])
+        c.get_closest(hcl[:m], hcd[:m])
+        c.get_links(hinf[:m], hbeh[:m])
+        moved[0] += m * (24 + 8 + 72 + 4)         # x, links, history, closest in
+        moved[1] += m * (24 + 24 + 72 + 4 + 8 + 8)  # x, u, history, closest(d), links out
 
     for it in range(3):
         e2e_step(it + 1)
     torch.cuda.synchronize()
     K = 10
+    moved[0] = moved[1] = 0
     t0 = time.perf_counter()
     for it in range(K):
         e2e_step(it + 4)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / K
     c.close()
-    h2d = n * (24 + 8 + 72 + 4)
-    d2h = n * (24 + 24 + 72 + 4 + 8)
     out["e2e"] = {"value": pairs_step / (e2e_ms * 1e-3), "unit": UNIT,
-                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                  "h2d_bytes_per_step": moved[0] // K, "d2h_bytes_per_step": moved[1] // K,
+                  "ms_per_step": e2e_ms,
                   "path": "qv_set_points/qv_set_history/qv_set_closest (pinned host) -> qv_step "
-                          "-> qv_get_points/qv_get_history/qv_get_closest (pinned host), "
-                          "wall clock"}
+                          "(line_ops 2) -> qv_get_points/qv_get_history/qv_get_closest/"
+                          "qv_get_links (pinned host), wall clock"}
 
     # ---- gradients/s on the differentiation workload: 16 trefoil rings,
     # N = 50,000, periodic, K = 256 Adams-Bashforth steps checkpointed every 16,

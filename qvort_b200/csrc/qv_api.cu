@@ -138,7 +138,8 @@ extern "C" int qv_destroy(qv_ctx *c) {
   if (c->dscalar) cudaFree(c->dscalar);
   if (c->d_nact) cudaFree(c->d_nact);
   {
-    void *adj[] = {c->adj_xb, c->adj_gib, c->adj_gbb, c->adj_giib, c->adj_gbbb, c->adj_nb};
+    void *adj[] = {c->adj_xb, c->adj_gib, c->adj_gbb, c->adj_giib, c->adj_gbbb, c->adj_nb,
+                   c->line_flags, c->line_st, c->line_rec};
     for (void *q : adj)
       if (q) cudaFree(q);
   }
@@ -471,6 +472,7 @@ static int velocity_collect(qv_ctx *c, long long *eval_count) {
     return qv_fail(c, QV_ERR_SINGULAR, "singularity in BS (tree) velocity field - this is normally "
                    "caused by having recon_shots too large");
   if (st & 2) return qv_fail(c, QV_ERR_TREE_DEPTH, "walk or search stack overflow");
+  if (st & 4) return qv_fail(c, QV_ERR_STATE, "line operation: too many re-tests pending");
   return QV_OK;
 }
 

@@ -129,7 +129,7 @@ struct qv_ctx {
   bool ghosts_valid = false;
   bool ghosts_stored = false;  // ghost arrays hold values (possibly from before a move)
   // line operations (pinsert / premove): flag and list scratch, sequential state
-  void *line_flags = nullptr, *line_st = nullptr;
+  void *line_flags = nullptr, *line_st = nullptr, *line_rec = nullptr;
   size_t line_cap = 0;
   TreeBuf tree;
   int sm_count = 148;

@@ -73,6 +73,7 @@ struct LineArgs {
   const int *cand, *empt;
   int *flag_a, *flag_b;
   LineState *st;
+  int *dstatus;  // the context's status word (bit 4: a scan's re-test heap overflowed)
 };
 
 // clear_particle, src/general.f90:11-22 (u3 is kept)
@@ -93,9 +94,17 @@ __device__ __forceinline__ double seg_len(const double *a, const double *b) {
 }
 
 // ------------------------------------------------------------ detection
+// Reset of the sequential state for a scan over n slots (done by the flag
+// kernel that starts each scan; the compaction then writes nc / ne).
+__device__ __forceinline__ void begin_state(LineState *s, int n) {
+  s->pc = 0; s->epos = 0; s->n_old = n; s->n_cur = n; s->last = -1; s->heap_n = 0;
+  s->status = 0; s->done = 0;
+}
+
 // pinsert's test on the stored ghosts (src/line.f90:41,49) and the empty slots.
 __global__ void k_ins_flags(int n, LineArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) begin_state(a.st, n);
   if (i >= n) return;
   int act = a.inf[i] != 0;
   a.flag_b[i] = !act;
@@ -112,14 +121,16 @@ __device__ __forceinline__ bool remove_test(const LineArgs &a, int i) {
 
 __global__ void k_rem_flags(int n, LineArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) begin_state(a.st, n);
   if (i >= n) return;
   a.flag_a[i] = a.inf[i] != 0 && remove_test(a, i);
 }
 
 // ------------------------------------------------------------- worklist
-__device__ void heap_push(LineState *s, int v) {
+__device__ void heap_push(LineState *s, int *dstatus, int v) {
   if (s->heap_n >= LHEAP) {
     s->status = 2;
+    atomicOr(dstatus, 4);
     return;
   }
   int k = s->heap_n++;
@@ -219,8 +230,8 @@ __global__ void k_pinsert_seq(LineArgs a) {
     ghost_one(i, a.x, a.inf, a.beh, a.gi, a.gb, a.gii, a.gbb, a.lo_axis, a.L);
     s->done++;
     // slots whose stored ghosts changed and that the loop still visits
-    if (ao > i && ao < s->n_old) heap_push(s, ao);
-    if (par > i && par < s->n_old) heap_push(s, par);
+    if (ao > i && ao < s->n_old) heap_push(s, a.dstatus, ao);
+    if (par > i && par < s->n_old) heap_push(s, a.dstatus, par);
     if (s->status) return;
   }
 }
@@ -262,7 +273,7 @@ __global__ void k_premove_seq(LineArgs a) {
     // i's behind now reaches a different point two ahead
     if (a.inf[i] != 0) {
       const int b = a.beh[i] - 1;
-      if (b > i && b < s->n_old) heap_push(s, b);
+      if (b > i && b < s->n_old) heap_push(s, a.dstatus, b);
     }
     if (s->status) return;
   }
@@ -275,6 +286,7 @@ __global__ void k_premove_seq(LineArgs a) {
 // fixed before it runs; each candidate is then tested on the current links.
 __global__ void k_rec_flags(int n, LineArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) begin_state(a.st, n);
   if (i >= n) return;
   double cd = a.closestd[i];
   a.flag_a[i] = a.inf[i] != 0 && (cd < a.delta / 2.) && (cd > QV_DEPS);
@@ -292,27 +304,59 @@ __device__ void norm_tan(const LineArgs &a, int i, double *t) {
   for (int c = 0; c < 3; c++) t[c] = t[c] / length;
 }
 
-__global__ void k_precon_seq(LineArgs a) {
+// What of a candidate's test does not depend on the links -- the tangents and
+// their dot product, the length before, the first three terms of the length
+// after (positions and stored ghosts, which precon does not change) -- is
+// evaluated for all candidates in parallel; the ordered pass re-reads the
+// links and recomputes only the last term when they have changed.
+struct RecEval {
+  int j, pari, parjb, parallel;
+  double l_before, s3, l_after;
+};
+
+__global__ void k_rec_eval(int n, LineArgs a, RecEval *rec) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n || q >= a.st->nc) return;
+  const int i = a.cand[q];
+  RecEval r;
+  r.j = a.closest[i] - 1;
+  r.pari = a.inf[i] - 1;
+  r.parjb = -1;
+  r.parallel = 1;
+  r.l_before = r.s3 = r.l_after = 0.;
+  if (r.j >= 0 && a.inf[r.j] != 0) {
+    const int j = r.j;
+    r.parjb = a.beh[j] - 1;
+    double t1[3], t2[3];
+    norm_tan(a, i, t1);
+    norm_tan(a, j, t2);
+    const double dot_val = t1[0] * t2[0] + t1[1] * t2[1] + t1[2] * t2[2];
+    r.parallel = dot_val > 0.9;
+    const double *xi = a.x + 3 * i, *xj = a.x + 3 * j;
+    r.l_before = seg_len(xi, a.gi + 3 * i) + seg_len(xi, a.gb + 3 * i) +
+                 seg_len(xj, a.gi + 3 * j) + seg_len(xj, a.gb + 3 * j);
+    r.s3 = seg_len(xi, a.gb + 3 * i) + seg_len(xi, xj) + seg_len(xj, a.gi + 3 * j);
+    r.l_after = r.s3 + seg_len(a.x + 3 * r.pari, a.x + 3 * r.parjb);
+  }
+  rec[q] = r;
+}
+
+__global__ void k_precon_seq(LineArgs a, const RecEval *rec) {
   LineState *s = a.st;
   for (; s->pc < s->nc; s->pc++) {
     const int i = a.cand[s->pc];
     if (a.inf[i] == 0) continue;  // cleared by an earlier loop_killer
     const int pari = a.inf[i] - 1, parb = a.beh[i] - 1;
-    const int j = a.closest[i] - 1;
+    const RecEval &r = rec[s->pc];
+    const int j = r.j;
     if (j == pari || j == parb || j < 0) continue;
     if (a.inf[j] == 0) continue;
     const int parjb = a.beh[j] - 1;
-    double t1[3], t2[3];
-    norm_tan(a, i, t1);
-    norm_tan(a, j, t2);
-    const double dot_val = t1[0] * t2[0] + t1[1] * t2[1] + t1[2] * t2[2];
-    if (dot_val > 0.9) continue;  // parallel filaments do not reconnect
-    const double *xi = a.x + 3 * i, *xj = a.x + 3 * j;
-    const double l_before = seg_len(xi, a.gi + 3 * i) + seg_len(xi, a.gb + 3 * i) +
-                            seg_len(xj, a.gi + 3 * j) + seg_len(xj, a.gb + 3 * j);
-    const double l_after = seg_len(xi, a.gb + 3 * i) + seg_len(xi, xj) +
-                           seg_len(xj, a.gi + 3 * j) + seg_len(a.x + 3 * pari, a.x + 3 * parjb);
-    if (l_after <= l_before) {
+    if (r.parallel) continue;  // parallel filaments do not reconnect
+    const double l_after = (pari == r.pari && parjb == r.parjb)
+                               ? r.l_after
+                               : r.s3 + seg_len(a.x + 3 * pari, a.x + 3 * parjb);
+    if (l_after <= r.l_before) {
       a.inf[parjb] = pari + 1;
       a.beh[pari] = parjb + 1;
       a.inf[i] = j + 1;
@@ -331,6 +375,7 @@ static int line_reserve(qv_ctx *c) {
   if (c->line_cap >= n && c->line_st) return QV_OK;
   int rc;
   if ((rc = qv_grow(c, (void **)&c->line_flags, sizeof(int) * 4 * n))) return rc;
+  if ((rc = qv_grow(c, (void **)&c->line_rec, sizeof(RecEval) * n))) return rc;
   if (!c->line_st)
     if ((rc = qv_grow(c, (void **)&c->line_st, sizeof(LineState)))) return rc;
   c->line_cap = n;
@@ -357,12 +402,44 @@ static LineArgs line_args(qv_ctx *c) {
   a.cand = f + 2 * n;
   a.empt = f + 3 * n;
   a.st = (LineState *)c->line_st;
+  a.dstatus = c->dstatus;
   return a;
+}
+
+// Ordered compaction in one block for up to CSMALL slots: each thread counts
+// a contiguous range, a block scan gives the offsets, each thread writes its
+// range's selected slots in order.
+#define CSMALL 65536
+__global__ void __launch_bounds__(1024) k_compact_small(int n, const int *__restrict__ flag,
+                                                        int *out, int *total) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x;
+  const int per = (n + 1023) / 1024, lo = t * per, hi = min(n, lo + per);
+  int cnt = 0;
+  for (int k = lo; k < hi; k++) cnt += flag[k] != 0;
+  part[t] = cnt;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - cnt;
+  for (int k = lo; k < hi; k++)
+    if (flag[k]) out[run++] = k;
+  if (t == 1023) *total = part[1023];
 }
 
 // Ordered compaction of flag[0..n) into out (the active-slot compaction run
 // on a flag array); the count goes to *total on the device.
 static int compact_flags(qv_ctx *c, int n, const int *flag, int *out, int *total) {
+  if (n <= CSMALL) {
+    k_compact_small<<<1, 1024, 0, c->stream>>>(n, flag, out, total);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    return QV_OK;
+  }
   int nb = nblk(n, 256);
   int *tmp = c->blkcnt;
   k_count_active<<<nb, 256, 0, c->stream>>>(n, flag, tmp);
@@ -378,11 +455,6 @@ static int read_state(qv_ctx *c, LineState *h) {
                              c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
   return QV_OK;
-}
-
-static __global__ void k_line_begin(LineState *s, int n) {
-  s->pc = 0; s->epos = 0; s->n_old = n; s->n_cur = n; s->last = -1; s->heap_n = 0;
-  s->status = 0; s->done = 0;
 }
 
 static __global__ void k_line_clear_status(LineState *s) { s->status = 0; }
@@ -401,10 +473,9 @@ int qv_line_insert(qv_ctx *c, int *inserted) {
   if ((rc = line_reserve(c))) return rc;
   LineArgs a = line_args(c);
   const int n = c->n;
-  k_line_begin<<<1, 1, 0, c->stream>>>(a.st, n);
   k_ins_flags<<<nblk(n, 256), 256, 0, c->stream>>>(n, a);
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 2);
+  QV_COUNT(c, 1);
   if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
   if ((rc = compact_flags(c, n, a.flag_b, (int *)a.empt, &a.st->ne))) return rc;
   LineState h;
@@ -435,14 +506,15 @@ int qv_line_reconnect(qv_ctx *c, int *count) {
   if ((rc = line_reserve(c))) return rc;
   LineArgs a = line_args(c);
   const int n = c->n;
-  k_line_begin<<<1, 1, 0, c->stream>>>(a.st, n);
   k_rec_flags<<<nblk(n, 256), 256, 0, c->stream>>>(n, a);
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 2);
-  if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
-  k_precon_seq<<<1, 1, 0, c->stream>>>(a);
-  QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
+  if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
+  RecEval *rec = (RecEval *)c->line_rec;
+  k_rec_eval<<<nblk(n, 128), 128, 0, c->stream>>>(n, a, rec);
+  k_precon_seq<<<1, 1, 0, c->stream>>>(a, rec);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 2);
   if (count) {
     LineState h;
     if ((rc = read_state(c, &h))) return rc;
@@ -457,17 +529,20 @@ int qv_line_remove(qv_ctx *c, int *removed) {
   if ((rc = line_reserve(c))) return rc;
   LineArgs a = line_args(c);
   const int n = c->n;
-  k_line_begin<<<1, 1, 0, c->stream>>>(a.st, n);
   k_rem_flags<<<nblk(n, 256), 256, 0, c->stream>>>(n, a);
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 2);
+  QV_COUNT(c, 1);
   if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
   k_premove_seq<<<1, 1, 0, c->stream>>>(a);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
-  LineState h;
-  if ((rc = read_state(c, &h))) return rc;
-  if (h.status == 2) return qv_fail(c, QV_ERR_STATE, "premove: more than %d re-tests pending", LHEAP);
-  if (removed) *removed = h.done;
+  // without a count to return, an overflow is reported through the status
+  // word at the step's end instead of a wait here
+  if (removed) {
+    LineState h;
+    if ((rc = read_state(c, &h))) return rc;
+    if (h.status == 2) return qv_fail(c, QV_ERR_STATE, "premove: more than %d re-tests pending", LHEAP);
+    *removed = h.done;
+  }
   return QV_OK;
 }

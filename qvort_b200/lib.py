@@ -351,9 +351,9 @@ class Context:
         self._check(_lib.qv_premove(self._h, C.byref(k)))
         return k.value
 
-    def get_links(self):
-        inf = np.empty(self.n, np.int32)
-        beh = np.empty(self.n, np.int32)
+    def get_links(self, inf=None, beh=None):
+        inf = np.empty(self.n, np.int32) if inf is None else inf
+        beh = np.empty(self.n, np.int32) if beh is None else beh
         self._check(_lib.qv_get_links(self._h, _ptr(inf), _ptr(beh)))
         return inf, beh
 
