@@ -67,8 +67,8 @@ struct BatchArgs {
 // order), the unshifted image restricted to root child sl: the same task as
 // the single-system mixed walk (its main image, without periodic images).
 __device__ __forceinline__ void walk_item(const BatchArgs &a, StkEnt *st, int g, int sl,
-                                          const int *perm, unsigned long long &ev,
-                                          unsigned long long &evf, bool &bad) {
+                                          const int *perm, unsigned &ev, unsigned &evf,
+                                          bool &bad) {
   const int lane = threadIdx.x & 31;
   const int4 G = a.groups[g];
   const int q = G.x + lane;
@@ -156,9 +156,8 @@ __device__ __forceinline__ void walk_item(const BatchArgs &a, StkEnt *st, int g,
     } else {
       bool open = false;
       if (in) {
-        float diff = d2 - h.rc2;
-        if (h.rc2 > 0.f && fabsf(diff) > 4e-6f * h.rc2) {
-          open = diff <= 0.f;
+        if (h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo)) {
+          open = d2 < h.rlo;
         } else {
           const WNode64 h64 = a.w64[node];
           open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
@@ -283,7 +282,7 @@ __global__ void k_batch_work(BatchArgs a) {
   if (*a.status) return;
   if (a.nroots > 0 && a.ctl[QV_CTL_OVERFLOW]) return;
   const int *perm = a.nroots > 0 ? a.ord + (size_t)a.ctl[QV_CTL_DEPTH] * a.cap_pts : nullptr;
-  unsigned long long ev = 0, evf = 0;
+  unsigned ev = 0, evf = 0;  // per warp: far below 2^32
   bool bad = false;
   for (;;) {
     int it = 0;
@@ -300,8 +299,8 @@ __global__ void k_batch_work(BatchArgs a) {
     ev += __shfl_down_sync(0xffffffffu, ev, o);
     evf += __shfl_down_sync(0xffffffffu, evf, o);
   }
-  if (lane == 0 && ev) atomicAdd(a.evals, ev);
-  if (lane == 0 && evf) atomicAdd(a.evals_far, evf);
+  if (lane == 0 && ev) atomicAdd(a.evals, (unsigned long long)ev);
+  if (lane == 0 && evf) atomicAdd(a.evals_far, (unsigned long long)evf);
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, BST_SINGULAR);
 }
 

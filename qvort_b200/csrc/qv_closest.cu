@@ -90,9 +90,8 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
           pass = true;
         } else {
           // theta = width/dist < 0.5  (src/tree.f90:248-249)  <=>  dist^2 > (2 width)^2
-          float diff = d2 - h.w4;
-          if (!tiny && fabsf(diff) > 4e-6f * h.w4) {
-            pass = diff > 0.f;
+          if (!tiny && (d2 > h.rhi || d2 < h.rlo)) {
+            pass = d2 > h.rhi;
           } else {
             const WNode64 hh = w64[node];
             d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
@@ -217,7 +216,7 @@ int qv_launch_closest(qv_ctx *c) {
       }
     }
     k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, smem, c->stream>>>(
-        c->n, c->x, c->infront, c->behind, c->tree.w64, c->tree.w32, cap, c->closest,
+        c->n, c->x, c->infront, c->behind, c->tree.w64, c->tree.c32, cap, c->closest,
         c->closestd, c->dstatus);
   } else {
     k_pclose<<<(c->n + PT - 1) / PT, PT, 0, c->stream>>>(c->n, c->x, c->infront, c->behind,

@@ -40,13 +40,16 @@ struct __align__(16) WPay64 {
 };
 
 // FP32 header (48 B): cent as a two-float (hi, lo) split of the FP64 value so
-// that target-source differences keep FP64-level information, and the two
-// opening radii squared: rc2 for the velocity walk and w4 for the candidate
-// search (see k_pack_nodes).
+// that target-source differences keep FP64-level information, and the node's
+// opening radius squared widened by a relative 4e-6 either way: a squared
+// distance above rhi passes the test, one below rlo fails it, one in between
+// is decided by the reference's FP64 expression.  Two arrays of headers: w32
+// for the velocity walk (radius geo + width/theta; rhi = rlo = -1 when only
+// the FP64 test is valid) and c32 for the candidate search (radius 2 width:
+// theta = width/dist < 0.5).  See k_pack_nodes.
 struct __align__(16) WNode32 {
   float ch[3], cl[3];
-  float rc2;  // (geo + width/theta)^2, or -1 when only the FP64 test is valid
-  float w4;   // (2 width)^2: theta = width/dist < 0.5 <=> dist^2 > w4
+  float rhi, rlo;
   int count, child_first, nchild, jb;
 };
 
@@ -73,7 +76,7 @@ struct TreeBuf {
   // walk packs
   WNode64 *w64 = nullptr;
   WPay64 *p64 = nullptr;
-  WNode32 *w32 = nullptr;
+  WNode32 *w32 = nullptr, *c32 = nullptr;
   WPay32 *p32 = nullptr;
   // build scratch
   int *ord = nullptr;       // cap_levels * cap_pts: per-level orders

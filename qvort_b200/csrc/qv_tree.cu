@@ -591,7 +591,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const int *__restrict__ nchild, const int *__restrict__ first,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
-                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
+                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, WNode32 *c32,
                           WPay32 *p32);
 
 __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nroots,
@@ -602,13 +602,13 @@ __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nro
                              const int *__restrict__ nchild, const int *__restrict__ first,
                              const double *__restrict__ x, const double *__restrict__ gi,
                              const int *__restrict__ inf, const int *__restrict__ beh,
-                             double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
+                             double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, WNode32 *c32,
                              WPay32 *p32) {
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
     pack_node(k, nroots, pos, width, cent, circ, C, count, child_first, nchild, first, x, gi, inf,
-              beh, theta, extra, w64, p64, w32, p32);
+              beh, theta, extra, w64, p64, w32, c32, p32);
 }
 
 __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
@@ -618,7 +618,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const int *__restrict__ nchild, const int *__restrict__ first,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
-                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32,
+                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, WNode32 *c32,
                           WPay32 *p32) {
   WNode64 h;
   h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
@@ -654,18 +654,25 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
   // margin and falls back to the FP64 expression near the threshold.  The root
   // (centroid anywhere, zero moments) always takes the FP64 path.
   bool fast = theta > 0. && (!extra || theta < 1.15);
-  if (root || !fast) {
-    h32.rc2 = -1.f;
-  } else {
-    double rc = (extra ? h.geo : 0.) + h.width / theta;
-    h32.rc2 = __double2float_rn(rc * rc);
-  }
-  h32.w4 = __double2float_rn(4. * h.width * h.width);
   h32.count = cnt;
   h32.child_first = h.child_first;
   h32.nchild = h.nchild;
   h32.jb = h.jb;
+  if (root || !fast) {
+    h32.rhi = h32.rlo = -1.f;
+  } else {
+    double rc = (extra ? h.geo : 0.) + h.width / theta;
+    double rc2 = rc * rc;
+    h32.rhi = __double2float_rn(rc2 * (1. + 4e-6));
+    h32.rlo = __double2float_rn(rc2 * (1. - 4e-6));
+  }
   w32[k] = h32;
+  {
+    double w4 = 4. * h.width * h.width;  // (2 width)^2
+    h32.rhi = __double2float_rn(w4 * (1. + 4e-6));
+    h32.rlo = __double2float_rn(w4 * (1. - 4e-6));
+  }
+  c32[k] = h32;
   if (cnt == 1 && f >= 0) {
     for (int c = 0; c < 3; c++) {
       q.a[c] = x[3 * f + c];
@@ -819,6 +826,7 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
     if ((rc = qv_grow(c, (void **)&t.w64, sizeof(WNode64) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.p64, sizeof(WPay64) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.w32, sizeof(WNode32) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.c32, sizeof(WNode32) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.p32, sizeof(WPay32) * m))) return rc;
     t.cap_nodes = cap_nodes;
   }
@@ -926,7 +934,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
         t.ctl, t.cap_nodes, 1, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
         t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
-        c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.p32);
+        c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 2);
     qv_phase_end_async(c, PH_BUILD_MOMENTS);
@@ -1017,7 +1025,7 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
       t.ctl, t.cap_nodes, f.nroots, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
       t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
-      c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.p32);
+      c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 7);
   return QV_OK;

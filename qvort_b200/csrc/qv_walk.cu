@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
     }
     Kahan3w k0;
     k0.zero();
-    unsigned long long ev = 0, evf = 0;
+    unsigned ev = 0, evf = 0;  // per task: far below 2^32
     bool bad = false;
     int ma, mb, mc;
     slot_image(BC, sl, ma, mb, mc);
@@ -303,9 +303,8 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
         if (in) {
           // accept (far field) iff d^2 > rc2, decided in FP32 outside a
           // relative margin of 4e-6 and by the reference's FP64 test inside it
-          float diff = d2 - h.rc2;
-          if (h.rc2 > 0.f && fabsf(diff) > 4e-6f * h.rc2) {
-            open = diff <= 0.f;
+          if (h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo)) {
+            open = d2 < h.rlo;
           } else {
             const WNode64 h64 = a.w64[node];
             open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
@@ -358,8 +357,8 @@ __global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
       ev += __shfl_down_sync(0xffffffffu, ev, o);
       evf += __shfl_down_sync(0xffffffffu, evf, o);
     }
-    if (lane == 0 && ev) atomicAdd(a.evals, ev);
-    if (lane == 0 && evf) atomicAdd(a.evals_far, evf);
+    if (lane == 0 && ev) atomicAdd(a.evals, (unsigned long long)ev);
+    if (lane == 0 && evf) atomicAdd(a.evals_far, (unsigned long long)evf);
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, 1);
   }
 }
