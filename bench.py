@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--suite", default="tangle", choices=["tangle", "batch", "gradient", "large"],
+    ap.add_argument("--suite", default="tangle",
+                    choices=["tangle", "batch", "gradient", "large", "ring"],
                     help="tangle: the headline line; batch / gradient / large: only that "
                          "workload's entry")
     ap.add_argument("--quick", action="store_true",
@@ -482,6 +483,43 @@ def gradient_rate(L, torch, steps: int = 256, reps: int = 2) -> dict:
                         "loss = E(x_K) + sum |x_K - x_0|^2; wall clock"}
 
 
+def ring_rate(L, torch, steps: int = 1000) -> dict:
+    """The single ring: N = 200, R = 0.01 cm, radial noise 1e-5, open, direct
+    Biot-Savart + LIA in FP64, dt 1e-7, 1000 AB steps through qv_step, against
+    the oracle's own steps on one host core; and the ring's translational
+    speed against the formula the reference prints (src/initial_loop.f90:17-19)."""
+    from oracle import oracle as O
+    from qvort_b200 import workloads as W
+
+    w = W.ring()
+    c = L.Context(L.default_params(**dict(w.params, precision="fp64")))
+    c.set_points(w.x, w.infront, w.behind)
+    c.step(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in range(2, steps + 2):
+        c.step(it)
+    gpu_s = (time.perf_counter() - t0) / steps
+    x, u = c.get_points()
+    c.close()
+    R = 0.01
+    v_ref = w.params["quant_circ"] / (4 * np.pi * R) * (np.log(8 * R / w.params["corea"]) - 0.5)
+    st = O.State(O.params(**w.params), w.x, w.infront, w.behind)
+    st.step()
+    t0 = time.perf_counter()
+    k = 50
+    for _ in range(k):
+        st.step()
+    cpu_s = (time.perf_counter() - t0) / k
+    n = w.n
+    return {"workload": "ring N=200, R=0.01 cm, open, BS direct + LIA, FP64, dt 1e-7",
+            "gpu_ms_per_step": gpu_s * 1e3, "gpu_steps_per_s": 1. / gpu_s,
+            "gpu_pairs_per_s": n * n / gpu_s, "cpu_ms_per_step": cpu_s * 1e3,
+            "cpu_steps_per_s": 1. / cpu_s, "cpu_cores": 1, "cpu_kind": "port",
+            "ring_speed_cm_s": float(abs(np.mean(u[:, 2]))), "formula_speed_cm_s": float(v_ref),
+            "timing": "wall clock around qv_step (one host wait per step)"}
+
+
 def large_rate(L, torch, steps: int = 5, warmup: int = 3) -> dict:
     """The large isotropic tangle: 3000 random rings, R ~ U(0.004, 0.015) cm,
     delta 3e-4 cm, periodic L = 0.1, Barnes-Hut theta 0.5, candidate search every
@@ -594,6 +632,8 @@ def main():
             r = batch_rate(L, torch, args.steps)
         elif args.suite == "large":
             r = large_rate(L, torch, args.steps, args.warmup)
+        elif args.suite == "ring":
+            r = ring_rate(L, torch)
         else:
             r = gradient_rate(L, torch)
         print(json.dumps({"suite": args.suite, **r}), flush=True)
