@@ -149,6 +149,16 @@ int qv_energy(qv_ctx *ctx, double *energy);
  * ghostp, construct_tree, pmotion/pmotion_RK3, the candidate search when
  * itime % recon_shots == 0, ghostp, boundary wrap.  Device-resident. */
 int qv_step(qv_ctx *ctx, int itime);
+/* nsteps steps itime0, itime0+1, ... with the results of calling qv_step for
+ * each.  When the point set cannot change and no step needs a host decision
+ * (Adams-Bashforth, line_ops 0, tree_theta 0 with velocity BS, LIA or Off, a
+ * context stream other than the legacy or per-thread default stream), the
+ * steps after the first are replayed from a CUDA graph of one step and the
+ * call waits once, at the end; a singularity is then reported after the last
+ * step rather than at the step where it occurred.  Otherwise it loops over
+ * qv_step.  Not a reference routine: it is the time loop of src/run.f90:36-107
+ * run nsteps times between two outputs. */
+int qv_steps(qv_ctx *ctx, int itime0, int nsteps);
 
 /* ------------------------------------------------------------- derivatives
  * Hand-written derivatives of the path (no counterpart in the reference, which

@@ -602,6 +602,106 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
   return velocity_collect(c, nullptr);  // one wait per step; reports any status
 }
 
+// One step of qv_step's sequence for a point set that does not change (no
+// line operations) and needs no host decision inside the step (direct, LIA or
+// no non-local velocity; Adams-Bashforth): everything is enqueued, nothing
+// waits.  The active list and the direct sum's chunking come from the call
+// that set them up.
+static int enqueue_fixed_step(qv_ctx *c, bool search) {
+  int rc;
+  if ((rc = qv_launch_ghosts(c))) return rc;                     // run.f90:41
+  if ((rc = qv_launch_lia(c))) return rc;                        // timestep.f90:196-225
+  if (c->p.velocity == QV_VEL_BS)
+    if ((rc = qv_launch_direct(c))) return rc;                   // timestep.f90:226-258
+  if ((rc = qv_launch_ab(c))) return rc;                         // timestep.f90:48-71
+  if (search)
+    if ((rc = qv_launch_closest(c))) return rc;                  // run.f90:63-69
+  if ((rc = qv_launch_ghosts(c))) return rc;                     // run.f90:75
+  if ((rc = qv_launch_wrap(c))) return rc;                       // run.f90:82-93
+  return QV_OK;
+}
+
+static int capture_step(qv_ctx *c, bool search, cudaGraphExec_t *exec, long long *launches) {
+  *exec = nullptr;
+  long long l0 = c->launches;
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return QV_ERR_UNSUPPORTED;
+  }
+  int rc = enqueue_fixed_step(c, search);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  *launches = c->launches - l0;
+  c->launches = l0;
+  if (rc || e != cudaSuccess || !g) {
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    return rc ? rc : QV_ERR_UNSUPPORTED;
+  }
+  e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *exec = nullptr;
+    return QV_ERR_UNSUPPORTED;
+  }
+  return QV_OK;
+}
+
+extern "C" int qv_steps(qv_ctx *c, int itime0, int nsteps) {
+  QV_CHECK_CTX(c);
+  if (nsteps < 0) return qv_fail(c, QV_ERR_ARG, "nsteps must be >= 0");
+  if (nsteps == 0) return QV_OK;
+  int rc;
+  const bool fixed = !c->p.runge_kutta && c->p.line_ops == 0 && c->p.tree_theta == 0. &&
+                     c->p.velocity != QV_VEL_TREE && !c->profile &&
+                     c->stream != nullptr && c->stream != cudaStreamLegacy &&
+                     c->stream != cudaStreamPerThread;
+  // the first step through qv_step: it sizes every buffer and checks the state
+  if ((rc = qv_step(c, itime0))) return rc;
+  if (nsteps == 1) return QV_OK;
+  if (!fixed) {
+    for (int k = 1; k < nsteps; k++)
+      if ((rc = qv_step(c, itime0 + k))) return rc;
+    return QV_OK;
+  }
+  // the links do not change: one compaction serves every step
+  if ((rc = qv_compact_active(c))) return rc;
+  cudaGraphExec_t g_search = nullptr, g_plain = nullptr;
+  long long l_search = 0, l_plain = 0;
+  bool need_plain = c->p.recon_shots > 1;
+  rc = capture_step(c, true, &g_search, &l_search);
+  if (!rc && need_plain) rc = capture_step(c, false, &g_plain, &l_plain);
+  if (rc) {
+    // capture refused (a stream that cannot be captured): step one by one
+    if (g_search) cudaGraphExecDestroy(g_search);
+    c->err[0] = 0;
+    for (int k = 1; k < nsteps; k++)
+      if ((rc = qv_step(c, itime0 + k))) return rc;
+    return QV_OK;
+  }
+  QV_CUDA(c, cudaMemsetAsync(c->dstatus, 0, sizeof(int), c->stream));
+  for (int k = 1; k < nsteps; k++) {
+    const bool search = (itime0 + k) % c->p.recon_shots == 0;
+    cudaError_t e = cudaGraphLaunch(search ? g_search : g_plain, c->stream);
+    if (e != cudaSuccess) {
+      cudaGraphExecDestroy(g_search);
+      if (g_plain) cudaGraphExecDestroy(g_plain);
+      return qv_fail(c, QV_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(e));
+    }
+    c->launches += search ? l_search : l_plain;
+  }
+  int st = 0;
+  QV_CUDA(c, cudaMemcpyAsync(&st, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  cudaGraphExecDestroy(g_search);
+  if (g_plain) cudaGraphExecDestroy(g_plain);
+  c->ghosts_valid = false;
+  if (st & 1)
+    return qv_fail(c, QV_ERR_SINGULAR, "singularity in BS velocity field during qv_steps");
+  return QV_OK;
+}
+
 extern "C" int qv_pinsert(qv_ctx *c, int *inserted) {
   QV_CHECK_CTX(c);
   if (!(c->p.delta > 0)) return qv_fail(c, QV_ERR_ARG, "pinsert needs delta > 0");

@@ -1,7 +1,7 @@
 // qvort_run -- a C++ stand-in for the reference's driver (src/run.f90) that
 // runs the velocity-and-timestep path of this library from a run.in:
 //   read_run_file -> initial condition (var_file, single_loop, leap-frog) ->
-//   do itime = 1, nsteps: qv_step (ghostp, construct_tree, pmotion /
+//   do itime = 1, nsteps: qv_steps between outputs (ghostp, construct_tree, pmotion /
 //   pmotion_RK3, pinsert, candidate search, precon unless switch_off_recon,
 //   premove, ghostp, boundary wrap), t = t + dt;
 //   every `shots` steps: data/var%04d.log and a one-line summary, STOP file.
@@ -71,13 +71,18 @@ int main(int argc, char **argv) {
   mkdir("data", 0755);
   std::vector<double> u(3 * (size_t)n);
   int shot = 0;
-  for (int itime = 1; itime <= r.nsteps; itime++) {
-    if ((rc = qv_step(ctx, itime))) {
-      std::fprintf(stderr, "qvort_run: step %d: %s\n", itime, qv_last_error(ctx));
+  for (int first = 1; first <= r.nsteps;) {
+    // the steps up to the next output in one call (qv_steps replays a CUDA
+    // graph of a step when the options allow it)
+    int itime = r.shots > 0 ? ((first + r.shots - 1) / r.shots) * r.shots : r.nsteps;
+    if (itime > r.nsteps) itime = r.nsteps;
+    if ((rc = qv_steps(ctx, first, itime - first + 1))) {
+      std::fprintf(stderr, "qvort_run: steps %d-%d: %s\n", first, itime, qv_last_error(ctx));
       qv_destroy(ctx);
       return 3;
     }
-    t = t + r.p.dt;
+    for (int k = first; k <= itime; k++) t = t + r.p.dt;
+    first = itime + 1;
     if (r.shots > 0 && itime % r.shots == 0) {
       // insertion can raise the slot count and every line operation relinks
       qv_point_count(ctx, &n);

@@ -113,6 +113,7 @@ _SIGS = {
     "qv_closest": [_P, _P, _P],
     "qv_energy": [_P, _D],
     "qv_step": [_P, C.c_int],
+    "qv_steps": [_P, C.c_int, C.c_int],
     "qv_sync": [_P],
     "qv_profile": [_P, C.c_int],
     "qv_phase_times": [_P, _P, C.c_int],
@@ -365,6 +366,11 @@ class Context:
 
     def step(self, itime: int = 1):
         self._check(_lib.qv_step(self._h, itime))
+        if self.params.line_ops:
+            self._sync_count()
+
+    def steps(self, itime0: int, nsteps: int):
+        self._check(_lib.qv_steps(self._h, itime0, nsteps))
         if self.params.line_ops:
             self._sync_count()
 

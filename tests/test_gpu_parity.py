@@ -357,3 +357,36 @@ def test_coincident_points_off_origin_match_oracle(L):
     t = O.Tree(p, x, og[0], inf)
     assert t.status == 0
     _compare_trees(gt, t.export())
+
+
+@pytest.mark.parametrize("velocity,boundary,recon_shots", [("BS", "open", 1), ("BS", "periodic", 3),
+                                                            ("LIA", "open", 1)])
+def test_steps_replay_equals_step_loop(velocity, boundary, recon_shots):
+    """qv_steps (a CUDA graph of one step, replayed) leaves the same state as
+    calling qv_step for each step: positions, history and candidate pairs."""
+    import torch
+
+    from qvort_b200 import lib as L
+    from qvort_b200 import workloads as W
+
+    w = W.random_rings(4, 0.006, 0.01, 5e-4, 0.1, seed=6, centre_box=0.05)
+    prm = dict(w.params, velocity=velocity, boundary=boundary, tree_theta=0.0,
+               recon_shots=recon_shots, precision="fp64")
+    s = torch.cuda.Stream()
+    a = L.Context(L.default_params(**prm), stream=s.cuda_stream)
+    b = L.Context(L.default_params(**prm), stream=s.cuda_stream)
+    for c in (a, b):
+        c.set_points(w.x, w.infront, w.behind)
+    a.steps(1, 12)
+    for it in range(1, 13):
+        b.step(it)
+    xa, ua = a.get_points()
+    xb, ub = b.get_points()
+    assert np.array_equal(xa, xb) and np.array_equal(ua, ub)
+    for ha, hb in zip(a.get_history(), b.get_history()):
+        assert np.array_equal(ha, hb)
+    ca, da = a.get_closest()
+    cb, db = b.get_closest()
+    assert np.array_equal(ca, cb) and np.array_equal(da, db)
+    a.close()
+    b.close()
