@@ -415,17 +415,11 @@ def extras(ctx, w, stream, L, torch, itime):
 
     def e2e_step(it):
         m = cur[0]
-        c.set_points(hx[:m], hinf[:m], hbeh[:m])
-        c.set_history(*[h[:m] for h in hist])
-        c.set_closest(hcl[:m])
+        c.set_state(m, x=hx, infront=hinf, behind=hbeh, u1=hist[0], u2=hist[1], u3=hist[2],
+                    closest=hcl)
         c.step(it)
-        m = cur[0] = c.n
-        if m > cap:
-            raise RuntimeError("more insertions than the host buffers hold")
-        c.get_points(hx[:m], hu[:m])
-        c.get_history(*[h[:m] for h in hist])
-        c.get_closest(hcl[:m], hcd[:m])
-        c.get_links(hinf[:m], hbeh[:m])
+        m = cur[0] = c.get_state(cap, x=hx, u=hu, u1=hist[0], u2=hist[1], u3=hist[2],
+                                 infront=hinf, behind=hbeh, closest=hcl, closestd=hcd)
         moved[0] += m * (24 + 8 + 72 + 4)         # x, links, history, closest in
         moved[1] += m * (24 + 24 + 72 + 4 + 8 + 8)  # x, u, history, closest(d), links out
 
@@ -443,9 +437,9 @@ def extras(ctx, w, stream, L, torch, itime):
     out["e2e"] = {"value": pairs_step / (e2e_ms * 1e-3), "unit": UNIT,
                   "h2d_bytes_per_step": moved[0] // K, "d2h_bytes_per_step": moved[1] // K,
                   "ms_per_step": e2e_ms,
-                  "path": "qv_set_points/qv_set_history/qv_set_closest (pinned host) -> qv_step "
-                          "(line_ops 2) -> qv_get_points/qv_get_history/qv_get_closest/"
-                          "qv_get_links (pinned host), wall clock"}
+                  "path": "qv_set_state (pinned host: x, links, AB history, closest) -> "
+                          "qv_step (line_ops 2) -> qv_get_state (pinned host: x, u, history, "
+                          "links, closest, closestd), wall clock"}
 
     # ---- gradients/s on the differentiation workload: 16 trefoil rings,
     # N = 50,000, periodic, K = 256 Adams-Bashforth steps checkpointed every 16,

@@ -104,6 +104,21 @@ int qv_set_closest(qv_ctx *ctx, const int *closest);
 int qv_get_points(qv_ctx *ctx, double *x, double *u);
 /* Scatter back f(:)%closest and f(:)%closestd of the last candidate search. */
 int qv_get_closest(qv_ctx *ctx, int *closest, double *closestd);
+
+/* The per-point state a host copy of f(:) exchanges with the path each step
+ * (src/cdata.f90:20-39): host arrays of 3n (vectors) or n (scalars) entries.
+ * qv_set_state is qv_set_points + qv_set_history + qv_set_closest in one call
+ * (u1..u3 or closest NULL: zeros; u and closestd are not read); qv_get_state
+ * copies every non-NULL array back for the n slots in use (*n), or returns
+ * QV_ERR_ARG with *n set when n exceeds cap (insertion grew the slot count:
+ * the host grows its arrays and calls again).  One wait each. */
+typedef struct qv_state {
+  double *x, *u, *u1, *u2, *u3;
+  int *infront, *behind, *closest;
+  double *closestd;
+} qv_state;
+int qv_set_state(qv_ctx *ctx, int n, const qv_state *s);
+int qv_get_state(qv_ctx *ctx, int cap, qv_state *s, int *n);
 /* Device pointers of the context's arrays (valid until the next set_points). */
 int qv_device_arrays(qv_ctx *ctx, double **x, double **u, int **infront, int **behind);
 

@@ -318,6 +318,62 @@ extern "C" int qv_get_closest(qv_ctx *c, int *closest, double *closestd) {
   return QV_OK;
 }
 
+// The whole per-step exchange with a host copy of f(:) in one call each way,
+// with one wait: the host arrays are free to reuse when the call returns.
+extern "C" int qv_set_state(qv_ctx *c, int n, const qv_state *s) {
+  QV_CHECK_CTX(c);
+  if (!s || n < 0 || (n > 0 && (!s->x || !s->infront || !s->behind)))
+    return qv_fail(c, QV_ERR_ARG, "qv_set_state: x, infront and behind are required");
+  int rc = reserve_points(c, std::max(n, 1));
+  if (rc) return rc;
+  c->n = n;
+  if (n > 0) {
+    const size_t v = sizeof(double) * 3 * (size_t)n;
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    QV_CUDA(c, cudaMemcpyAsync(c->x, s->x, v, h2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->infront, s->infront, sizeof(int) * n, h2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->behind, s->behind, sizeof(int) * n, h2d, c->stream));
+    const double *hs[] = {s->u1, s->u2, s->u3};
+    double *hd[] = {c->u1, c->u2, c->u3};
+    for (int k = 0; k < 3; k++) {
+      if (hs[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], hs[k], v, h2d, c->stream));
+      else QV_CUDA(c, cudaMemsetAsync(hd[k], 0, v, c->stream));
+    }
+    if (s->closest) QV_CUDA(c, cudaMemcpyAsync(c->closest, s->closest, sizeof(int) * n, h2d, c->stream));
+    else QV_CUDA(c, cudaMemsetAsync(c->closest, 0, sizeof(int) * n, c->stream));
+    double *zv[] = {c->u, c->u_li, c->u_bs};
+    for (double *q : zv) QV_CUDA(c, cudaMemsetAsync(q, 0, v, c->stream));
+    QV_CUDA(c, cudaMemsetAsync(c->closestd, 0, sizeof(double) * n, c->stream));
+  }
+  c->ghosts_valid = false;
+  c->ghosts_stored = false;
+  c->tree.valid = false;
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+extern "C" int qv_get_state(qv_ctx *c, int cap, qv_state *s, int *n) {
+  QV_CHECK_CTX(c);
+  if (!s || !n) return qv_fail(c, QV_ERR_ARG, "qv_get_state: null state or count");
+  *n = c->n;
+  if (c->n > cap)
+    return qv_fail(c, QV_ERR_ARG, "qv_get_state: %d slots in use, host arrays hold %d", c->n, cap);
+  if (c->n == 0) return QV_OK;
+  const size_t v = sizeof(double) * 3 * (size_t)c->n, ni = sizeof(int) * (size_t)c->n;
+  const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
+  double *hd[] = {s->x, s->u, s->u1, s->u2, s->u3};
+  const double *dd[] = {c->x, c->u, c->u1, c->u2, c->u3};
+  for (int k = 0; k < 5; k++)
+    if (hd[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], dd[k], v, d2h, c->stream));
+  if (s->infront) QV_CUDA(c, cudaMemcpyAsync(s->infront, c->infront, ni, d2h, c->stream));
+  if (s->behind) QV_CUDA(c, cudaMemcpyAsync(s->behind, c->behind, ni, d2h, c->stream));
+  if (s->closest) QV_CUDA(c, cudaMemcpyAsync(s->closest, c->closest, ni, d2h, c->stream));
+  if (s->closestd)
+    QV_CUDA(c, cudaMemcpyAsync(s->closestd, c->closestd, sizeof(double) * c->n, d2h, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
 extern "C" int qv_device_arrays(qv_ctx *c, double **x, double **u, int **inf, int **beh) {
   QV_CHECK_CTX(c);
   if (x) *x = c->x;

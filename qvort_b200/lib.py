@@ -69,6 +69,11 @@ class QvRun(C.Structure):
     ]
 
 
+class QvState(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("x", "u", "u1", "u2", "u3", "infront", "behind",
+                                          "closest", "closestd")]
+
+
 class QvError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"qv error {code}: {msg}")
@@ -113,6 +118,8 @@ _SIGS = {
     "qv_closest": [_P, _P, _P],
     "qv_energy": [_P, _D],
     "qv_step": [_P, C.c_int],
+    "qv_set_state": [_P, C.c_int, C.POINTER(QvState)],
+    "qv_get_state": [_P, C.c_int, C.POINTER(QvState), _I],
     "qv_steps": [_P, C.c_int, C.c_int],
     "qv_sync": [_P],
     "qv_profile": [_P, C.c_int],
@@ -242,6 +249,25 @@ class Context:
     def set_points_device(self, n: int, x_ptr: int, inf_ptr: int, beh_ptr: int):
         self._check(_lib.qv_set_points_device(self._h, n, x_ptr, inf_ptr, beh_ptr))
         self.n = n
+
+    @staticmethod
+    def _state(arrays) -> QvState:
+        return QvState(*[None if arrays.get(k) is None else _ptr(arrays[k])
+                         for k, _ in QvState._fields_])
+
+    def set_state(self, n: int, **arrays):
+        """One upload of x, infront, behind (required), u1..u3, closest (optional;
+        host arrays of at least n entries, contiguous)."""
+        self._check(_lib.qv_set_state(self._h, n, C.byref(self._state(arrays))))
+        self.n = n
+
+    def get_state(self, cap: int, **arrays) -> int:
+        """One download into the given host arrays (capacity cap slots); returns
+        the slot count in use."""
+        m = C.c_int()
+        self._check(_lib.qv_get_state(self._h, cap, C.byref(self._state(arrays)), C.byref(m)))
+        self.n = m.value
+        return m.value
 
     def set_history(self, u1=None, u2=None, u3=None):
         arrs = [None if u is None else _f64(u, self.n) for u in (u1, u2, u3)]

@@ -24,6 +24,11 @@ module qv_iface
     integer(c_int) :: line_ops
   end type
 
+  ! the per-step exchange of qv_set_state / qv_get_state (host arrays by address)
+  type, bind(C) :: qv_state_t
+    type(c_ptr) :: x, u, u1, u2, u3, infront, behind, closest, closestd
+  end type
+
   interface
     integer(c_int) function qv_default_params(p) bind(C, name='qv_default_params')
       import :: qv_params_t
@@ -93,12 +98,25 @@ module qv_iface
       import :: c_ptr
       type(c_ptr), value :: ctx
     end function
+    integer(c_int) function qv_set_state(ctx, n, s) bind(C, name='qv_set_state')
+      import :: c_ptr, c_int, qv_state_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      type(qv_state_t), intent(in) :: s
+    end function
+    integer(c_int) function qv_get_state(ctx, cap, s, n) bind(C, name='qv_get_state')
+      import :: c_ptr, c_int, qv_state_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: cap
+      type(qv_state_t), intent(in) :: s
+      integer(c_int), intent(out) :: n
+    end function
   end interface
 
   type(c_ptr), save :: ctx = c_null_ptr
-  real(c_double), allocatable, save :: xs(:,:), us(:,:), h1(:,:), h2(:,:), h3(:,:)
-  real(c_double), allocatable, save :: cds(:), uli(:,:), ubs(:,:)
-  integer(c_int), allocatable, save :: infs(:), behs(:), cls(:)
+  real(c_double), allocatable, target, save :: xs(:,:), us(:,:), h1(:,:), h2(:,:), h3(:,:)
+  real(c_double), allocatable, target, save :: cds(:), uli(:,:), ubs(:,:)
+  integer(c_int), allocatable, target, save :: infs(:), behs(:), cls(:)
 
 contains
 
@@ -167,15 +185,20 @@ contains
     h2(1,:) = f(:)%u2(1) ; h2(2,:) = f(:)%u2(2) ; h2(3,:) = f(:)%u2(3)
     h3(1,:) = f(:)%u3(1) ; h3(2,:) = f(:)%u3(2) ; h3(3,:) = f(:)%u3(3)
     infs = f(:)%infront ; behs = f(:)%behind ; cls = f(:)%closest
-    call check(qv_set_points(ctx, int(n, c_int), xs, infs, behs), 'qv_iface:qv_set_points')
-    call check(qv_set_history(ctx, h1, h2, h3), 'qv_iface:qv_set_history')
-    call check(qv_set_closest(ctx, cls), 'qv_iface:qv_set_closest')
+    call check(qv_set_state(ctx, int(n, c_int), state()), 'qv_iface:qv_set_state')
   end subroutine
 
+  function state() result(s)
+    type(qv_state_t) :: s
+    s%x = c_loc(xs) ; s%u = c_loc(us) ; s%u1 = c_loc(h1) ; s%u2 = c_loc(h2) ; s%u3 = c_loc(h3)
+    s%infront = c_loc(infs) ; s%behind = c_loc(behs) ; s%closest = c_loc(cls)
+    s%closestd = c_loc(cds)
+  end function
+
+  !> the slot count does not change here (line operations stay on the host)
   subroutine scatter()
-    call check(qv_get_points(ctx, xs, us), 'qv_iface:qv_get_points')
-    call check(qv_get_history(ctx, h1, h2, h3), 'qv_iface:qv_get_history')
-    call check(qv_get_closest(ctx, cls, cds), 'qv_iface:qv_get_closest')
+    integer(c_int) :: n
+    call check(qv_get_state(ctx, int(size(xs, 2), c_int), state(), n), 'qv_iface:qv_get_state')
     f(:)%x(1) = xs(1,:) ; f(:)%x(2) = xs(2,:) ; f(:)%x(3) = xs(3,:)
     f(:)%u(1) = us(1,:) ; f(:)%u(2) = us(2,:) ; f(:)%u(3) = us(3,:)
     f(:)%u1(1) = h1(1,:) ; f(:)%u1(2) = h1(2,:) ; f(:)%u1(3) = h1(3,:)

@@ -390,3 +390,47 @@ def test_steps_replay_equals_step_loop(velocity, boundary, recon_shots):
     assert np.array_equal(ca, cb) and np.array_equal(da, db)
     a.close()
     b.close()
+
+
+def test_state_exchange_equals_separate_calls():
+    """qv_set_state / qv_get_state move the same data as the separate set/get
+    calls, in one call each way."""
+    from qvort_b200 import lib as L
+    from qvort_b200 import workloads as W
+
+    w = W.random_rings(4, 0.006, 0.01, 5e-4, 0.1, seed=8, centre_box=0.05)
+    prm = dict(w.params, precision="mixed", tree_theta=0.4, velocity="Tree")
+    a = L.Context(L.default_params(**prm))
+    a.set_points(w.x, w.infront, w.behind)
+    for it in range(1, 4):
+        a.step(it)
+    n = a.n
+    cap = n + 5
+    got = dict(x=np.zeros((cap, 3)), u=np.zeros((cap, 3)), u1=np.zeros((cap, 3)),
+               u2=np.zeros((cap, 3)), u3=np.zeros((cap, 3)), infront=np.zeros(cap, np.int32),
+               behind=np.zeros(cap, np.int32), closest=np.zeros(cap, np.int32),
+               closestd=np.zeros(cap))
+    assert a.get_state(cap, **got) == n
+    x, u = a.get_points()
+    hist = a.get_history()
+    inf, beh = a.get_links()
+    cl, cd = a.get_closest()
+    ref = dict(x=x, u=u, u1=hist[0], u2=hist[1], u3=hist[2], infront=inf, behind=beh,
+               closest=cl, closestd=cd)
+    for k, v in ref.items():
+        assert np.array_equal(got[k][:n], v), k
+    with pytest.raises(L.QvError):
+        a.get_state(n - 1, **got)
+    # one upload == the three separate ones: the next step agrees bit for bit
+    b = L.Context(L.default_params(**prm))
+    b.set_state(n, **{k: got[k] for k in ("x", "infront", "behind", "u1", "u2", "u3", "closest")})
+    c = L.Context(L.default_params(**prm))
+    c.set_points(x, inf, beh)
+    c.set_history(*hist)
+    c.set_closest(cl)
+    b.step(4)
+    c.step(4)
+    assert np.array_equal(b.get_points()[0], c.get_points()[0])
+    assert np.array_equal(b.get_closest()[0], c.get_closest()[0])
+    for ctx in (a, b, c):
+        ctx.close()
