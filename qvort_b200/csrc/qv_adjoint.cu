@@ -272,7 +272,7 @@ __device__ __forceinline__ bool open_exact(const double *xi, const WNode64 &h, c
 }
 
 template <int BC>
-__global__ void __launch_bounds__(AW * 32) k_walk_vjp(WalkVjpArgs a) {
+__global__ void __launch_bounds__(AW * 32, 5) k_walk_vjp(WalkVjpArgs a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   __shared__ int2 stk[AW][ASTK];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
