@@ -364,6 +364,16 @@ def extras(ctx, w, stream, L, torch, itime):
         "leaf_evals": cnt["leaf_evals"], "far_evals": cnt["far_evals"],
         "walk_ms": walk_ms,
     }
+    # the same kernel against HBM: its DRAM traffic (one ncu capture, per launch)
+    # over its time, against the measured copy bandwidth -- far from the bound
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    if traffic and peaks_file.exists():
+        hbm = json.loads(peaks_file.read_text()).get("hbm_gbs")
+        if hbm:
+            gbs = traffic / (walk_ms * 1e-3) / 1e9
+            out["roofline"]["hbm"] = {"achieved": gbs, "peak": hbm, "unit": "GB/s",
+                                      "frac": gbs / hbm,
+                                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
     out["evals_per_step"] = cnt["leaf_evals"] + cnt["far_evals"] + 2 * n
 
     # ---- accuracy at the initial state: mixed BH vs FP64 BH vs FP64 direct
