@@ -194,6 +194,14 @@ int qv_energy_grad(qv_ctx *ctx, const double *u, double *energy, double *x_bar, 
  * grad_images = 0 differentiates the unshifted sum as the reference does. */
 int qv_field_velocity(qv_ctx *ctx, int m, const double *pts, int grad_images, double *u,
                       double *dudx);
+/* tree_walk_general (src/tree.f90:425-488) at m host points: the Tree arm of
+ * mesh_velocity (src/timestep.f90:374-452), the unshifted tree then the
+ * boundary's images, on the tree of the last build (built if there is none;
+ * needs tree_theta > 0).  Kept as the reference computes it: the leaf term is
+ * divided by 4 pi, the far-field term is not, and neither is multiplied by
+ * quant_circ; a cell whose centroid lies within epsilon of the point adds
+ * nothing.  u: 3m host values; *evals (may be NULL): evaluations. */
+int qv_field_velocity_tree(qv_ctx *ctx, int m, const double *pts, double *u, long long *evals);
 
 /* ---------------------------------------------------------------- host side
  * The parts of the reference's driver that feed this path, for a host that

@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         _lib.qo_pinsert.argtypes = [P, C.POINTER(C.c_int), C.c_int, C.POINTER(QoState)]
         _lib.qo_premove.argtypes = [P, C.c_int, C.POINTER(QoState)]
         _lib.qo_precon.argtypes = [P, C.c_int, C.POINTER(QoState)]
+        _lib.qo_field_velocity_tree.argtypes = [P, v, C.c_int, v, v]
+        _lib.qo_field_velocity_tree.restype = C.c_longlong
     return _lib
 
 
@@ -264,6 +266,14 @@ def premove(p: QoParams, n: int, st) -> int:
 def precon(p: QoParams, n: int, st) -> int:
     """precon_original on the state dict in place; returns the reconnections."""
     return lib().qo_precon(C.byref(p), n, C.byref(_qostate(st)))
+
+
+def field_velocity_tree(p: QoParams, tree, pts):
+    """tree_walk_general at the points (the Tree arm of mesh_velocity)."""
+    pts = _f(pts).reshape(-1, 3)
+    u = np.zeros_like(pts)
+    ev = lib().qo_field_velocity_tree(C.byref(p), tree.h, pts.shape[0], _p(pts), _p(u))
+    return u, ev
 
 
 def dt_max(p: QoParams) -> float:

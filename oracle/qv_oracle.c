@@ -991,3 +991,70 @@ int qo_precon(const qo_params *p, int pcount, qo_state *S) {
   }
   return count;
 }
+
+/* ------------------------------------------------ tree_walk_general */
+/* tree_walk_general, src/tree.f90:425-488 (hollow_mesh_core off): the velocity
+ * at an arbitrary point from the tree, as mesh_velocity uses it
+ * (src/timestep.f90:374-452).  The leaf term is divided by 4 pi and the
+ * far-field term is not, and neither is multiplied by quant_circ: the
+ * reference's own scaling, kept as it is. */
+static void walk_general(const qo_params *p, const qo_node *t, const double *x,
+                         const double *shift, double *u, long long *evals) {
+  if (!t || t->pcount == 0) return;
+  double dist = sqrt(sq(x[0] - (t->cent[0] + shift[0])) + sq(x[1] - (t->cent[1] + shift[1])) +
+                     sq(x[2] - (t->cent[2] + shift[2])));
+  if (dist < QO_EPS) return;
+  double theta = t->width / dist;
+  if (t->pcount == 1) {
+    double v1[3], v2[3], cr[3];
+    for (int c = 0; c < 3; c++) {
+      v1[c] = t->cent[c] + shift[c] - x[c];
+      v2[c] = t->cent[c] + t->circ[c] + shift[c] - x[c];
+    }
+    double a = sqrt(dot3(v1, v1)), b = sqrt(dot3(v2, v2));
+    double c = a * b * (a * b + dot3(v1, v2));
+    cross(v1, v2, cr);
+    for (int m = 0; m < 3; m++) {
+      double ub = (a + b) / c * cr[m];
+      u[m] = u[m] + ub / 4 / QO_PI;
+    }
+    (*evals)++;
+  } else if (theta < p->tree_theta) {
+    double v[3], ub[3];
+    for (int c = 0; c < 3; c++) v[c] = x[c] - (t->cent[c] + shift[c]);
+    double d3 = dist * dist * dist;
+    double d2 = dist * dist;
+    double d5 = d2 * d2 * dist;
+    cross(t->circ, v, ub);
+    for (int m = 0; m < 3; m++) ub[m] = ub[m] / d3;
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) {
+        double vc = v[0] * t->Cij[0][l];
+        vc = vc + v[1] * t->Cij[1][l];
+        vc = vc + v[2] * t->Cij[2][l];
+        for (int m = 0; m < 3; m++) ub[m] = ub[m] - levi(m, k, l) * t->Cij[k][l] / d3;
+        for (int m = 0; m < 3; m++) ub[m] = ub[m] + 3 * levi(m, k, l) * v[k] * vc / d5;
+      }
+    for (int m = 0; m < 3; m++) u[m] = u[m] + ub[m];
+    (*evals)++;
+  } else {
+    for (int k = 0; k < 8; k++) walk_general(p, t->child[k], x, shift, u, evals);
+  }
+}
+
+/* The Tree arm of mesh_velocity for m points: the unshifted tree, then the
+ * images of the boundary in the reference's loop order. */
+long long qo_field_velocity_tree(const qo_params *p, const qo_tree *T, int m, const double *pts,
+                                 double *u) {
+  double sh[27 * 3];
+  int ns = image_shifts(p, sh);
+  long long evals = 0;
+  for (int q = 0; q < m; q++) {
+    double *uq = u + 3 * q;
+    uq[0] = uq[1] = uq[2] = 0.;
+    const double zero[3] = {0., 0., 0.};
+    walk_general(p, T->root, pts + 3 * q, zero, uq, &evals);
+    for (int s = 0; s < ns; s++) walk_general(p, T->root, pts + 3 * q, sh + 3 * s, uq, &evals);
+  }
+  return evals;
+}

@@ -136,6 +136,7 @@ struct qv_ctx {
   size_t line_cap = 0;
   TreeBuf tree;
   int sm_count = 148;
+  int build_grid = 0;  // co-resident blocks of the cooperative tree build
   // instrumentation
   bool profile = false;
   cudaEvent_t ev_beg[PH_N] = {}, ev_end[PH_N] = {};

@@ -847,15 +847,15 @@ int qv_aux_streams(qv_ctx *c) {
   return QV_OK;
 }
 
+// Co-resident blocks of the cooperative build on this context's device.
 static int build_grid(qv_ctx *c) {
-  static int cached = 0;
-  if (cached) return cached;
+  if (c->build_grid) return c->build_grid;
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_build, BT, 0);
   if (per < 1) per = 1;
   if (per > 2) per = 2;
-  cached = per * c->sm_count;
-  return cached;
+  c->build_grid = per * c->sm_count;
+  return c->build_grid;
 }
 
 int qv_launch_tree_build(qv_ctx *c) {

@@ -441,3 +441,194 @@ int qv_launch_walk(qv_ctx *c) {
   QV_COUNT(c, 2);
   return QV_OK;
 }
+
+// ------------------------------------------------------- field points (tree)
+// tree_walk_general (src/tree.f90:425-488) at m arbitrary points, as the Tree
+// arm of mesh_velocity uses it (src/timestep.f90:374-452): per point the
+// unshifted tree, then the boundary's images in the reference's loop order,
+// all into one running FP64 sum, with the reference's operations: a node
+// within epsilon of the point adds nothing (its subtree included), the
+// opening test is width/dist < tree_theta, a leaf's segment runs from its
+// centroid to centroid + circ, the leaf term is divided by 4 pi, the far term
+// is not, and neither carries quant_circ.  One warp per 32 points with the
+// warp-coherent (node, lane mask) stack of the velocity walk.
+#define GW 4
+template <int BC>
+__global__ void __launch_bounds__(GW * 32) k_walk_general(int m, const double *__restrict__ pts,
+                                                         const WNode64 *__restrict__ w64,
+                                                         const WPay64 *__restrict__ p64,
+                                                         const double *__restrict__ cent,
+                                                         const double *__restrict__ circ,
+                                                         double L, double theta, int nroots,
+                                                         double *u, unsigned long long *evals,
+                                                         int *status) {
+  constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
+  __shared__ int2 stk[GW][STK];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int2 *st = stk[wid];
+  const int ngroups = (m + 31) / 32;
+  for (int g = blockIdx.x * GW + wid; g < ngroups; g += gridDim.x * GW) {
+    const int q = g * 32 + lane;
+    const bool live = q < m;
+    double x[3] = {0., 0., 0.};
+    if (live) { x[0] = pts[3 * q]; x[1] = pts[3 * q + 1]; x[2] = pts[3 * q + 2]; }
+    double acc[3] = {0., 0., 0.};
+    unsigned long long ev = 0;
+    bool bad = false;
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    for (int img = -1; img < NIMG; img++) {
+      int ma = 0, mb = 0, mc = 0;
+      if (img >= 0) qv_img_shift(BC, img, &ma, &mb, &mc);
+      const double s[3] = {shift_of(ma, L), shift_of(mb, L), shift_of(mc, L)};
+      int top = 0;
+      if (lane == 0) st[0] = make_int2(0, (int)live_mask);
+      top = live_mask ? 1 : 0;
+      __syncwarp();
+      while (top > 0) {
+        top--;
+        const int2 e = st[top];
+        __syncwarp();
+        const int node = e.x;
+        const bool in = (((unsigned)e.y) >> lane) & 1u;
+        const WNode64 h = w64[node];
+        bool open = false;
+        if (in && h.count > 0) {
+          const double dist = exact_dist(x, h, s);
+          if (!(dist < QV_DEPS)) {
+            const double th = __ddiv_rn(h.width, dist);
+            const double zero3[3] = {0., 0., 0.};
+            const double *C0 = cent + 3 * node, *R = node < nroots ? zero3 : circ + 3 * node;
+            if (h.count == 1) {
+              double v1[3], v2[3];
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                v1[c] = __dsub_rn(__dadd_rn(C0[c], s[c]), x[c]);
+                v2[c] = __dsub_rn(__dadd_rn(__dadd_rn(C0[c], R[c]), s[c]), x[c]);
+              }
+              const double a = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(v1[0], v1[0]), __dmul_rn(v1[1], v1[1])), __dmul_rn(v1[2], v1[2])));
+              const double b = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(v2[0], v2[0]), __dmul_rn(v2[1], v2[1])), __dmul_rn(v2[2], v2[2])));
+              const double dv = __dadd_rn(__dadd_rn(__dmul_rn(v1[0], v2[0]), __dmul_rn(v1[1], v2[1])), __dmul_rn(v1[2], v2[2]));
+              const double ab = __dmul_rn(a, b);
+              const double cc = __dmul_rn(ab, __dadd_rn(ab, dv));
+              const double f = __ddiv_rn(__dadd_rn(a, b), cc);
+              const double cr[3] = {__dsub_rn(__dmul_rn(v1[1], v2[2]), __dmul_rn(v1[2], v2[1])),
+                                    __dsub_rn(__dmul_rn(v1[2], v2[0]), __dmul_rn(v1[0], v2[2])),
+                                    __dsub_rn(__dmul_rn(v1[0], v2[1]), __dmul_rn(v1[1], v2[0]))};
+#pragma unroll
+              for (int c = 0; c < 3; c++)
+                acc[c] = __dadd_rn(acc[c], __ddiv_rn(__ddiv_rn(__dmul_rn(f, cr[c]), 4.), QV_PI));
+              ev++;
+            } else if (th < theta) {
+              const double v[3] = {__dsub_rn(x[0], __dadd_rn(C0[0], s[0])),
+                                   __dsub_rn(x[1], __dadd_rn(C0[1], s[1])),
+                                   __dsub_rn(x[2], __dadd_rn(C0[2], s[2]))};
+              const double d2 = __dmul_rn(dist, dist);
+              const double d3 = __dmul_rn(d2, dist);
+              const double d5 = __dmul_rn(__dmul_rn(d2, d2), dist);
+              const WPay64 &P = p64[node];
+              double ci[3], Cm[9];
+#pragma unroll
+              for (int c = 0; c < 3; c++) ci[c] = node < nroots ? 0. : P.a[c];
+#pragma unroll
+              for (int c = 0; c < 9; c++) Cm[c] = node < nroots ? 0. : P.C[c];
+              double ub[3] = {__ddiv_rn(__dsub_rn(__dmul_rn(ci[1], v[2]), __dmul_rn(ci[2], v[1])), d3),
+                              __ddiv_rn(__dsub_rn(__dmul_rn(ci[2], v[0]), __dmul_rn(ci[0], v[2])), d3),
+                              __ddiv_rn(__dsub_rn(__dmul_rn(ci[0], v[1]), __dmul_rn(ci[1], v[0])), d3)};
+              for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++) {
+                  double vc = __dmul_rn(v[0], Cm[l]);
+                  vc = __dadd_rn(vc, __dmul_rn(v[1], Cm[3 + l]));
+                  vc = __dadd_rn(vc, __dmul_rn(v[2], Cm[6 + l]));
+#pragma unroll
+                  for (int mm = 0; mm < 3; mm++) {
+                    const double e = (mm == k || k == l || l == mm) ? 0.
+                                     : ((mm + 1) % 3 == k ? 1. : -1.);  // eps(m,k,l)
+                    ub[mm] = __dsub_rn(ub[mm], __ddiv_rn(__dmul_rn(e, Cm[3 * k + l]), d3));
+                  }
+#pragma unroll
+                  for (int mm = 0; mm < 3; mm++) {
+                    const double e = (mm == k || k == l || l == mm) ? 0.
+                                     : ((mm + 1) % 3 == k ? 1. : -1.);
+                    ub[mm] = __dadd_rn(ub[mm], __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(3., e), v[k]), vc), d5));
+                  }
+                }
+#pragma unroll
+              for (int c = 0; c < 3; c++) acc[c] = __dadd_rn(acc[c], ub[c]);
+              ev++;
+            } else {
+              open = true;
+            }
+          }
+        }
+        const unsigned om = __ballot_sync(0xffffffffu, open);
+        if (om) {
+          int nc = h.nchild;
+          if (top + nc > STK) {  // unreachable for trees within QV_MAX_DEPTH
+            bad = true;
+            nc = 0;
+          }
+          if (lane < nc) st[top + lane] = make_int2(h.child_first + nc - 1 - lane, (int)om);
+          top += nc;
+        }
+        __syncwarp();
+      }
+    }
+    if (live) { u[3 * q] = acc[0]; u[3 * q + 1] = acc[1]; u[3 * q + 2] = acc[2]; }
+    for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
+    if (lane == 0 && ev) atomicAdd(evals, ev);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, 2);
+  }
+}
+
+extern "C" int qv_field_velocity_tree(qv_ctx *c, int m, const double *pts, double *u,
+                                      long long *evals) {
+  if (!c || m < 0 || (m > 0 && (!pts || !u))) return QV_ERR_ARG;
+  if (!(c->p.tree_theta > 0) || !(c->p.box_size > 0))
+    return qv_fail(c, QV_ERR_ARG, "tree_walk_general needs tree_theta > 0 and a box");
+  if (m == 0 || c->n == 0) {
+    for (int k = 0; k < 3 * m; k++) u[k] = 0.;
+    if (evals) *evals = 0;
+    return QV_OK;
+  }
+  int rc;
+  if (!c->tree.valid)
+    if ((rc = qv_launch_tree_build(c))) return rc;
+  TreeBuf &t = c->tree;
+  double *dp = nullptr;
+  QV_CUDA(c, cudaMalloc((void **)&dp, sizeof(double) * 6 * (size_t)m));
+  struct Free {
+    double *p;
+    ~Free() { cudaFree(p); }
+  } guard{dp};  // freed on every return path
+  double *du = dp + 3 * (size_t)m;
+  QV_CUDA(c, cudaMemcpyAsync(dp, pts, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, c->stream));
+  QV_CUDA(c, cudaMemsetAsync(c->evals, 0, sizeof(unsigned long long), c->stream));
+  QV_CUDA(c, cudaMemsetAsync(c->dstatus, 0, sizeof(int), c->stream));
+  const int nb = std::max(1, std::min((m + 32 * GW - 1) / (32 * GW), 64 * c->sm_count));
+  switch (c->p.boundary) {
+#define QV_GW_CASE(BCV)                                                                          \
+  case BCV:                                                                                      \
+    k_walk_general<BCV><<<nb, GW * 32, 0, c->stream>>>(m, dp, t.w64, t.p64, t.cent, t.circ,     \
+                                                       c->p.box_size, c->p.tree_theta, 1, du,   \
+                                                       c->evals, c->dstatus);                   \
+    break;
+    QV_GW_CASE(QV_BC_OPEN)
+    QV_GW_CASE(QV_BC_PERIODIC)
+    QV_GW_CASE(QV_BC_OPENX)
+    QV_GW_CASE(QV_BC_OPENXY)
+#undef QV_GW_CASE
+    default:
+      return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
+  }
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  unsigned long long ev = 0;
+  int st = 0;
+  QV_CUDA(c, cudaMemcpyAsync(u, du, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaMemcpyAsync(&ev, c->evals, sizeof(ev), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaMemcpyAsync(&st, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (evals) *evals = (long long)ev;
+  if (st & 2) return qv_fail(c, QV_ERR_TREE_DEPTH, "tree_walk_general stack overflow");
+  return QV_OK;
+}

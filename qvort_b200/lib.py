@@ -132,6 +132,7 @@ _SIGS = {
     "qv_velocity_vjp": [_P, _P, _P],
     "qv_energy_grad": [_P, _P, _D, _P, _P],
     "qv_field_velocity": [_P, C.c_int, _P, C.c_int, _P, _P],
+    "qv_field_velocity_tree": [_P, C.c_int, _P, _P, C.POINTER(C.c_longlong)],
     "qv_read_run_file": [C.c_char_p, C.POINTER(QvRun)],
     "qv_read_var_file": [C.c_char_p, C.c_int, _I, _D, _P, _P, _P],
     "qv_write_var_file": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
@@ -414,6 +415,15 @@ class Context:
         e = C.c_double()
         self._check(_lib.qv_energy_grad(self._h, u_ptr, C.byref(e), xbar_ptr, ubar_ptr))
         return e.value
+
+    def field_velocity_tree(self, pts):
+        """tree_walk_general at the given points (the mesh_velocity Tree arm)."""
+        pts = _f64(pts).reshape(-1, 3)
+        u = np.empty_like(pts)
+        ev = C.c_longlong()
+        self._check(_lib.qv_field_velocity_tree(self._h, pts.shape[0], _ptr(pts), _ptr(u),
+                                                C.byref(ev)))
+        return u, ev.value
 
     def field_velocity(self, pts, grad_images: bool = False):
         pts = _f64(pts).reshape(-1, 3)

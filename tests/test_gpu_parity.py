@@ -434,3 +434,29 @@ def test_state_exchange_equals_separate_calls():
     assert np.array_equal(b.get_closest()[0], c.get_closest()[0])
     for ctx in (a, b, c):
         ctx.close()
+
+
+@pytest.mark.parametrize("bc,theta", [("periodic", 0.4), ("open", 0.5), ("openx", 0.3)])
+def test_field_velocity_tree_matches_oracle(L, bc, theta):
+    """tree_walk_general at points of a mesh, at random points and at filament
+    points themselves, against the oracle: the same evaluations and the same
+    FP64 sums.  At a filament point the reference's own arithmetic can give
+    NaN (its leaf is skipped by the epsilon test, but the segment ending there
+    may have |R2| = 0); both sides must agree on where."""
+    w = small_tangle()
+    c = ctx_for(L, w, boundary=bc, velocity="Tree", tree_theta=theta, precision="fp64")
+    rng = np.random.default_rng(3)
+    g = np.linspace(-0.045, 0.045, 8)
+    mesh = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pts = np.concatenate([mesh, rng.uniform(-0.05, 0.05, (200, 3)), w.x[::37]])
+    u, ev = c.field_velocity_tree(pts)
+    p = opar(w, boundary=bc, velocity="Tree", tree_theta=theta)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    tree = O.Tree(p, w.x, og[0], w.infront)
+    uo, evo = O.field_velocity_tree(p, tree, pts)
+    c.close()
+    assert ev == evo
+    nan = np.isnan(uo)
+    assert np.array_equal(np.isnan(u), nan)
+    ok = ~nan.any(axis=1)
+    assert rel_max(u[ok], uo[ok]) < 1e-12, rel_max(u[ok], uo[ok])

@@ -303,3 +303,24 @@ def test_precon_merges_two_touching_rings():
     # one loop through every surviving point (the two-point loop the second
     # reconnection cuts off goes to loop_killer)
     assert i == start and seen == len(alive) >= n - 8
+
+
+def test_tree_walk_general_at_tiny_theta_is_the_segment_sum():
+    """With theta -> 0 every leaf is visited: tree_walk_general is the sum over
+    all segments (x_j -> ghosti_j) of the straight-segment term divided by
+    4 pi (src/tree.f90:444-459), here summed independently with numpy."""
+    w = W.random_rings(3, 0.006, 0.01, 5e-4, 0.1, seed=2, centre_box=0.05)
+    p = O.params(**dict(w.params, boundary="open", velocity="Tree", tree_theta=1e-9))
+    g = O.ghosts(p, w.x, w.infront, w.behind)
+    tree = O.Tree(p, w.x, g[0], w.infront)
+    pts = np.random.default_rng(5).uniform(-0.03, 0.03, (20, 3))
+    u, ev = O.field_velocity_tree(p, tree, pts)
+    assert ev == 20 * w.n
+    for q, x in enumerate(pts):
+        r1 = w.x - x
+        r2 = g[0] - x
+        a = np.linalg.norm(r1, axis=1)
+        b = np.linalg.norm(r2, axis=1)
+        c = a * b * (a * b + (r1 * r2).sum(1))
+        ref = (((a + b) / c)[:, None] * np.cross(r1, r2)).sum(0) / (4 * np.pi)
+        assert np.abs(u[q] - ref).max() <= 1e-9 * np.abs(ref).max()
