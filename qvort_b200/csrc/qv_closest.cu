@@ -26,20 +26,100 @@ __device__ __forceinline__ double dist_exact(const double *a, double b0, double 
 // of the reference evaluated, so the outcome is always the FP64 outcome.
 // Children's headers are fetched when they are pushed (stack entries carry
 // them), so popping a node costs a shared-memory read.
+//
+// Pruning.  The traversal visits every cell that the reference's walk visits
+// until it can prove that a subtree holds nothing that changes the result.
+// Per target the walk is a fold over the visited cells in depth-first order:
+// a one-point cell with a valid partner j at distance d < closestd sets
+// (closest, closestd) = (j, d); a cell that passes the theta test at distance
+// d < closestd sets closest = 0.  So the result is fixed by the valid leaf of
+// least distance (its first occurrence in that order) and by whether a passing
+// cell after it lies closer than that distance.  Let T bound the least valid
+// leaf distance from above: any subtree whose cell is farther than T from the
+// target holds neither that leaf nor a passing cell closer than it, and
+// skipping it leaves the result unchanged.  T is the running closestd, and,
+// from the start, the distance to the leaf of the point two links ahead or
+// behind when that leaf is itself a valid visited cell (every ancestor opens
+// for the target, checked on the parent chain with the same tests).  The box
+// distance is a lower bound taken in FP32 with a relative 1e-5 and an absolute
+// 2e-6 (|x| + L) margin, above every rounding of the operands.
 struct __align__(16) CStkEnt {
-  WNode32 h;
+  SNode32 h;
   int node;
   unsigned mask;
   int pad[2];
 };
 
+// The theta test of closest_tree (src/tree.f90:248-249) for a cell with more
+// than one point: true when width/dist < 0.5 (the cell is taken whole).
+// d2 is the FP32 squared distance of the target from the centroid; d64 is
+// set to the FP64 distance when it had to be computed (else left alone).
+__device__ __forceinline__ bool search_far(const SNode32 &h, const WNode64 *__restrict__ w64,
+                                           int node, float d2, bool tiny, const double *xi,
+                                           double &d64) {
+  if (!tiny && (d2 > h.rhi || d2 < h.rlo)) return d2 > h.rhi;
+  const WNode64 hh = w64[node];
+  d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
+  return __ddiv_rn(hh.width, d64) < .5;
+}
+
+__device__ __forceinline__ float cent_d2(const SNode32 &h, const float *xh, const float *xl) {
+  float v0 = (xh[0] - h.ch[0]) + (xl[0] - h.cl[0]);
+  float v1 = (xh[1] - h.ch[1]) + (xl[1] - h.cl[1]);
+  float v2 = (xh[2] - h.ch[2]) + (xl[2] - h.cl[2]);
+  return fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+}
+
+// Lower bound on the distance from xh to anything in the cell's box.
+__device__ __forceinline__ float box_dist(const SNode32 &h, const float *xh) {
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float a = fmaxf(0.f, fmaxf(h.lo[c] - xh[c], xh[c] - (h.lo[c] + h.w)));
+    s = fmaf(a, a, s);
+  }
+  return sqrtf(s);
+}
+
+// Distance to the one-point leaf holding slot s when that leaf is a valid cell
+// of target i's walk (partner not i or its neighbours; every ancestor opens);
+// else 100, the reference's starting closestd.
+__device__ double leaf_bound(int s, int n, int nn, int n_leaf, const int *__restrict__ leaf_of,
+                             const int *__restrict__ parent, const int *__restrict__ beh,
+                             const WNode64 *__restrict__ w64, const SNode32 *__restrict__ c32,
+                             int ii, int fi, int bi, const double *xi, const float *xh,
+                             const float *xl) {
+  if (s < 0 || s >= n_leaf) return 100.;
+  const int k = leaf_of[s];
+  if (k < 0 || k >= nn) return 100.;
+  const WNode64 hh = w64[k];
+  if (hh.count != 1 || hh.first != s || hh.finf < 1 || hh.finf > n) return 100.;
+  const int j = beh[hh.finf - 1];
+  if (j == ii || j == fi || j == bi) return 100.;
+  int a = parent[k];
+  for (int it = 0; a >= 0; it++) {
+    if (it > QV_MAX_DEPTH + 2 || a >= nn) return 100.;
+    const SNode32 h = c32[a];
+    if (h.count <= 1) return 100.;
+    const float d2 = cent_d2(h, xh, xl);
+    double d64 = -1.;
+    if (search_far(h, w64, a, d2, d2 < 1e-20f, xi, d64)) return 100.;
+    a = parent[a];
+  }
+  return dist_exact(xi, hh.cx, hh.cy, hh.cz);
+}
+
 __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *__restrict__ x,
                                                          const int *__restrict__ inf,
                                                          const int *__restrict__ beh,
                                                          const WNode64 *__restrict__ w64,
-                                                         const WNode32 *__restrict__ w32,
-                                                         int stk_cap, int *closest,
-                                                         double *closestd, int *status) {
+                                                         const SNode32 *__restrict__ c32,
+                                                         const int *__restrict__ parent,
+                                                         const int *__restrict__ leaf_of,
+                                                         int n_leaf, int nn, float box,
+                                                         int stk_cap,
+                                                         int *closest, double *closestd,
+                                                         int *status) {
   extern __shared__ CStkEnt cstk[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   CStkEnt *st = cstk + wid * stk_cap;
@@ -52,20 +132,33 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
     double cd = 100.;
     float cd2 = 1e4f;
     float xh[3] = {0.f, 0.f, 0.f}, xl[3] = {0.f, 0.f, 0.f};
+    float thr = 0.f, slack = 0.f;
+    double ub = 100.;
     if (live) {
       xi[0] = x[3 * i]; xi[1] = x[3 * i + 1]; xi[2] = x[3 * i + 2];
       fi = inf[i]; bi = beh[i]; cl = closest[i];
+      float amax = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         xh[c] = __double2float_rn(xi[c]);
         xl[c] = __double2float_rn(xi[c] - (double)xh[c]);
+        amax = fmaxf(amax, fabsf(xh[c]));
       }
+      slack = 2e-6f * (amax + box);
+      // the points two links ahead and behind
+      int s1 = (fi >= 1 && fi <= n) ? inf[fi - 1] - 1 : -1;
+      int s2 = (bi >= 1 && bi <= n) ? beh[bi - 1] - 1 : -1;
+      ub = leaf_bound(s1, n, nn, n_leaf, leaf_of, parent, beh, w64, c32, ii, fi, bi, xi, xh, xl);
+      if (s2 != s1)
+        ub = fmin(ub, leaf_bound(s2, n, nn, n_leaf, leaf_of, parent, beh, w64, c32, ii, fi, bi, xi,
+                                 xh, xl));
+      thr = __double2float_ru(ub) * 1.00001f + slack;
     }
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);
     bool bad = false;
     int top = 0;
     if (lane == 0) {
-      st[0].h = w32[0];
+      st[0].h = c32[0];
       st[0].node = 0;
       st[0].mask = live_mask;
     }
@@ -73,31 +166,17 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
     __syncwarp();
     while (top > 0) {
       top--;
-      const WNode32 h = st[top].h;
+      const SNode32 h = st[top].h;
       const int node = st[top].node;
-      const bool in = (st[top].mask >> lane) & 1u;
+      bool in = (st[top].mask >> lane) & 1u;
       __syncwarp();
       bool open = false;
+      if (in && h.count > 0 && box_dist(h, xh) > thr) in = false;
       if (in && h.count > 0) {
-        float v0 = (xh[0] - h.ch[0]) + (xl[0] - h.cl[0]);
-        float v1 = (xh[1] - h.ch[1]) + (xl[1] - h.cl[1]);
-        float v2 = (xh[2] - h.ch[2]) + (xl[2] - h.cl[2]);
-        float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+        float d2 = cent_d2(h, xh, xl);
         bool tiny = d2 < 1e-20f;
         double d64 = -1.;  // exact distance, computed on demand
-        bool pass;
-        if (h.count == 1) {
-          pass = true;
-        } else {
-          // theta = width/dist < 0.5  (src/tree.f90:248-249)  <=>  dist^2 > (2 width)^2
-          if (!tiny && (d2 > h.rhi || d2 < h.rlo)) {
-            pass = d2 > h.rhi;
-          } else {
-            const WNode64 hh = w64[node];
-            d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
-            pass = __ddiv_rn(hh.width, d64) < .5;
-          }
-        }
+        bool pass = h.count == 1 || search_far(h, w64, node, d2, tiny, xi, d64);
         if (pass) {
           // dist < closestd
           bool closer;
@@ -121,8 +200,9 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
                 if (d64 < 0.) d64 = dist_exact(xi, hh.cx, hh.cy, hh.cz);
                 cl = j;
                 cd = d64;
-                float c32 = __double2float_rn(cd);
-                cd2 = c32 * c32;
+                float c32f = __double2float_rn(cd);
+                cd2 = c32f * c32f;
+                thr = __double2float_ru(fmin(cd, ub)) * 1.00001f + slack;
               }
             }
           }
@@ -140,7 +220,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
         if (lane < nc) {
           int ch = h.child_first + nc - 1 - lane;
           CStkEnt &E = st[top + lane];
-          E.h = w32[ch];
+          E.h = c32[ch];
           E.node = ch;
           E.mask = om;
         }
@@ -215,9 +295,11 @@ int qv_launch_closest(qv_ctx *c) {
         opted = smem;
       }
     }
+    const TreeBuf &t = c->tree;
     k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, smem, c->stream>>>(
-        c->n, c->x, c->infront, c->behind, c->tree.w64, c->tree.c32, cap, c->closest,
-        c->closestd, c->dstatus);
+        c->n, c->x, c->infront, c->behind, t.w64, t.c32, t.parent, t.leaf_of, t.n_leaf,
+        std::min(t.n_nodes, t.cap_nodes), (float)c->p.box_size, cap, c->closest, c->closestd,
+        c->dstatus);
   } else {
     k_pclose<<<(c->n + PT - 1) / PT, PT, 0, c->stream>>>(c->n, c->x, c->infront, c->behind,
                                                          c->closest, c->closestd);

@@ -27,7 +27,7 @@ struct __align__(16) WNode64 {
   int nchild;       // number of non-empty children
   int jb;           // leaf: f(parray(1)%infront)%behind at build time (1-based)
   int finf;         // parray(1)%infront at build time (1-based)
-  int pad;
+  int first;        // slot of parray(1) (0-based), -1 if none
 };
 
 // FP64 payload (128 B): leaf -> segment x, ghosti; internal -> circ, the
@@ -43,14 +43,25 @@ struct __align__(16) WPay64 {
 // that target-source differences keep FP64-level information, and the node's
 // opening radius squared widened by a relative 4e-6 either way: a squared
 // distance above rhi passes the test, one below rlo fails it, one in between
-// is decided by the reference's FP64 expression.  Two arrays of headers: w32
-// for the velocity walk (radius geo + width/theta; rhi = rlo = -1 when only
-// the FP64 test is valid) and c32 for the candidate search (radius 2 width:
-// theta = width/dist < 0.5).  See k_pack_nodes.
+// is decided by the reference's FP64 expression.  w32 holds these headers for
+// the velocity walk (radius geo + width/theta; rhi = rlo = -1 when only the
+// FP64 test is valid).  See k_pack_nodes.
 struct __align__(16) WNode32 {
   float ch[3], cl[3];
   float rhi, rlo;
   int count, child_first, nchild, jb;
+};
+
+// Candidate-search header (64 B): the same centroid split and widened radius
+// for theta = width/dist < 0.5 (radius 2 width), plus the cell's box as an
+// FP32 corner rounded down and a width rounded up, so that a lower bound on
+// the distance from a target to anything inside the cell costs a few FP32
+// operations.
+struct __align__(16) SNode32 {
+  float ch[3], cl[3];
+  float rhi, rlo;
+  float lo[3], w;
+  int count, child_first, nchild, pad;
 };
 
 // FP32 payload (64 B): internal -> circ, w, C; leaf -> ghosti as (hi, lo)
@@ -76,7 +87,8 @@ struct TreeBuf {
   // walk packs
   WNode64 *w64 = nullptr;
   WPay64 *p64 = nullptr;
-  WNode32 *w32 = nullptr, *c32 = nullptr;
+  WNode32 *w32 = nullptr;
+  SNode32 *c32 = nullptr;
   WPay32 *p32 = nullptr;
   // build scratch
   int *ord = nullptr;       // cap_levels * cap_pts: per-level orders
@@ -87,6 +99,8 @@ struct TreeBuf {
   int *chunk9 = nullptr;                   // per chunk of positions
   int *ctl = nullptr;                      // device control block
   int *perm = nullptr;                     // final (DFS) order of active points
+  int *leaf_of = nullptr;                  // slot -> its one-point leaf (unverified)
+  int n_leaf = 0;                          // slots covered by leaf_of
   int *h_ctl = nullptr;                    // pinned copy of the control block
   cudaEvent_t ev_ctl = nullptr;
   std::vector<int> lvl_start;

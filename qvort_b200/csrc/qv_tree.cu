@@ -591,8 +591,8 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const int *__restrict__ nchild, const int *__restrict__ first,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
-                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, WNode32 *c32,
-                          WPay32 *p32);
+                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
+                          WPay32 *p32, int *leaf_of, int n_leaf);
 
 __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nroots,
                              const double *__restrict__ pos,
@@ -602,13 +602,13 @@ __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nro
                              const int *__restrict__ nchild, const int *__restrict__ first,
                              const double *__restrict__ x, const double *__restrict__ gi,
                              const int *__restrict__ inf, const int *__restrict__ beh,
-                             double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, WNode32 *c32,
-                             WPay32 *p32) {
+                             double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
+                             WPay32 *p32, int *leaf_of, int n_leaf) {
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
     pack_node(k, nroots, pos, width, cent, circ, C, count, child_first, nchild, first, x, gi, inf,
-              beh, theta, extra, w64, p64, w32, c32, p32);
+              beh, theta, extra, w64, p64, w32, c32, p32, leaf_of, n_leaf);
 }
 
 __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
@@ -618,8 +618,8 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const int *__restrict__ nchild, const int *__restrict__ first,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
-                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, WNode32 *c32,
-                          WPay32 *p32) {
+                          double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
+                          WPay32 *p32, int *leaf_of, int n_leaf) {
   WNode64 h;
   h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
   h.width = width[k];
@@ -638,8 +638,9 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
   int f = first[k];
   h.finf = (f >= 0) ? inf[f] : 0;
   h.jb = (f >= 0 && h.finf > 0) ? beh[h.finf - 1] : 0;
-  h.pad = 0;
+  h.first = f;
   w64[k] = h;
+  if (leaf_of && cnt == 1 && f >= 0 && f < n_leaf) leaf_of[f] = k;
   WPay64 q;
   WPay32 r;
   WNode32 h32;
@@ -668,11 +669,22 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
   }
   w32[k] = h32;
   {
+    SNode32 s32;
+    for (int c = 0; c < 3; c++) {
+      s32.ch[c] = h32.ch[c];
+      s32.cl[c] = h32.cl[c];
+      s32.lo[c] = __double2float_rd(pos[3 * k + c]);
+    }
     double w4 = 4. * h.width * h.width;  // (2 width)^2
-    h32.rhi = __double2float_rn(w4 * (1. + 4e-6));
-    h32.rlo = __double2float_rn(w4 * (1. - 4e-6));
+    s32.rhi = __double2float_rn(w4 * (1. + 4e-6));
+    s32.rlo = __double2float_rn(w4 * (1. - 4e-6));
+    s32.w = __double2float_ru(h.width);
+    s32.count = cnt;
+    s32.child_first = h.child_first;
+    s32.nchild = h.nchild;
+    s32.pad = 0;
+    c32[k] = s32;
   }
-  c32[k] = h32;
   if (cnt == 1 && f >= 0) {
     for (int c = 0; c < 3; c++) {
       q.a[c] = x[3 * f + c];
@@ -799,6 +811,7 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
       if ((rc = qv_grow(c, (void **)&t.nodeB, sizeof(int) * np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.dig, np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.rnk, sizeof(int) * np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.leaf_of, sizeof(int) * np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.cnt9, sizeof(int) * 9 * (size_t)(2 * np + 2)))) return rc;
       if ((rc = qv_grow(c, (void **)&t.rs9, sizeof(int) * 9 * (size_t)(np + 1)))) return rc;
       if ((rc = qv_grow(c, (void **)&t.chunk9, sizeof(int) * 9 * (size_t)(np / CH + 2)))) return rc;
@@ -826,7 +839,7 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
     if ((rc = qv_grow(c, (void **)&t.w64, sizeof(WNode64) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.p64, sizeof(WPay64) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.w32, sizeof(WNode32) * m))) return rc;
-    if ((rc = qv_grow(c, (void **)&t.c32, sizeof(WNode32) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.c32, sizeof(SNode32) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.p32, sizeof(WPay32) * m))) return rc;
     t.cap_nodes = cap_nodes;
   }
@@ -934,7 +947,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
         t.ctl, t.cap_nodes, 1, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
         t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
-        c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32);
+        c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, t.leaf_of, n);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 2);
     qv_phase_end_async(c, PH_BUILD_MOMENTS);
@@ -960,6 +973,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     c->n_act = t.n_act;
     t.lvl_start.assign(hc + CTL_LVL, hc + CTL_LVL + t.depth + 2);
     t.perm = t.ord + (size_t)t.depth * t.cap_pts;
+    t.n_leaf = n;
     t.valid = true;
     return QV_OK;
   }
@@ -1025,7 +1039,7 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
       t.ctl, t.cap_nodes, f.nroots, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
       t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
-      c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32);
+      c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, nullptr, 0);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 7);
   return QV_OK;

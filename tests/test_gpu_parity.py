@@ -229,6 +229,66 @@ def test_walk_mixed_vs_fp64(L):
     assert rel_rms(r[1][2], r[0][2]) < 1e-5
 
 
+@pytest.mark.parametrize("velocity,bc,opts", [
+    ("Tree", "openx", {}),
+    ("Tree", "openxy", {}),
+    ("Tree", "periodic", {"deriv_order": 4}),
+    ("Tree", "periodic", {"tree_extra_correction": 0}),
+    ("BS", "openx", {"deriv_order": 4}),
+    ("LIA", "periodic", {}),
+    ("LIA", "periodic", {"fixed_lia_beta": 1}),
+    ("LIA", "open", {"deriv_order": 4}),
+])
+def test_velocity_options_match_oracle(L, velocity, bc, opts, nthreads):
+    """Every velocity arm, boundary and option of calc_velocity
+    (src/timestep.f90) in FP64 against the oracle: the same tree traversal
+    (identical evaluation counts) and velocities within 1e-10 relative."""
+    w = small_tangle(5, 24)
+    theta = 0.4 if velocity == "Tree" else 0.0
+    c = ctx_for(L, w, boundary=bc, velocity=velocity, tree_theta=theta, precision="fp64", **opts)
+    c.ghosts()
+    if velocity == "Tree":
+        c.build_tree()
+    u, uli, ubs, ev = c.velocity()
+    p = opar(w, boundary=bc, velocity=velocity, tree_theta=theta, **opts)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    tr = O.Tree(p, w.x, og[0], w.infront) if velocity == "Tree" else None
+    ou, ouli, oubs, oev, st = O.velocity(p, w.x, w.infront, w.behind, og, tr, nthreads=nthreads)
+    assert st == 0
+    if velocity == "Tree":         # the oracle counts tree evaluations only
+        assert ev == oev
+    # the direct sum adds ~3e4 terms per target in blocked order (the oracle:
+    # one running sum), so its FP64 bar is 1e-9 of the largest velocity
+    assert rel_max(u, ou) < (1e-9 if velocity == "BS" else 1e-10)
+    if velocity != "LIA":          # the LIA arm reports neither part separately
+        assert rel_max(uli, ouli) < 1e-12
+        assert rel_max(ubs, oubs) < 1e-9
+
+
+@pytest.mark.parametrize("velocity,bc,opts", [
+    ("Tree", "openx", {}),
+    ("Tree", "openxy", {"deriv_order": 4}),
+    ("Tree", "periodic", {"tree_extra_correction": 0}),
+    ("BS", "openxy", {}),
+])
+def test_velocity_options_mixed_vs_fp64(L, velocity, bc, opts):
+    """The mixed-precision kernels under the same options: same traversal as
+    FP64, velocities within 1e-6 RMS relative."""
+    w = small_tangle(6, 24)
+    theta = 0.4 if velocity == "Tree" else 0.0
+    r = []
+    for prec in ("fp64", "mixed"):
+        c = ctx_for(L, w, boundary=bc, velocity=velocity, tree_theta=theta, precision=prec,
+                    **opts)
+        c.ghosts()
+        if velocity == "Tree":
+            c.build_tree()
+        r.append(c.velocity())
+        c.close()
+    assert r[0][3] == r[1][3]
+    assert rel_rms(r[1][0], r[0][0]) < 1e-6
+
+
 # ------------------------------------------------------------------ steps
 def test_ab_step_bit_exact_given_velocity(L):
     w = small_tangle(4, 10)
@@ -271,6 +331,58 @@ def test_closest_tree_bit_exact(L, nthreads):
     np.testing.assert_array_equal(cl, ocl)
     np.testing.assert_array_equal(cd, ocd)
 
+
+
+def test_closest_tree_after_pinsert_bit_exact(L):
+    """The candidate search after pinsert, as in a step: the tree and its
+    parray(1)%infront links are from before the move, the positions and links
+    are current, and new points (not in the tree) search too."""
+    w = W.random_rings(12, 0.004, 0.008, 3e-4, 0.1, seed=3, theta=0.4)
+    c = ctx_for(L, w, precision="fp64", delta=2.2e-4, dt=5e-6)
+    c.ghosts()
+    c.build_tree()
+    x0, _ = c.get_points()
+    inf0, beh0 = c.get_links()
+    g0 = c.get_ghosts()
+    c.velocity(False)
+    c.step_ab()
+    assert c.pinsert() > 0
+    n = c.n
+    rng = np.random.default_rng(2)
+    seedcl = rng.integers(0, n, n).astype(np.int32)
+    c.set_closest(seedcl)
+    cl, cd = c.closest()
+    xn, _ = c.get_points()
+    infn, behn = c.get_links()
+    p = opar(w, delta=2.2e-4)
+    tr = O.Tree(p, x0, g0[0], inf0)
+    ocl, ocd = O.pclose_tree(tr, xn, infn, behn, seedcl)
+    np.testing.assert_array_equal(cl, ocl)
+    np.testing.assert_array_equal(cd, ocd)
+    c.close()
+
+
+@pytest.mark.parametrize("n,theta", [(64, 0.4), (200, 0.5), (7, 0.4)])
+def test_closest_tree_regular_ring_ties(L, n, theta):
+    """A regular polygon: every point has two partners at the same distance
+    (two links ahead and behind), so the walk order decides which one is
+    kept; tiny rings leave no valid partner at all."""
+    w = W.ring(n, 0.01, 0.0)
+    prm = dict(w.params, velocity="Tree", tree_theta=theta)
+    c = L.Context(L.default_params(**prm))
+    c.set_points(w.x, w.infront, w.behind)
+    c.ghosts()
+    c.build_tree()
+    seedcl = np.arange(n, dtype=np.int32)[::-1].copy()
+    c.set_closest(seedcl)
+    cl, cd = c.closest()
+    p = O.params(**prm)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    tr = O.Tree(p, w.x, og[0], w.infront)
+    ocl, ocd = O.pclose_tree(tr, w.x, w.infront, w.behind, seedcl)
+    np.testing.assert_array_equal(cl, ocl)
+    np.testing.assert_array_equal(cd, ocd)
+    c.close()
 
 def test_pclose_bit_exact(L):
     w = small_tangle(6, 10)

@@ -61,6 +61,40 @@ def test_ring_speed_energy_known_answer():
     assert abs(abs(e) / (2 * np.pi * G * R ** 2 * speed) - 1) < 1e-3
 
 
+
+@pytest.mark.parametrize("order", [2, 4])
+@pytest.mark.parametrize("fixed", [0, 1])
+def test_lia_ring_closed_form(order, fixed):
+    """The LIA arm of calc_velocity (src/timestep.f90) on a regular n-gon
+    inscribed in a circle of radius R, in closed form.  With chord c =
+    2R sin(t/2), t = 2 pi/n, the finite differences of get_deriv_1/2
+    (src/derivatives.f90) reduce to the uniform stencils: second order
+    |s'| = R sin t / c, |s''| = 2R(1 - cos t)/c^2; fourth order
+    |s'| = R(8 sin t - sin 2t)/(6c), |s''| = R(5/2 - 8 cos t/3 + cos 2t/6)/c^2.
+    The velocity is beta s' x s'' along the ring's axis with beta = 1.3e-3
+    (fixed_LIA_beta) or Gamma/(4 pi) ln(1/(|s''| a))."""
+    n, R = 48, 0.01
+    w = W.ring(n, R, 0.0)
+    p = O.params(**dict(w.params, velocity="LIA", deriv_order=order, fixed_lia_beta=fixed))
+    gh = O.ghosts(p, w.x, w.infront, w.behind)
+    u, uli, ubs, ev, st = O.velocity(p, w.x, w.infront, w.behind, gh)
+    t = 2 * np.pi / n
+    c = 2 * R * np.sin(t / 2)
+    if order == 2:
+        T, K = R * np.sin(t) / c, 2 * R * (1 - np.cos(t)) / c ** 2
+    else:
+        T = R * (8 * np.sin(t) - np.sin(2 * t)) / (6 * c)
+        K = R * (2.5 - 8 * np.cos(t) / 3 + np.cos(2 * t) / 6) / c ** 2
+    G, a = w.params["quant_circ"], w.params["corea"]
+    beta = 1.3e-3 if fixed else G / (4 * np.pi) * np.log(1 / (K * a))
+    speed = beta * T * K
+    assert np.abs(np.abs(u[:, 2]) / speed - 1).max() < 1e-9
+    assert np.abs(u[:, :2]).max() / speed < 1e-9
+    assert np.all(np.sign(u[:, 2]) == np.sign(u[0, 2]))
+    # the second-order stencil is exact for the curvature of a circle
+    if order == 2:
+        assert abs(K * R - 1) < 1e-12
+
 def test_dt_bound():
     # timestep_check, src/initial.f90:606-622
     p = O.params(delta=5e-4, corea=1.3e-8)
