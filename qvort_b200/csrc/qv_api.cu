@@ -100,7 +100,7 @@ static void free_tree(TreeBuf &t) {
   if (t.ev_ctl) cudaEventDestroy(t.ev_ctl);
   void *ps[] = {t.pos, t.width, t.cent, t.circ, t.C, t.count, t.start, t.parent, t.child_first,
                 t.nchild, t.first, t.level, t.digit, t.cmask, t.w64, t.p64, t.w32, t.c32, t.p32, t.leaf_of,
-                t.ord, t.nodeA, t.nodeB, t.dig, t.rnk, t.cnt9, t.rs9, t.chunk9, t.ctl};
+                t.ord, t.nodeA, t.nodeB, t.dig, t.rnk, t.cnt9, t.rs9, t.chunk9, t.ctl, t.permb};
   for (void *q : ps)
     if (q) cudaFree(q);
   t = TreeBuf();

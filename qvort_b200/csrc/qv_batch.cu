@@ -48,7 +48,7 @@ struct BatchArgs {
   const int4 *groups;   // walk group: (first perm position, targets, root node, system)
   const int4 *sys;      // (first slot, slots, method, chunks)
   const int2 *dsrc;     // direct system: (first pack position, chunk length)
-  const int *ctl, *ord;
+  const int *ctl, *perm;
   const double *x;
   const int *inf, *beh;
   const WNode64 *w64;
@@ -281,7 +281,7 @@ __global__ void k_batch_work(BatchArgs a) {
   unsigned char *mine = bsm + per_warp * wid;
   if (*a.status) return;
   if (a.nroots > 0 && a.ctl[QV_CTL_OVERFLOW]) return;
-  const int *perm = a.nroots > 0 ? a.ord + (size_t)a.ctl[QV_CTL_DEPTH] * a.cap_pts : nullptr;
+  const int *perm = a.nroots > 0 ? a.perm : nullptr;
   unsigned ev = 0, evf = 0;  // per warp: far below 2^32
   bool bad = false;
   for (;;) {
@@ -479,7 +479,7 @@ static BatchArgs work_args(qv_batch *b) {
   a.sys = b->d_sys;
   a.dsrc = b->d_dsrc;
   a.ctl = t.ctl;
-  a.ord = t.ord;
+  a.perm = t.permb;
   a.x = c->x;
   a.inf = c->infront;
   a.beh = c->behind;

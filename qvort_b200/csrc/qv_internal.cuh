@@ -99,6 +99,7 @@ struct TreeBuf {
   int *chunk9 = nullptr;                   // per chunk of positions
   int *ctl = nullptr;                      // device control block
   int *perm = nullptr;                     // final (DFS) order of active points
+  int *permb = nullptr;                    // its storage, written by the build
   int *leaf_of = nullptr;                  // slot -> its one-point leaf (unverified)
   int n_leaf = 0;                          // slots covered by leaf_of
   int *h_ctl = nullptr;                    // pinned copy of the control block

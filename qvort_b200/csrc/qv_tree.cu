@@ -44,7 +44,11 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 #define CTL_NACT 6      // active points of this build
 #define CTL_LVL 8       // lvl_start[0..QV_MAX_DEPTH+2]
 #define CTL_NS (CTL_LVL + QV_MAX_DEPTH + 4)  // splitting nodes per level
-#define CTL_SIZE (CTL_NS + QV_MAX_DEPTH + 4)
+#define CTL_MAXC (CTL_NS + QV_MAX_DEPTH + 4) // largest splitting node per level
+#define CTL_SIZE (CTL_MAXC + QV_MAX_DEPTH + 4)
+#define LPT 4             // positions per thread in the block-local levels
+#define LMAX (BT * LPT)   // positions per block-local range (whole nodes)
+#define LCH (LMAX / 2)    // largest splitting node handed to the block-local levels
 
 struct BuildArgs {
   const int *d_nact;  // active points (device-resident count of the compaction)
@@ -55,6 +59,7 @@ struct BuildArgs {
   unsigned char *digit, *cmask;
   int *ord, *nodeA, *nodeB, *rnk, *cnt9A, *cnt9B, *rs9, *chunk9, *ctl;
   unsigned char *dig;
+  int *perm;  // out: final (depth-first) order of the active points
 };
 
 // packed per-digit counters: digits 0..4 in lo (12-bit fields), 5..8 in hi
@@ -119,7 +124,238 @@ __device__ __forceinline__ int child_digit(const double *X, const double *P, dou
   return b[0] + 2 * b[2] + 4 * b[1];
 }
 
+// Block-local levels.  Once every splitting node of level d0 holds at most LCH
+// points, the positions [0, n_act) are cut into ranges of whole nodes: range c
+// runs from the start of the node holding position c*LCH (or that position, if
+// its node does not split) to the same point of range c+1, so a range holds
+// fewer than 2*LCH positions (bounds in chunk9[0..nch], written before a grid
+// barrier).  A block then runs the remaining levels of its range with block
+// barriers instead of grid barriers: the same child digits, the same stable
+// partition (ranks from one block-wide scan of packed digit counts, a node's
+// counts from the scan at its first and one-past-last positions) and the same
+// node records; child ids are claimed with one atomic per block and level, and
+// each child's record is written by its first point.  Each position's slot,
+// node, node start and count travel with it in shared memory, so a level costs
+// one batched gather of (x, corner, width) and one atomic; the order rows are
+// written for the moment chains and the final order for the walks.  Node ids
+// are not ordered by level in this part, which nothing downstream needs.
+struct LocalSmem {
+  Pack2 exs[LMAX + 1];  // exclusive digit-count prefix at each position
+  int ordl[LMAX];       // slot at each position
+  int nodl[LMAX];       // node at each position (-1: in no splitting node)
+  int scl[LMAX];        // node start (relative) | node count << 16
+  int cfl[LMAX];        // at a node's first position: its first child
+  int cml[LMAX];        // at a node's first position: its child mask
+};
+#define LOCAL_SMEM ((int)sizeof(LocalSmem))
+
+__device__ __forceinline__ int fld12(unsigned long long v, int f) {
+  return (int)((v >> (12 * f)) & 0xFFF);
+}
+// Position offset of digit g's group inside a node whose packed per-digit
+// counts are D: the exclusive prefix sum of D's fields, taken for all fields
+// at once by multiplying with 1 + 2^12 + 2^24 + ... (no field exceeds 12 bits).
+__device__ __forceinline__ int digit_offset(const Pack2 &D, int g) {
+  const unsigned long long ilo = D.lo * 0x001001001001001ull;
+  if (g < 5) return fld12(ilo, g) - fld12(D.lo, g);
+  const unsigned long long ihi = D.hi * 0x001001001001ull;
+  return fld12(ilo, 4) + fld12(ihi, g - 5) - fld12(D.hi, g - 5);
+}
+
+__device__ void build_local(const BuildArgs &a, const int d0, const int n_act, Pack2 *sh,
+                            LocalSmem &L) {
+  __shared__ int s_base, s_more, s_split, s_stop;
+  __shared__ int wsum[BT / 32 + 1];
+  volatile int *ctl = a.ctl;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int nch = (n_act + LCH - 1) / LCH;
+  const int *nod0 = (d0 & 1) ? a.nodeB : a.nodeA;
+  const int *ord0 = a.ord + (size_t)d0 * a.cap_pts;
+  int depth = d0;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int P0 = a.chunk9[c], P1 = a.chunk9[c + 1], m = P1 - P0;
+    for (int q = tid; q < m; q += BT) {
+      const int k = nod0[P0 + q];
+      L.ordl[q] = ord0[P0 + q];
+      L.nodl[q] = k;
+      L.scl[q] = k >= 0 ? (a.start[k] - P0) | (a.count[k] << 16) : 0;
+    }
+    __syncthreads();
+    int d = d0;
+    for (;;) {
+      int *ordn = a.ord + (size_t)(d + 1) * a.cap_pts;
+      // digits of this thread's positions (one batched gather)
+      int gs[LPT], ks[LPT], ss[LPT], sc[LPT];
+      double X[LPT][3], P[LPT][3], Wd[LPT];
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        const int q = tid * LPT + j;
+        ks[j] = q < m ? L.nodl[q] : -1;
+        ss[j] = q < m ? L.ordl[q] : 0;
+        sc[j] = q < m ? L.scl[q] : 0;
+        gs[j] = NOD;
+      }
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        const bool sp = ks[j] >= 0 && (sc[j] >> 16) >= 2;
+        const int s = sp ? ss[j] : 0, k = sp ? ks[j] : 0;
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++) {
+          X[j][cc] = a.x[3 * s + cc];
+          P[j][cc] = a.pos[3 * k + cc];
+        }
+        Wd[j] = a.width[k];
+      }
+      Pack2 loc{0ull, 0ull};
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        if (ks[j] >= 0 && (sc[j] >> 16) >= 2) {
+          const int g = child_digit(X[j], P[j], Wd[j]);
+          gs[j] = g;
+          Pack2 o = pk_one(g);
+          loc.lo += o.lo; loc.hi += o.hi;
+        }
+      }
+      Pack2 tot;
+      Pack2 run = block_scan_pack(loc, &tot, sh);
+      Pack2 mine[LPT];
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        mine[j] = run;
+        L.exs[tid * LPT + j] = run;
+        if (gs[j] != NOD) {
+          Pack2 o = pk_one(gs[j]);
+          run.lo += o.lo; run.hi += o.hi;
+        }
+      }
+      if (tid == 0) {
+        L.exs[LMAX] = tot;
+        s_more = 0;
+        s_split = 0;
+      }
+      __syncthreads();
+      // splitting nodes that start here: child count and mask (first position's thread)
+      int nct = 0;
+      unsigned msk[LPT];
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        const int q = tid * LPT + j, st = sc[j] & 0xFFFF;
+        msk[j] = 0;
+        if (gs[j] != NOD && q == st) {
+          const Pack2 e = L.exs[q + (sc[j] >> 16)];
+          const Pack2 D{e.lo - mine[j].lo, e.hi - mine[j].hi};
+#pragma unroll
+          for (int g = 0; g < 8; g++) {
+            const int cg = g < 5 ? fld12(D.lo, g) : fld12(D.hi, g - 5);
+            if (cg > 0) msk[j] |= 1u << g;
+            if (cg >= 2) s_more = 1;
+          }
+          nct += __popc(msk[j]);
+        }
+      }
+      int inc = nct;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+      }
+      if (lane == 31) wsum[wid] = inc;
+      __syncthreads();
+      if (tid == 0) {
+        int r = 0;
+        for (int w = 0; w < BT / 32; w++) { int t = wsum[w]; wsum[w] = r; r += t; }
+        s_base = r > 0 ? atomicAdd((int *)&ctl[CTL_NNODES], r) : 0;
+        s_stop = (r > 0 && s_base + r > a.cap_nodes) ? 1 : 0;
+        if (s_stop) ctl[CTL_OVERFLOW] = 1;
+        if (r > 0) s_split = 1;
+      }
+      __syncthreads();
+      if (s_stop) return;
+      int id = s_base + wsum[wid] + inc - nct;
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        const int q = tid * LPT + j, st = sc[j] & 0xFFFF;
+        if (gs[j] != NOD && q == st) {
+          const int k = ks[j];
+          L.cfl[q] = id;
+          L.cml[q] = (int)msk[j];
+          a.child_first[k] = id;
+          a.nchild[k] = __popc(msk[j]);
+          a.cmask[k] = (unsigned char)msk[j];
+          id += __popc(msk[j]);
+        }
+      }
+      __syncthreads();
+      // stable scatter (next level's position, node, node start and count);
+      // the first point of each child writes the child's record
+      int nq[LPT], nk[LPT], nsc[LPT];
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        const int q = tid * LPT + j, g = gs[j];
+        nq[j] = q;
+        nk[j] = -1;
+        nsc[j] = 0;
+        if (g != NOD) {
+          const int st = sc[j] & 0xFFFF;
+          const Pack2 b = L.exs[st], e = L.exs[st + (sc[j] >> 16)];
+          const Pack2 D{e.lo - b.lo, e.hi - b.hi};
+          const int off = digit_offset(D, g);
+          const int rank = (g < 5 ? fld12(mine[j].lo, g) - fld12(b.lo, g)
+                                  : fld12(mine[j].hi, g - 5) - fld12(b.hi, g - 5));
+          nq[j] = st + off + rank;
+          ordn[P0 + nq[j]] = ss[j];
+          if (g < 8) {
+            const int cnt = g < 5 ? fld12(D.lo, g) : fld12(D.hi, g - 5);
+            const int id2 = L.cfl[st] + __popc((unsigned)L.cml[st] & ((1u << g) - 1));
+            nk[j] = id2;
+            nsc[j] = (st + off) | (cnt << 16);
+            if (rank == 0) {
+              const int k = ks[j];
+              const double W = Wd[j], w = W * 0.5;
+              const int bx = g & 1, bz = (g >> 1) & 1, by = (g >> 2) & 1;
+              a.pos[3 * id2] = bx ? __dadd_rn(P[j][0], W / 2) : P[j][0];
+              a.pos[3 * id2 + 1] = by ? __dadd_rn(P[j][1], W / 2) : P[j][1];
+              a.pos[3 * id2 + 2] = bz ? __dadd_rn(P[j][2], W / 2) : P[j][2];
+              a.width[id2] = w;
+              a.count[id2] = cnt;
+              a.start[id2] = P0 + st + off;
+              a.parent[id2] = k;
+              a.level[id2] = d + 1;
+              a.digit[id2] = (unsigned char)g;
+              a.nchild[id2] = 0;
+              a.cmask[id2] = 0;
+              a.child_first[id2] = -1;
+            }
+          }
+        }
+      }
+      const bool split = s_split, more = s_more;
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < LPT; j++) {
+        if (tid * LPT + j < m) {
+          L.ordl[nq[j]] = ss[j];
+          L.nodl[nq[j]] = nk[j];
+          L.scl[nq[j]] = nsc[j];
+        }
+      }
+      __syncthreads();
+      d++;
+      if (split) depth = max(depth, d);
+      if (!more) break;
+      if (d + 1 >= a.cap_levels || d + 1 > QV_MAX_DEPTH) {
+        if (tid == 0) ctl[CTL_OVERFLOW] = 2;
+        return;
+      }
+    }
+    for (int q = tid; q < m; q += BT) a.perm[P0 + q] = L.ordl[q];
+    __syncthreads();
+  }
+  if (tid == 0) atomicMax((int *)&ctl[CTL_DEPTH], depth);
+}
+
 __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
+  extern __shared__ __align__(16) unsigned char build_smem[];
   cg::grid_group grid = cg::this_grid();
   __shared__ Pack2 sh[BT / 32 + 1];
   __shared__ int s9[BT / 32][9];
@@ -127,11 +363,17 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
   const int n_act = *a.d_nact;
   if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_NACT] = n_act;
   int d = 0;
+  bool local = false;
   for (;;) {
     int nsplit = ctl[CTL_NS + d];
     if (nsplit == 0 || n_act == 0) break;
     if (d + 1 >= a.cap_levels || d + 1 > QV_MAX_DEPTH) {
       if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_OVERFLOW] = 2;
+      break;
+    }
+    // every splitting node of this level fits one block: finish block-locally
+    if (d > 0 && ctl[CTL_MAXC + d] <= LCH) {
+      local = true;
       break;
     }
     const int ls = ctl[CTL_LVL + d], le = ctl[CTL_LVL + d + 1];
@@ -220,7 +462,9 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
       double W = a.width[k], w = W * 0.5;
       double P[3] = {a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]};
       double M[3] = {__dadd_rn(P[0], W / 2), __dadd_rn(P[1], W / 2), __dadd_rn(P[2], W / 2)};
-      int off = 0, id = base;
+      int off = 0, id = base, cmax = 0;
+      for (int g = 0; g < 8; g++) cmax = max(cmax, c9[g]);
+      if (cmax >= 2) atomicMax((int *)&ctl[CTL_MAXC + d + 1], cmax);
       for (int g = 0; g < 8; g++) {
         if (c9[g] > 0) {
           int bx = g & 1, bz = (g >> 1) & 1, by = (g >> 2) & 1;
@@ -333,7 +577,27 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
     d++;
     grid.sync();
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_DEPTH] = d;
+  if (local) {
+    // range bounds first, for all ranges: the local levels overwrite the
+    // level-d node array of their own positions
+    const int nch = (n_act + LCH - 1) / LCH;
+    const int *nod0 = (d & 1) ? a.nodeB : a.nodeA;
+    for (int c = blockIdx.x * BT + threadIdx.x; c <= nch; c += gridDim.x * BT) {
+      const int p = c * LCH;
+      int b = n_act;
+      if (p < n_act) {
+        const int k = nod0[p];
+        b = (k >= 0 && a.count[k] >= 2) ? a.start[k] : p;
+      }
+      a.chunk9[c] = b;
+    }
+    grid.sync();
+    build_local(a, d, n_act, sh, *reinterpret_cast<LocalSmem *>(build_smem));
+  } else {
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_DEPTH] = d;
+    const int *fin = a.ord + (size_t)d * a.cap_pts;
+    for (int p = blockIdx.x * BT + threadIdx.x; p < n_act; p += gridDim.x * BT) a.perm[p] = fin[p];
+  }
 }
 
 // --------------------------------------------------------------- moments
@@ -812,6 +1076,7 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
       if ((rc = qv_grow(c, (void **)&t.dig, np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.rnk, sizeof(int) * np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.leaf_of, sizeof(int) * np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.permb, sizeof(int) * np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.cnt9, sizeof(int) * 9 * (size_t)(2 * np + 2)))) return rc;
       if ((rc = qv_grow(c, (void **)&t.rs9, sizeof(int) * 9 * (size_t)(np + 1)))) return rc;
       if ((rc = qv_grow(c, (void **)&t.chunk9, sizeof(int) * 9 * (size_t)(np / CH + 2)))) return rc;
@@ -864,7 +1129,8 @@ int qv_aux_streams(qv_ctx *c) {
 static int build_grid(qv_ctx *c) {
   if (c->build_grid) return c->build_grid;
   int per = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_build, BT, 0);
+  cudaFuncSetAttribute(k_build, cudaFuncAttributeMaxDynamicSharedMemorySize, LOCAL_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_build, BT, LOCAL_SMEM);
   if (per < 1) per = 1;
   if (per > 2) per = 2;
   c->build_grid = per * c->sm_count;
@@ -912,11 +1178,11 @@ int qv_launch_tree_build(qv_ctx *c) {
     a.start = t.start; a.parent = t.parent; a.child_first = t.child_first; a.nchild = t.nchild;
     a.level = t.level; a.digit = t.digit; a.cmask = t.cmask; a.ord = t.ord; a.nodeA = t.nodeA;
     a.nodeB = t.nodeB; a.rnk = t.rnk; a.cnt9A = t.cnt9; a.cnt9B = t.cnt9 + 9 * (size_t)(t.cap_pts + 1);
-    a.rs9 = t.rs9; a.chunk9 = t.chunk9; a.ctl = t.ctl; a.dig = t.dig;
+    a.rs9 = t.rs9; a.chunk9 = t.chunk9; a.ctl = t.ctl; a.dig = t.dig; a.perm = t.permb;
     int grid = std::min(build_grid(c), std::max(1, a.nchunks) * 4);
     grid = std::max(grid, 1);
     void *args[] = {&a};
-    QV_CUDA(c, cudaLaunchCooperativeKernel((void *)k_build, grid, BT, args, 0, c->stream));
+    QV_CUDA(c, cudaLaunchCooperativeKernel((void *)k_build, grid, BT, args, LOCAL_SMEM, c->stream));
     QV_COUNT(c, 2);
     qv_phase_end_async(c, PH_BUILD_LEVELS);
     // control block to the host, read once the moment kernels are queued
@@ -972,7 +1238,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     t.n_act = hc[CTL_NACT];
     c->n_act = t.n_act;
     t.lvl_start.assign(hc + CTL_LVL, hc + CTL_LVL + t.depth + 2);
-    t.perm = t.ord + (size_t)t.depth * t.cap_pts;
+    t.perm = t.permb;
     t.n_leaf = n;
     t.valid = true;
     return QV_OK;
@@ -1010,14 +1276,14 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   a.start = t.start; a.parent = t.parent; a.child_first = t.child_first; a.nchild = t.nchild;
   a.level = t.level; a.digit = t.digit; a.cmask = t.cmask; a.ord = t.ord; a.nodeA = t.nodeA;
   a.nodeB = t.nodeB; a.rnk = t.rnk; a.cnt9A = t.cnt9; a.cnt9B = t.cnt9 + 9 * (size_t)(t.cap_pts + 1);
-  a.rs9 = t.rs9; a.chunk9 = t.chunk9; a.ctl = t.ctl; a.dig = t.dig;
+  a.rs9 = t.rs9; a.chunk9 = t.chunk9; a.ctl = t.ctl; a.dig = t.dig; a.perm = t.permb;
   int grid = std::max(1, std::min(build_grid(c), std::max(1, a.nchunks) * 4));
   // a cooperative launch written as a launch attribute, which stream capture
   // records as a cooperative kernel node
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(BT);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = LOCAL_SMEM;
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;

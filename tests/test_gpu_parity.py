@@ -156,6 +156,22 @@ def test_tree_bit_exact_tangle(L, seed):
     _compare_trees(gt, ot)
 
 
+
+def test_tree_bit_exact_many_ranges(L):
+    """~420k points: more block-local ranges of the build than co-resident
+    blocks, so blocks take several ranges each."""
+    w = W.large_tangle(2, n_rings=1600)
+    assert w.n > 400_000  # > 2 ranges per co-resident block (296)
+    c = ctx_for(L, w)
+    c.ghosts()
+    c.build_tree()
+    gt = c.tree_export()
+    p = opar(w)
+    og = O.ghosts(p, w.x, w.infront, w.behind)
+    ot = O.Tree(p, w.x, og[0], w.infront).export()
+    _compare_trees(gt, ot)
+    c.close()
+
 def test_tree_bit_exact_edge_cases(L):
     rng = np.random.default_rng(7)
     n = 3000
