@@ -38,6 +38,8 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 // control block layout
 #define CTL_NNODES 0
+#define CTL_NGLOB 1     // nodes made by the grid-wide levels (all nodes of > LCH points)
+#define CTL_LOCALD 2    // first block-local level, -1 if none
 #define CTL_OVERFLOW 3  // 1 = node capacity, 2 = level capacity
 #define CTL_DEPTH 4
 #define CTL_NBIG 5      // number of nodes handled by k_moments_big
@@ -355,7 +357,6 @@ __device__ void build_local(const BuildArgs &a, const int d0, const int n_act, P
 }
 
 __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
-  extern __shared__ __align__(16) unsigned char build_smem[];
   cg::grid_group grid = cg::this_grid();
   __shared__ Pack2 sh[BT / 32 + 1];
   __shared__ int s9[BT / 32][9];
@@ -578,8 +579,8 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
     grid.sync();
   }
   if (local) {
-    // range bounds first, for all ranges: the local levels overwrite the
-    // level-d node array of their own positions
+    // hand over to k_build_local: the bounds of all ranges, fixed before any
+    // range's levels overwrite the level-d node array of its positions
     const int nch = (n_act + LCH - 1) / LCH;
     const int *nod0 = (d & 1) ? a.nodeB : a.nodeA;
     for (int c = blockIdx.x * BT + threadIdx.x; c <= nch; c += gridDim.x * BT) {
@@ -591,13 +592,30 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
       }
       a.chunk9[c] = b;
     }
-    grid.sync();
-    build_local(a, d, n_act, sh, *reinterpret_cast<LocalSmem *>(build_smem));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl[CTL_DEPTH] = d;
+      ctl[CTL_NGLOB] = ctl[CTL_NNODES];
+      ctl[CTL_LOCALD] = d;
+    }
   } else {
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl[CTL_DEPTH] = d;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl[CTL_DEPTH] = d;
+      ctl[CTL_NGLOB] = ctl[CTL_NNODES];
+      ctl[CTL_LOCALD] = -1;
+    }
     const int *fin = a.ord + (size_t)d * a.cap_pts;
     for (int p = blockIdx.x * BT + threadIdx.x; p < n_act; p += gridDim.x * BT) a.perm[p] = fin[p];
   }
+}
+
+// The block-local levels after k_build (nothing to do when the grid-wide
+// levels finished the tree or ran out of capacity).
+__global__ void __launch_bounds__(BT) k_build_local(BuildArgs a) {
+  extern __shared__ __align__(16) unsigned char lsm[];
+  __shared__ Pack2 sh[BT / 32 + 1];
+  const int d0 = a.ctl[CTL_LOCALD];
+  if (d0 < 0 || a.ctl[CTL_OVERFLOW]) return;
+  build_local(a, d0, *a.d_nact, sh, *reinterpret_cast<LocalSmem *>(lsm));
 }
 
 // --------------------------------------------------------------- moments
@@ -606,7 +624,7 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
 // be reassociated, so their latency is the floor; the kernels below keep the
 // chain lanes fed from shared memory while other warps gather and precompute.
 #define MW 8      // warps per block (small nodes: one warp per node)
-#define BIGN 256  // nodes with more points use a whole block
+#define BIGN LCH  // nodes with more points use a whole block (all made grid-wide)
 #define MC 256    // points per shared-memory chunk in the block kernel
 
 // One warp per node with at most BIGN points.
@@ -695,7 +713,9 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
 __global__ void k_list_big(const int *__restrict__ ctl, int cap_nodes, int k0,
                            const int *__restrict__ count, int *list, int *nlist) {
   if (ctl[CTL_OVERFLOW]) return;
-  const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
+  // nodes of more than BIGN points all come from the grid-wide levels, which
+  // are complete when this runs (the block-local levels may still be adding)
+  const int n_nodes = min(ctl[CTL_NGLOB], cap_nodes);
   for (int k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
     if (count[k] > BIGN) list[atomicAdd(nlist, 1)] = k;
 }
@@ -1007,6 +1027,7 @@ __global__ void k_build_init(double *pos, double *width, int *count, int *start,
     if (q == CTL_NNODES) v = 1;
     else if (q == CTL_NS) v = n_slots > 1 ? 1 : 0;
     else if (q == CTL_LVL + 1) v = 1;
+    else if (q == CTL_LOCALD) v = -1;
     ctl[q] = v;
   }
   for (size_t q = tid; q < (size_t)n_slots; q += stride) {
@@ -1052,6 +1073,7 @@ __global__ void k_forest_init(int nroots, const int4 *__restrict__ roots, double
     int v = 0;
     if (q == CTL_NNODES) v = nroots;
     else if (q == CTL_LVL + 1) v = nroots;
+    else if (q == CTL_LOCALD) v = -1;
     ctl[q] = v;
   }
   for (size_t q = tid; q < (size_t)n_fact; q += stride) {
@@ -1129,8 +1151,7 @@ int qv_aux_streams(qv_ctx *c) {
 static int build_grid(qv_ctx *c) {
   if (c->build_grid) return c->build_grid;
   int per = 0;
-  cudaFuncSetAttribute(k_build, cudaFuncAttributeMaxDynamicSharedMemorySize, LOCAL_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_build, BT, LOCAL_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_build, BT, 0);
   if (per < 1) per = 1;
   if (per > 2) per = 2;
   c->build_grid = per * c->sm_count;
@@ -1182,16 +1203,10 @@ int qv_launch_tree_build(qv_ctx *c) {
     int grid = std::min(build_grid(c), std::max(1, a.nchunks) * 4);
     grid = std::max(grid, 1);
     void *args[] = {&a};
-    QV_CUDA(c, cudaLaunchCooperativeKernel((void *)k_build, grid, BT, args, LOCAL_SMEM, c->stream));
+    QV_CUDA(c, cudaLaunchCooperativeKernel((void *)k_build, grid, BT, args, 0, c->stream));
     QV_COUNT(c, 2);
-    qv_phase_end_async(c, PH_BUILD_LEVELS);
-    // control block to the host, read once the moment kernels are queued
-    QV_CUDA(c, cudaMemcpyAsync(t.h_ctl, t.ctl, sizeof(int) * CTL_SIZE, cudaMemcpyDeviceToHost,
-                               c->stream));
-    QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->stream));
-    qv_phase_begin(c, PH_BUILD_MOMENTS);
-    // moments of all non-root nodes on two streams (big nodes get a block each);
-    // node counts and the overflow flag are read on the device
+    // the chains of the big nodes (all made by the grid-wide levels) start on a
+    // side stream while the block-local levels finish the tree
     QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
     QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
@@ -1200,11 +1215,25 @@ int qv_launch_tree_build(qv_ctx *c) {
     k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
         t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
         t.cent, t.circ, t.C, t.first);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 2);
+    k_build_local<<<std::max(1, std::min(nblk(n, LCH), 2 * c->sm_count)), BT, LOCAL_SMEM,
+                    c->stream>>>(a);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    qv_phase_end_async(c, PH_BUILD_LEVELS);
+    // control block to the host, read once the moment kernels are queued
+    QV_CUDA(c, cudaMemcpyAsync(t.h_ctl, t.ctl, sizeof(int) * CTL_SIZE, cudaMemcpyDeviceToHost,
+                               c->stream));
+    QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->stream));
+    qv_phase_begin(c, PH_BUILD_MOMENTS);
+    // moments of the other non-root nodes; node counts and the overflow flag
+    // are read on the device
     k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, 1, t.level, t.start,
                                                            t.count, t.ord, t.cap_pts, c->x, c->gi,
                                                            t.cent, t.circ, t.C, t.first);
     QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 3);
+    QV_COUNT(c, 1);
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
@@ -1283,7 +1312,7 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(BT);
-  cfg.dynamicSmemBytes = LOCAL_SMEM;
+  cfg.dynamicSmemBytes = 0;
   cfg.stream = c->stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -1291,6 +1320,8 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   QV_CUDA(c, cudaLaunchKernelEx(&cfg, k_build, a));
+  k_build_local<<<std::max(1, std::min(nblk(f.n_fact, LCH), 2 * c->sm_count)), BT, LOCAL_SMEM,
+                  c->stream>>>(a);
   QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->stream));
   k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
                                                       t.ctl + CTL_NBIG);
@@ -1307,6 +1338,6 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
       t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
       c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, nullptr, 0);
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 7);
+  QV_COUNT(c, 8);
   return QV_OK;
 }
