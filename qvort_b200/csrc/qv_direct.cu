@@ -78,8 +78,63 @@ __global__ void k_scatter_active(int n, const int *__restrict__ inf, const int *
   if (a) act[blk_off[blockIdx.x] + wsum[wid] + __popc(m & ((1u << lane) - 1))] = i;
 }
 
+// Ordered compaction of the k in [0, n) with flag[k] != 0 into out, count to
+// *total, for n <= QV_COMPACT1_MAX in one block: warp w takes a contiguous
+// segment of the flags 32 at a time (coalesced loads, one ballot each, lane i
+// keeps the ballots of iterations i and i + 32); a scan of the 32 warp counts
+// gives each segment's base, and a second pass over the kept ballots writes
+// the indices in order.
+__global__ void __launch_bounds__(1024) k_compact1(int n, const int *__restrict__ flag, int *out,
+                                                   int *total) {
+  __shared__ int wbase[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int seg = ((n + 1023) / 1024) * 32;  // per warp, a multiple of 32
+  const int iters = seg / 32;                // <= 64 for n <= QV_COMPACT1_MAX
+  const int lo = w * seg;
+  unsigned m0 = 0, m1 = 0;
+  int cnt = 0;
+#pragma unroll 8
+  for (int it = 0; it < iters; it++) {
+    const int k = lo + it * 32 + lane;
+    const unsigned b = __ballot_sync(0xffffffffu, k < n && flag[k] != 0);
+    if (lane == (it & 31)) {
+      if (it < 32) m0 = b; else m1 = b;
+    }
+    cnt += __popc(b);
+  }
+  if (lane == 0) wbase[w] = cnt;
+  __syncthreads();
+  if (w == 0) {
+    const int v = wbase[lane];
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    wbase[lane] = inc - v;
+    if (lane == 31) *total = inc;
+  }
+  __syncthreads();
+  int base = wbase[w];
+  for (int it = 0; it < iters; it++) {
+    const unsigned b = __shfl_sync(0xffffffffu, it < 32 ? m0 : m1, it & 31);
+    if ((b >> lane) & 1u) out[base + __popc(b & ((1u << lane) - 1))] = lo + it * 32 + lane;
+    base += __popc(b);
+  }
+}
+
 // Stable compaction of the active slots (ascending index) into c->act.
 int qv_compact_active(qv_ctx *c) {
+  if (c->n <= QV_COMPACT1_MAX) {
+    k_compact1<<<1, 1024, 0, c->stream>>>(c->n, c->infront, c->act, c->d_nact);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    QV_CUDA(c, cudaMemcpyAsync(&c->n_act, c->d_nact, sizeof(int), cudaMemcpyDeviceToHost,
+                               c->stream));
+    QV_CUDA(c, cudaStreamSynchronize(c->stream));
+    return QV_OK;
+  }
   int nb = nblk(c->n, 256);
   int *tmp = c->blkcnt;
   k_count_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp);
@@ -94,6 +149,12 @@ int qv_compact_active(qv_ctx *c) {
 
 // The same compaction without waiting for it: the count goes to c->d_nact.
 int qv_compact_active_async(qv_ctx *c) {
+  if (c->n <= QV_COMPACT1_MAX) {
+    k_compact1<<<1, 1024, 0, c->stream>>>(c->n, c->infront, c->act, c->d_nact);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    return QV_OK;
+  }
   int nb = nblk(c->n, 256);
   int *tmp = c->blkcnt;
   k_count_active<<<nb, 256, 0, c->stream>>>(c->n, c->infront, tmp);

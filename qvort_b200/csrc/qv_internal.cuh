@@ -204,6 +204,8 @@ int qv_line_reconnect(qv_ctx *c, int *count);
 __global__ void k_count_active(int n, const int *__restrict__ inf, int *blk_cnt);
 __global__ void k_scan_small(int m, int *v, int *total);
 __global__ void k_scatter_active(int n, const int *__restrict__ inf, const int *blk_off, int *act);
+#define QV_COMPACT1_MAX 65536
+__global__ void k_compact1(int n, const int *__restrict__ flag, int *out, int *total);
 int qv_compact_active_async(qv_ctx *c);
 int qv_aux_streams(qv_ctx *c);
 

@@ -406,36 +406,11 @@ static LineArgs line_args(qv_ctx *c) {
   return a;
 }
 
-// Ordered compaction in one block for up to CSMALL slots: each thread counts
-// a contiguous range, a block scan gives the offsets, each thread writes its
-// range's selected slots in order.
-#define CSMALL 65536
-__global__ void __launch_bounds__(1024) k_compact_small(int n, const int *__restrict__ flag,
-                                                        int *out, int *total) {
-  __shared__ int part[1024];
-  const int t = threadIdx.x;
-  const int per = (n + 1023) / 1024, lo = t * per, hi = min(n, lo + per);
-  int cnt = 0;
-  for (int k = lo; k < hi; k++) cnt += flag[k] != 0;
-  part[t] = cnt;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    int v = t >= off ? part[t - off] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
-  }
-  int run = part[t] - cnt;
-  for (int k = lo; k < hi; k++)
-    if (flag[k]) out[run++] = k;
-  if (t == 1023) *total = part[1023];
-}
-
-// Ordered compaction of flag[0..n) into out (the active-slot compaction run
-// on a flag array); the count goes to *total on the device.
+// Ordered compaction of flag[0..n) into out (one block up to QV_COMPACT1_MAX
+// slots, else count / scan / scatter); the count goes to *total on the device.
 static int compact_flags(qv_ctx *c, int n, const int *flag, int *out, int *total) {
-  if (n <= CSMALL) {
-    k_compact_small<<<1, 1024, 0, c->stream>>>(n, flag, out, total);
+  if (n <= QV_COMPACT1_MAX) {
+    k_compact1<<<1, 1024, 0, c->stream>>>(n, flag, out, total);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
     return QV_OK;
