@@ -40,7 +40,8 @@ __device__ __forceinline__ double dist_exact(const double *a, double b0, double 
 // skipping it leaves the result unchanged.  T is the running closestd, and,
 // from the start, the distance to the leaf of the point two links ahead or
 // behind when that leaf is itself a valid visited cell (every ancestor opens
-// for the target, checked on the parent chain with the same tests).  The box
+// for the target, checked on the parent chain with the same tests), else the
+// distance to the first valid visited cell of a near-first descent.  The box
 // distance is a lower bound taken in FP32 with a relative 1e-5 and an absolute
 // 2e-6 (|x| + L) margin, above every rounding of the operands.
 struct __align__(16) CStkEnt {
@@ -109,6 +110,47 @@ __device__ double leaf_bound(int s, int n, int nn, int n_leaf, const int *__rest
   return dist_exact(xi, hh.cx, hh.cy, hh.cz);
 }
 
+#define NFCAP 128  // per-lane stack of the near-first bound search
+#define NFMAX 512  // its node visits before it gives up (no bound)
+
+// A bound for a target whose link candidates gave none: the first valid cell
+// of the target's walk met by a depth-first descent that takes the children
+// of every opened cell nearest octant first (the target's own octant, then
+// those differing in one, two, three axes).  It only enters cells that open
+// for the target, so the leaf it returns is one the walk visits.
+__device__ double near_bound(const SNode32 *__restrict__ c32, const WNode64 *__restrict__ w64,
+                             const int *__restrict__ beh, int n, int ii, int fi, int bi,
+                             const double *xi, const float *xh, const float *xl) {
+  int stk[NFCAP];
+  int top = 0;
+  stk[top++] = 0;
+  for (int it = 0; it < NFMAX && top > 0; it++) {
+    const int node = stk[--top];
+    const SNode32 h = c32[node];
+    if (h.count <= 0) continue;
+    const float d2 = cent_d2(h, xh, xl);
+    if (h.count == 1) {
+      const WNode64 hh = w64[node];
+      if (hh.finf < 1 || hh.finf > n) continue;
+      const int j = beh[hh.finf - 1];
+      if (j == ii || j == fi || j == bi) continue;
+      return dist_exact(xi, hh.cx, hh.cy, hh.cz);
+    }
+    double d64 = -1.;
+    if (search_far(h, w64, node, d2, d2 < 1e-20f, xi, d64)) continue;  // taken whole
+    if (top + h.nchild > NFCAP) return 100.;
+    const float hw = 0.5f * h.w;
+    const int gx = (xh[0] >= h.lo[0] + hw ? 1 : 0) + (xh[2] >= h.lo[2] + hw ? 2 : 0) +
+                   (xh[1] >= h.lo[1] + hw ? 4 : 0);
+    const unsigned cm = (unsigned)h.cmask;
+    for (int r = 7; r >= 0; r--) {  // XOR masks by rising popcount: 0 1 2 4 3 5 6 7
+      const int g = gx ^ ((0x76534210u >> (4 * r)) & 0xFu);
+      if ((cm >> g) & 1u) stk[top++] = h.child_first + __popc(cm & ((1u << g) - 1u));
+    }
+  }
+  return 100.;
+}
+
 __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *__restrict__ x,
                                                          const int *__restrict__ inf,
                                                          const int *__restrict__ beh,
@@ -152,6 +194,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
       if (s2 != s1)
         ub = fmin(ub, leaf_bound(s2, n, nn, n_leaf, leaf_of, parent, beh, w64, c32, ii, fi, bi, xi,
                                  xh, xl));
+      if (ub >= 100.) ub = near_bound(c32, w64, beh, n, ii, fi, bi, xi, xh, xl);
       thr = __double2float_ru(ub) * 1.00001f + slack;
     }
     const unsigned live_mask = __ballot_sync(0xffffffffu, live);

@@ -56,12 +56,12 @@ struct __align__(16) WNode32 {
 // for theta = width/dist < 0.5 (radius 2 width), plus the cell's box as an
 // FP32 corner rounded down and a width rounded up, so that a lower bound on
 // the distance from a target to anything inside the cell costs a few FP32
-// operations.
+// operations, and the digits of the children present (bit g = child g).
 struct __align__(16) SNode32 {
   float ch[3], cl[3];
   float rhi, rlo;
   float lo[3], w;
-  int count, child_first, nchild, pad;
+  int count, child_first, nchild, cmask;
 };
 
 // FP32 payload (64 B): internal -> circ, w, C; leaf -> ghosti as (hi, lo)

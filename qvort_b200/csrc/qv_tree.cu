@@ -872,7 +872,8 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
                           const double *__restrict__ circ, const double *__restrict__ C,
                           const int *__restrict__ count, const int *__restrict__ child_first,
-                          const int *__restrict__ nchild, const int *__restrict__ first,
+                          const int *__restrict__ nchild, const unsigned char *__restrict__ cmask,
+                          const int *__restrict__ first,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
@@ -883,7 +884,9 @@ __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nro
                              const double *__restrict__ width, const double *__restrict__ cent,
                              const double *__restrict__ circ, const double *__restrict__ C,
                              const int *__restrict__ count, const int *__restrict__ child_first,
-                             const int *__restrict__ nchild, const int *__restrict__ first,
+                             const int *__restrict__ nchild,
+                             const unsigned char *__restrict__ cmask,
+                             const int *__restrict__ first,
                              const double *__restrict__ x, const double *__restrict__ gi,
                              const int *__restrict__ inf, const int *__restrict__ beh,
                              double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
@@ -891,7 +894,7 @@ __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nro
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
-    pack_node(k, nroots, pos, width, cent, circ, C, count, child_first, nchild, first, x, gi, inf,
+    pack_node(k, nroots, pos, width, cent, circ, C, count, child_first, nchild, cmask, first, x, gi, inf,
               beh, theta, extra, w64, p64, w32, c32, p32, leaf_of, n_leaf);
 }
 
@@ -899,7 +902,8 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
                           const double *__restrict__ circ, const double *__restrict__ C,
                           const int *__restrict__ count, const int *__restrict__ child_first,
-                          const int *__restrict__ nchild, const int *__restrict__ first,
+                          const int *__restrict__ nchild, const unsigned char *__restrict__ cmask,
+                          const int *__restrict__ first,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
@@ -966,7 +970,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
     s32.count = cnt;
     s32.child_first = h.child_first;
     s32.nchild = h.nchild;
-    s32.pad = 0;
+    s32.cmask = cmask[k];
     c32[k] = s32;
   }
   if (cnt == 1 && f >= 0) {
@@ -1241,7 +1245,7 @@ int qv_launch_tree_build(qv_ctx *c) {
                                c->stream));
     k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
         t.ctl, t.cap_nodes, 1, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
-        t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
+        t.nchild, t.cmask, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
         c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, t.leaf_of, n);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 2);
@@ -1335,7 +1339,7 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
                        c->stream>>>(f.nroots, f.roots, f.fact, c->x, t.ctl, t.cent);
   k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
       t.ctl, t.cap_nodes, f.nroots, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
-      t.nchild, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
+      t.nchild, t.cmask, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
       c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, nullptr, 0);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 8);
