@@ -23,6 +23,7 @@
 // octal digit per level).  A separate kernel runs the moment chains of all
 // nodes of all levels concurrently, one warp per node, with explicit
 // round-to-nearest FP64 intrinsics so no FMA contraction changes a bit.
+#include <climits>
 #include <cooperative_groups.h>
 
 #include "qv_internal.cuh"
@@ -41,6 +42,7 @@ static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 #define CTL_NGLOB 1     // nodes made by the grid-wide levels (all nodes of > LCH points)
 #define CTL_LOCALD 2    // first block-local level, -1 if none
 #define CTL_OVERFLOW 3  // 1 = node capacity, 2 = level capacity
+#define CTL_NMID 7      // number of nodes handled by the second k_moments_big
 #define CTL_DEPTH 4
 #define CTL_NBIG 5      // number of nodes handled by k_moments_big
 #define CTL_NACT 6      // active points of this build
@@ -624,10 +626,40 @@ __global__ void __launch_bounds__(BT) k_build_local(BuildArgs a) {
 // be reassociated, so their latency is the floor; the kernels below keep the
 // chain lanes fed from shared memory while other warps gather and precompute.
 #define MW 8      // warps per block (small nodes: one warp per node)
-#define BIGN LCH  // nodes with more points use a whole block (all made grid-wide)
+#define BIGN LCH  // nodes with more points: a block each, early (all made grid-wide)
+#define MIDN 128  // nodes with more points (up to BIGN): a block each, after the tree
 #define MC 256    // points per shared-memory chunk in the block kernel
+#define MBT 512   // threads of the block kernel: warp 0 runs the chains, the rest gather
 
-// One warp per node with at most BIGN points.
+// The 15 moment chains over m staged points (row stride `stride` doubles:
+// x(3), ghosti(3), x_m (ghosti_k - x_k) (9)), lane l < 15 owning chain l:
+// lanes 0-2 sum x, lanes 6-14 sum the products, and lanes 3-5 take
+// circ = (circ + ghosti) - x (src/tree.f90:160).  Every lane runs the same
+// add-then-subtract, the subtrahend being +0 outside lanes 3-5 (s - 0 = s
+// exactly), so the warp never splits into two serialised paths; each group
+// of four points is loaded ahead of its eight dependent roundings (measured
+// on B200: 19 cycles per point, the floor of two 10-cycle FP64 roundings).
+__device__ __forceinline__ double chain15(double acc, const double *rows, int stride, int m,
+                                          int lane) {
+  const bool cl = lane >= 3 && lane < 6;
+  const double *pa = rows + lane, *pz = rows + (cl ? lane - 3 : lane);
+  int q = 0;
+  for (; q + 4 <= m; q += 4) {
+    double a0 = pa[stride * q], a1 = pa[stride * (q + 1)];
+    double a2 = pa[stride * (q + 2)], a3 = pa[stride * (q + 3)];
+    double z0 = pz[stride * q], z1 = pz[stride * (q + 1)];
+    double z2 = pz[stride * (q + 2)], z3 = pz[stride * (q + 3)];
+    if (!cl) { z0 = 0.; z1 = 0.; z2 = 0.; z3 = 0.; }
+    acc = __dsub_rn(__dadd_rn(acc, a0), z0);
+    acc = __dsub_rn(__dadd_rn(acc, a1), z1);
+    acc = __dsub_rn(__dadd_rn(acc, a2), z2);
+    acc = __dsub_rn(__dadd_rn(acc, a3), z3);
+  }
+  for (; q < m; q++) acc = __dsub_rn(__dadd_rn(acc, pa[stride * q]), cl ? pz[stride * q] : 0.);
+  return acc;
+}
+
+// One thread per one-point node, then one warp per node of at most MIDN points.
 __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl, int cap_nodes, int k0,
                                                      const int *__restrict__ level,
                                                      const int *__restrict__ start,
@@ -665,19 +697,22 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
       }
     first[kl] = idx;
   }
-  // nodes of 2..BIGN points: one warp per node
+  // nodes of 2..MIDN points: one warp per node, the next 32 points' gather
+  // in flight while the chains run over the current 32
   for (int k = k0 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
     int s = start[k], n = count[k];
-    if (n < 2 || n > BIGN) continue;
+    if (n < 2 || n > MIDN) continue;
     const int *o = ord + (size_t)level[k] * cap_pts + s;
     double acc = 0.;
-    for (int base = 0; base < n; base += 32) {
-      int m = min(32, n - base);
-      if (lane < m) {
-        int idx = o[base + lane];
-        double X[3], G[3];
+    double X[3] = {0., 0., 0.}, G[3] = {0., 0., 0.};
+    if (lane < n) {
+      const int idx = o[lane];
 #pragma unroll
-        for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
+      for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
+    }
+    for (int base = 0; base < n; base += 32) {
+      const int m = min(32, n - base);
+      if (lane < m) {
         double *b = buf[wid][lane];
 #pragma unroll
         for (int c = 0; c < 3; c++) { b[c] = X[c]; b[3 + c] = G[c]; }
@@ -687,14 +722,12 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
           for (int kk = 0; kk < 3; kk++) b[6 + 3 * mm + kk] = __dmul_rn(X[mm], __dsub_rn(G[kk], X[kk]));
       }
       __syncwarp();
-      if (lane < 3) {
-        for (int q = 0; q < m; q++) acc = __dadd_rn(acc, buf[wid][q][lane]);
-      } else if (lane < 6) {
-        int c = lane - 3;
-        for (int q = 0; q < m; q++) acc = __dsub_rn(__dadd_rn(acc, buf[wid][q][3 + c]), buf[wid][q][c]);
-      } else if (lane < 15) {
-        for (int q = 0; q < m; q++) acc = __dadd_rn(acc, buf[wid][q][lane]);
+      if (base + 32 + lane < n) {
+        const int idx = o[base + 32 + lane];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
       }
+      if (lane < 15) acc = chain15(acc, &buf[wid][0][0], 15, m, lane);
       __syncwarp();
     }
     double cm = lane < 3 ? __ddiv_rn(acc, (double)n) : 0.;
@@ -709,21 +742,23 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
   }
 }
 
-// List the non-root nodes (k >= k0) with more than BIGN points (order irrelevant).
+// List the non-root nodes (k >= k0) with lo < points <= hi (order irrelevant),
+// among the nodes of the grid-wide levels (glob) or of the whole tree.  Nodes
+// of more than BIGN points all come from the grid-wide levels, which are
+// complete once k_build ends (the block-local levels may still be adding).
 __global__ void k_list_big(const int *__restrict__ ctl, int cap_nodes, int k0,
-                           const int *__restrict__ count, int *list, int *nlist) {
+                           const int *__restrict__ count, int *list, int *nlist, int lo, int hi,
+                           int glob) {
   if (ctl[CTL_OVERFLOW]) return;
-  // nodes of more than BIGN points all come from the grid-wide levels, which
-  // are complete when this runs (the block-local levels may still be adding)
-  const int n_nodes = min(ctl[CTL_NGLOB], cap_nodes);
+  const int n_nodes = min(ctl[glob ? CTL_NGLOB : CTL_NNODES], cap_nodes);
   for (int k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
-    if (count[k] > BIGN) list[atomicAdd(nlist, 1)] = k;
+    if (count[k] > lo && count[k] <= hi) list[atomicAdd(nlist, 1)] = k;
 }
 
 // One block per node with more than BIGN points: warps 1.. gather x, ghosti and
 // the Cij products of the next chunk into shared memory while warp 0's lanes
 // 0..14 run the chains over the current chunk (double buffered).
-__global__ void __launch_bounds__(256) k_moments_big(const int *__restrict__ list,
+__global__ void __launch_bounds__(MBT) k_moments_big(const int *__restrict__ list,
                                                      const int *__restrict__ nlist,
                                                      const int *__restrict__ level,
                                                      const int *__restrict__ start,
@@ -765,22 +800,7 @@ __global__ void __launch_bounds__(256) k_moments_big(const int *__restrict__ lis
       if (wid > 0) {
         if (ch + 1 < nch) produce(ch + 1, mb + ((ch + 1) & 1) * MC * 15);
       } else if (lane < 15) {
-        const int m = min(MC, n - ch * MC);
-        const double *b = cur + lane;
-        if (lane < 3 || lane >= 6) {
-          int q = 0;
-          for (; q + 4 <= m; q += 4) {
-            double a0 = b[15 * q], a1 = b[15 * (q + 1)], a2 = b[15 * (q + 2)], a3 = b[15 * (q + 3)];
-            acc = __dadd_rn(acc, a0);
-            acc = __dadd_rn(acc, a1);
-            acc = __dadd_rn(acc, a2);
-            acc = __dadd_rn(acc, a3);
-          }
-          for (; q < m; q++) acc = __dadd_rn(acc, b[15 * q]);
-        } else {
-          const double *gx = cur + (lane - 3);
-          for (int q = 0; q < m; q++) acc = __dsub_rn(__dadd_rn(acc, gx[15 * q + 3]), gx[15 * q]);
-        }
+        acc = chain15(acc, cur, 15, min(MC, n - ch * MC), lane);
       }
       __syncthreads();
     }
@@ -1215,8 +1235,8 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
     k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rnk,
-                                                        t.ctl + CTL_NBIG);
-    k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
+                                                        t.ctl + CTL_NBIG, BIGN, INT_MAX, 1);
+    k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
         t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
         t.cent, t.circ, t.C, t.first);
     QV_LAUNCH_CHECK(c);
@@ -1231,8 +1251,19 @@ int qv_launch_tree_build(qv_ctx *c) {
                                c->stream));
     QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->stream));
     qv_phase_begin(c, PH_BUILD_MOMENTS);
-    // moments of the other non-root nodes; node counts and the overflow flag
-    // are read on the device
+    // moments of the other non-root nodes: a block each above MIDN points on the
+    // root-centroid stream, a warp each below on this one; node counts and the
+    // overflow flag are read on the device
+    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
+    QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NMID, 0, sizeof(int), c->aux[1]));
+    k_list_big<<<4 * c->sm_count, 256, 0, c->aux[1]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rs9,
+                                                        t.ctl + CTL_NMID, MIDN, BIGN, 0);
+    k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[1]>>>(
+        t.rs9, t.ctl + CTL_NMID, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
+        t.cent, t.circ, t.C, t.first);
+    QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
+    QV_COUNT(c, 2);
     k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, 1, t.level, t.start,
                                                            t.count, t.ord, t.cap_pts, c->x, c->gi,
                                                            t.cent, t.circ, t.C, t.first);
@@ -1328,8 +1359,8 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
                   c->stream>>>(a);
   QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->stream));
   k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
-                                                      t.ctl + CTL_NBIG);
-  k_moments_big<<<2 * c->sm_count, 256, 2 * MC * 15 * sizeof(double), c->stream>>>(
+                                                      t.ctl + CTL_NBIG, MIDN, INT_MAX, 0);
+  k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->stream>>>(
       t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
       t.circ, t.C, t.first);
   k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.level,
