@@ -144,11 +144,12 @@ extern "C" int qv_destroy(qv_ctx *c) {
       if (q) cudaFree(q);
   }
   if (c->walk_part) cudaFree(c->walk_part);
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < 3; k++) {
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     if (c->ev_join[k]) cudaEventDestroy(c->ev_join[k]);
   }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return QV_OK;

@@ -159,8 +159,8 @@ struct qv_ctx {
   double phase_ms[PH_N] = {};
   long long launches = 0;
   unsigned long long *evals_far = nullptr;
-  cudaStream_t aux[2] = {nullptr, nullptr};  // side streams for independent chains
-  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};  // side streams for independent chains
+  cudaEvent_t ev_fork = nullptr, ev_fork2 = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
   long long last_leaf = 0, last_far = 0;
   char err[512] = {0};
 };

@@ -66,6 +66,27 @@ struct BuildArgs {
   int *perm;  // out: final (depth-first) order of the active points
 };
 
+// What pack_node needs.
+struct PackArgs {
+  int nroots;
+  const double *pos, *width, *cent, *circ, *C;
+  const int *count, *child_first, *nchild;
+  const unsigned char *cmask;
+  const int *first;
+  const double *x, *gi;
+  const int *inf, *beh;
+  double theta;
+  int extra;
+  WNode64 *w64;
+  WPay64 *p64;
+  WNode32 *w32;
+  SNode32 *c32;
+  WPay32 *p32;
+  int *leaf_of;
+  int n_leaf;
+};
+__device__ void pack_one(const PackArgs &P, int k);
+
 // packed per-digit counters: digits 0..4 in lo (12-bit fields), 5..8 in hi
 struct Pack2 {
   unsigned long long lo, hi;
@@ -899,25 +920,6 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
                           WPay32 *p32, int *leaf_of, int n_leaf);
 
-__global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, int nroots,
-                             const double *__restrict__ pos,
-                             const double *__restrict__ width, const double *__restrict__ cent,
-                             const double *__restrict__ circ, const double *__restrict__ C,
-                             const int *__restrict__ count, const int *__restrict__ child_first,
-                             const int *__restrict__ nchild,
-                             const unsigned char *__restrict__ cmask,
-                             const int *__restrict__ first,
-                             const double *__restrict__ x, const double *__restrict__ gi,
-                             const int *__restrict__ inf, const int *__restrict__ beh,
-                             double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
-                             WPay32 *p32, int *leaf_of, int n_leaf) {
-  if (ctl[CTL_OVERFLOW]) return;
-  const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
-    pack_node(k, nroots, pos, width, cent, circ, C, count, child_first, nchild, cmask, first, x, gi, inf,
-              beh, theta, extra, w64, p64, w32, c32, p32, leaf_of, n_leaf);
-}
-
 __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
                           const double *__restrict__ circ, const double *__restrict__ C,
@@ -1107,6 +1109,26 @@ __global__ void k_forest_init(int nroots, const int4 *__restrict__ roots, double
   for (size_t q = tid; q < ncnt9; q += stride) cnt9[q] = 0;
 }
 
+__device__ void pack_one(const PackArgs &P, int k) {
+  pack_node(k, P.nroots, P.pos, P.width, P.cent, P.circ, P.C, P.count, P.child_first, P.nchild,
+            P.cmask, P.first, P.x, P.gi, P.inf, P.beh, P.theta, P.extra, P.w64, P.p64, P.w32,
+            P.c32, P.p32, P.leaf_of, P.n_leaf);
+}
+
+// Walk packs of every node once all moments are in.  root_cent: the single
+// tree's root centroid, read here in place of cent[0..2] (the chain that makes
+// it runs on its own stream), or null when the roots' centroids are in place.
+__global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, PackArgs pk,
+                             const double *root_cent, double *cent) {
+  if (ctl[CTL_OVERFLOW]) return;
+  const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
+  if (root_cent && blockIdx.x == 0 && threadIdx.x < 3) cent[threadIdx.x] = root_cent[threadIdx.x];
+  __syncthreads();
+  // node 0 falls to block 0, which made the copy before the barrier
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
+    pack_one(pk, k);
+}
+
 // --------------------------------------------------------------- host side
 static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
   TreeBuf &t = c->tree;
@@ -1159,7 +1181,8 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
 
 int qv_aux_streams(qv_ctx *c) {
   if (c->aux[0]) return QV_OK;
-  for (int k = 0; k < 2; k++) {
+  QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming));
+  for (int k = 0; k < 3; k++) {
     QV_CUDA(c, cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
     QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));
   }
@@ -1180,6 +1203,19 @@ static int build_grid(qv_ctx *c) {
   if (per > 2) per = 2;
   c->build_grid = per * c->sm_count;
   return c->build_grid;
+}
+
+static PackArgs pack_args(qv_ctx *c, int nroots, int *leaf_of, int n_leaf) {
+  const TreeBuf &t = c->tree;
+  PackArgs pk;
+  pk.nroots = nroots;
+  pk.pos = t.pos; pk.width = t.width; pk.cent = t.cent; pk.circ = t.circ; pk.C = t.C;
+  pk.count = t.count; pk.child_first = t.child_first; pk.nchild = t.nchild; pk.cmask = t.cmask;
+  pk.first = t.first; pk.x = c->x; pk.gi = c->gi; pk.inf = c->infront; pk.beh = c->behind;
+  pk.theta = c->p.tree_theta; pk.extra = c->p.tree_extra_correction;
+  pk.w64 = t.w64; pk.p64 = t.p64; pk.w32 = t.w32; pk.c32 = t.c32; pk.p32 = t.p32;
+  pk.leaf_of = leaf_of; pk.n_leaf = n_leaf;
+  return pk;
 }
 
 int qv_launch_tree_build(qv_ctx *c) {
@@ -1236,6 +1272,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
     k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rnk,
                                                         t.ctl + CTL_NBIG, BIGN, INT_MAX, 1);
+    const PackArgs pk = pack_args(c, 1, t.leaf_of, n);
     k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
         t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
         t.cent, t.circ, t.C, t.first);
@@ -1246,23 +1283,23 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
     qv_phase_end_async(c, PH_BUILD_LEVELS);
-    // control block to the host, read once the moment kernels are queued
-    QV_CUDA(c, cudaMemcpyAsync(t.h_ctl, t.ctl, sizeof(int) * CTL_SIZE, cudaMemcpyDeviceToHost,
-                               c->stream));
-    QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->stream));
     qv_phase_begin(c, PH_BUILD_MOMENTS);
-    // moments of the other non-root nodes: a block each above MIDN points on the
-    // root-centroid stream, a warp each below on this one; node counts and the
-    // overflow flag are read on the device
-    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
-    QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
-    QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NMID, 0, sizeof(int), c->aux[1]));
-    k_list_big<<<4 * c->sm_count, 256, 0, c->aux[1]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rs9,
+    // After the local levels, on a third stream: the control block to the host
+    // and the moments of the nodes of MIDN..BIGN points (a block each); here,
+    // the warp-per-node moments.  Every moment kernel packs the nodes it
+    // finishes; the root is packed once its centroid (second stream) is in.
+    QV_CUDA(c, cudaEventRecord(c->ev_fork2, c->stream));
+    QV_CUDA(c, cudaStreamWaitEvent(c->aux[2], c->ev_fork2, 0));
+    QV_CUDA(c, cudaMemcpyAsync(t.h_ctl, t.ctl, sizeof(int) * CTL_SIZE, cudaMemcpyDeviceToHost,
+                               c->aux[2]));
+    QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->aux[2]));
+    QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NMID, 0, sizeof(int), c->aux[2]));
+    k_list_big<<<4 * c->sm_count, 256, 0, c->aux[2]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rs9,
                                                         t.ctl + CTL_NMID, MIDN, BIGN, 0);
-    k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[1]>>>(
+    k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[2]>>>(
         t.rs9, t.ctl + CTL_NMID, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
         t.cent, t.circ, t.C, t.first);
-    QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
+    QV_CUDA(c, cudaEventRecord(c->ev_join[2], c->aux[2]));
     QV_COUNT(c, 2);
     k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, 1, t.level, t.start,
                                                            t.count, t.ord, t.cap_pts, c->x, c->gi,
@@ -1270,16 +1307,11 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
-    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
-    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
-    QV_CUDA(c, cudaMemcpyAsync(t.cent, c->dscalar, 3 * sizeof(double), cudaMemcpyDeviceToDevice,
-                               c->stream));
-    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
-        t.ctl, t.cap_nodes, 1, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
-        t.nchild, t.cmask, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
-        c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, t.leaf_of, n);
+    for (int k = 0; k < 3; k++) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[k], 0));
+    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, c->dscalar,
+                                                          t.cent);
     QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 2);
+    QV_COUNT(c, 1);
     qv_phase_end_async(c, PH_BUILD_MOMENTS);
     QV_CUDA(c, cudaEventSynchronize(t.ev_ctl));
     const int *hc = t.h_ctl;
@@ -1360,6 +1392,7 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->stream));
   k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
                                                       t.ctl + CTL_NBIG, MIDN, INT_MAX, 0);
+  const PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
   k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->stream>>>(
       t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
       t.circ, t.C, t.first);
@@ -1368,10 +1401,7 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
                                                          c->gi, t.cent, t.circ, t.C, t.first);
   k_forest_root_cent<<<std::min(f.nroots, 2 * c->sm_count), 512, 2 * RC * 3 * sizeof(double),
                        c->stream>>>(f.nroots, f.roots, f.fact, c->x, t.ctl, t.cent);
-  k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(
-      t.ctl, t.cap_nodes, f.nroots, t.pos, t.width, t.cent, t.circ, t.C, t.count, t.child_first,
-      t.nchild, t.cmask, t.first, c->x, c->gi, c->infront, c->behind, c->p.tree_theta,
-      c->p.tree_extra_correction, t.w64, t.p64, t.w32, t.c32, t.p32, nullptr, 0);
+  k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 8);
   return QV_OK;
