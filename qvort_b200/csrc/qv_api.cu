@@ -143,6 +143,8 @@ extern "C" int qv_destroy(qv_ctx *c) {
     for (void *q : adj)
       if (q) cudaFree(q);
   }
+  if (c->line_host) cudaFreeHost(c->line_host);
+  if (c->ev_line) cudaEventDestroy(c->ev_line);
   if (c->walk_part) cudaFree(c->walk_part);
   for (int k = 0; k < 3; k++) {
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -634,15 +636,34 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
     qv_phase_end(c, PH_UPDATE);
     c->ghosts_valid = false;
   }
+  const bool search = itime % c->p.recon_shots == 0;
+  bool searched = false;
   if (c->p.line_ops) {                                           // run.f90:59
     qv_phase_begin(c, PH_LINE);
-    if ((rc = qv_line_insert(c, nullptr))) return rc;
+    if ((rc = qv_line_insert_queue(c))) return rc;
     qv_phase_end(c, PH_LINE);
+    // the candidate search goes in behind pinsert before the host waits for
+    // the new slot count: it reads that count on the device, and does nothing
+    // if pinsert stopped to have the arrays grown (it then runs again below)
+    if (search && c->n > 0) {
+      qv_phase_begin(c, PH_CLOSEST);
+      if ((rc = qv_launch_closest_ex(c, qv_line_count_dev(c), qv_line_status_dev(c), c->cap)))
+        return rc;
+      qv_phase_end(c, PH_CLOSEST);
+      searched = true;
+    }
+    qv_phase_begin(c, PH_LINE);
+    bool resumed = false;
+    if ((rc = qv_line_insert_finish(c, nullptr, &resumed))) return rc;
+    qv_phase_end(c, PH_LINE);
+    if (resumed) searched = false;
   }
-  if (itime % c->p.recon_shots == 0) {                           // run.f90:63-69
-    qv_phase_begin(c, PH_CLOSEST);
-    if ((rc = qv_launch_closest(c))) return rc;
-    qv_phase_end(c, PH_CLOSEST);
+  if (search) {                                                  // run.f90:63-69
+    if (!searched) {
+      qv_phase_begin(c, PH_CLOSEST);
+      if ((rc = qv_launch_closest(c))) return rc;
+      qv_phase_end(c, PH_CLOSEST);
+    }
     if (c->p.line_ops) {
       qv_phase_begin(c, PH_LINE);
       if (c->p.line_ops == 2)                                    // run.f90:70

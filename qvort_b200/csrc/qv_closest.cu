@@ -151,7 +151,9 @@ __device__ double near_bound(const SNode32 *__restrict__ c32, const WNode64 *__r
   return 100.;
 }
 
-__global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *__restrict__ x,
+__global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int *d_n,
+                                                         const int *d_skip,
+                                                         const double *__restrict__ x,
                                                          const int *__restrict__ inf,
                                                          const int *__restrict__ beh,
                                                          const WNode64 *__restrict__ w64,
@@ -163,6 +165,8 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
                                                          int *closest, double *closestd,
                                                          int *status) {
   extern __shared__ CStkEnt cstk[];
+  if (d_skip && *d_skip) return;
+  const int n = d_n ? *d_n : n_host;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   CStkEnt *st = cstk + wid * stk_cap;
   const int nwarps = (n + 31) / 32;
@@ -280,12 +284,16 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n, const double *_
 }
 
 #define PT 128
-__global__ void __launch_bounds__(PT) k_pclose(int n, const double *__restrict__ x,
+__global__ void __launch_bounds__(PT) k_pclose(int n_host, const int *d_n, const int *d_skip,
+                                              const double *__restrict__ x,
                                               const int *__restrict__ inf,
                                               const int *__restrict__ beh, int *closest,
                                               double *closestd) {
   __shared__ double sx[PT][3];
   __shared__ int sa[PT];
+  if (d_skip && *d_skip) return;
+  const int n = d_n ? *d_n : n_host;
+  if (blockIdx.x * PT >= n) return;  // grid sized for the capacity
   int i = blockIdx.x * PT + threadIdx.x;
   bool live = i < n && inf[i] != 0;
   double xi[3] = {0., 0., 0.};
@@ -324,11 +332,15 @@ __global__ void __launch_bounds__(PT) k_pclose(int n, const double *__restrict__
   }
 }
 
-int qv_launch_closest(qv_ctx *c) {
-  if (c->n == 0) return QV_OK;
+// The candidate search over the slots [0, n).  d_n / d_skip: when given, the
+// slot count and a skip flag are read on the device when the kernel starts
+// (the search queued behind pinsert, whose new count the host has not read
+// yet), and the grid covers n_grid slots, an upper bound on that count.
+int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_grid) {
+  if (n_grid == 0) return QV_OK;
   if (c->p.tree_theta > 0) {
     if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
-    int nwarps = (c->n + 31) / 32;
+    int nwarps = (n_grid + 31) / 32;
     int cap = 7 * (c->tree.depth + 1) + 8;
     size_t smem = sizeof(CStkEnt) * cap * CW;
     if (smem > 48 * 1024) {
@@ -340,14 +352,16 @@ int qv_launch_closest(qv_ctx *c) {
     }
     const TreeBuf &t = c->tree;
     k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, smem, c->stream>>>(
-        c->n, c->x, c->infront, c->behind, t.w64, t.c32, t.parent, t.leaf_of, t.n_leaf,
-        std::min(t.n_nodes, t.cap_nodes), (float)c->p.box_size, cap, c->closest, c->closestd,
-        c->dstatus);
+        c->n, d_n, d_skip, c->x, c->infront, c->behind, t.w64, t.c32, t.parent, t.leaf_of,
+        t.n_leaf, std::min(t.n_nodes, t.cap_nodes), (float)c->p.box_size, cap, c->closest,
+        c->closestd, c->dstatus);
   } else {
-    k_pclose<<<(c->n + PT - 1) / PT, PT, 0, c->stream>>>(c->n, c->x, c->infront, c->behind,
-                                                         c->closest, c->closestd);
+    k_pclose<<<(n_grid + PT - 1) / PT, PT, 0, c->stream>>>(c->n, d_n, d_skip, c->x, c->infront,
+                                                           c->behind, c->closest, c->closestd);
   }
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
   return QV_OK;
 }
+
+int qv_launch_closest(qv_ctx *c) { return qv_launch_closest_ex(c, nullptr, nullptr, c->n); }

@@ -148,6 +148,8 @@ struct qv_ctx {
   bool ghosts_stored = false;  // ghost arrays hold values (possibly from before a move)
   // line operations (pinsert / premove): flag and list scratch, sequential state
   void *line_flags = nullptr, *line_st = nullptr, *line_rec = nullptr;
+  void *line_host = nullptr;       // pinned copy of the ordered passes' state
+  cudaEvent_t ev_line = nullptr;   // recorded when that copy is queued
   size_t line_cap = 0;
   TreeBuf tree;
   int sm_count = 148;
@@ -193,6 +195,14 @@ int qv_launch_ab(qv_ctx *c);
 int qv_launch_rk3_stage(qv_ctx *c, int stage);
 int qv_launch_wrap(qv_ctx *c);
 int qv_launch_closest(qv_ctx *c);
+int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_grid);
+// pinsert in two halves: everything queued (flags, lists, the ordered pass),
+// then the wait for the new slot count (growing and resuming when the slots
+// ran out; *resumed tells whether that happened)
+int qv_line_insert_queue(qv_ctx *c);
+int qv_line_insert_finish(qv_ctx *c, int *inserted, bool *resumed);
+const int *qv_line_count_dev(qv_ctx *c);   // device slot count after pinsert
+const int *qv_line_status_dev(qv_ctx *c);  // device status of the ordered passes
 int qv_launch_energy(qv_ctx *c, double *out_host);
 int qv_compact_active(qv_ctx *c);
 int qv_grow_points(qv_ctx *c, int new_cap);

@@ -23,6 +23,8 @@
 // order of roundings (gfortran -O2 does not contract either).
 #include <algorithm>
 
+#include <cstring>
+
 #include "qv_internal.cuh"
 #include "qv_lia.cuh"
 
@@ -341,30 +343,64 @@ __global__ void k_rec_eval(int n, LineArgs a, RecEval *rec) {
   rec[q] = r;
 }
 
-__global__ void k_precon_seq(LineArgs a, const RecEval *rec) {
+// The ordered pass of precon_original.  The block first gathers, for a batch
+// of candidates, the candidate, its precomputed record and the current links
+// of i and j into shared memory; thread 0 then runs the candidates in order
+// from there, and after its first change of a link within the batch reads the
+// links from global memory again, so every test sees the current links.
+#define PB 512  // candidates gathered per batch
+__global__ void __launch_bounds__(256) k_precon_seq(LineArgs a, const RecEval *rec) {
+  __shared__ RecEval s_r[PB];
+  __shared__ int s_i[PB], s_ii[PB], s_ib[PB], s_jf[PB], s_jb[PB];
   LineState *s = a.st;
-  for (; s->pc < s->nc; s->pc++) {
-    const int i = a.cand[s->pc];
-    if (a.inf[i] == 0) continue;  // cleared by an earlier loop_killer
-    const int pari = a.inf[i] - 1, parb = a.beh[i] - 1;
-    const RecEval &r = rec[s->pc];
-    const int j = r.j;
-    if (j == pari || j == parb || j < 0) continue;
-    if (a.inf[j] == 0) continue;
-    const int parjb = a.beh[j] - 1;
-    if (r.parallel) continue;  // parallel filaments do not reconnect
-    const double l_after = (pari == r.pari && parjb == r.parjb)
-                               ? r.l_after
-                               : r.s3 + seg_len(a.x + 3 * pari, a.x + 3 * parjb);
-    if (l_after <= r.l_before) {
-      a.inf[parjb] = pari + 1;
-      a.beh[pari] = parjb + 1;
-      a.inf[i] = j + 1;
-      a.beh[j] = i + 1;
-      loop_killer(a, pari);
-      loop_killer(a, i);
-      s->done++;
+  const int nc = s->nc, pc0 = s->pc;
+  int done = 0;
+  for (int base = pc0; base < nc; base += PB) {
+    const int m = min(PB, nc - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < m; q += blockDim.x) {
+      const int i = a.cand[base + q];
+      const RecEval r = rec[base + q];
+      s_r[q] = r;
+      s_i[q] = i;
+      s_ii[q] = a.inf[i];
+      s_ib[q] = a.beh[i];
+      s_jf[q] = r.j >= 0 ? a.inf[r.j] : 0;
+      s_jb[q] = r.j >= 0 ? a.beh[r.j] : 0;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      bool dirty = false;  // a link changed since the gather
+      for (int q = 0; q < m; q++) {
+        const int i = s_i[q];
+        const int infi = dirty ? a.inf[i] : s_ii[q];
+        if (infi == 0) continue;  // cleared by an earlier loop_killer
+        const int pari = infi - 1, parb = (dirty ? a.beh[i] : s_ib[q]) - 1;
+        const RecEval &r = s_r[q];
+        const int j = r.j;
+        if (j == pari || j == parb || j < 0) continue;
+        if ((dirty ? a.inf[j] : s_jf[q]) == 0) continue;
+        const int parjb = (dirty ? a.beh[j] : s_jb[q]) - 1;
+        if (r.parallel) continue;  // parallel filaments do not reconnect
+        const double l_after = (pari == r.pari && parjb == r.parjb)
+                                   ? r.l_after
+                                   : r.s3 + seg_len(a.x + 3 * pari, a.x + 3 * parjb);
+        if (l_after <= r.l_before) {
+          a.inf[parjb] = pari + 1;
+          a.beh[pari] = parjb + 1;
+          a.inf[i] = j + 1;
+          a.beh[j] = i + 1;
+          loop_killer(a, pari);
+          loop_killer(a, i);
+          done++;
+          dirty = true;
+        }
+      }
+    }
+  }
+  if (threadIdx.x == 0) {
+    s->pc = max(nc, pc0);
+    s->done += done;
   }
 }
 
@@ -432,11 +468,30 @@ static int read_state(qv_ctx *c, LineState *h) {
   return QV_OK;
 }
 
+// The state's copy to pinned host memory, queued now and waited for later
+// (only for it, not for what is queued behind it).
+static int queue_state_copy(qv_ctx *c) {
+  if (!c->line_host) {
+    QV_CUDA(c, cudaMallocHost(&c->line_host, offsetof(LineState, heap)));
+    QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_line, cudaEventDisableTiming));
+  }
+  QV_CUDA(c, cudaMemcpyAsync(c->line_host, c->line_st, offsetof(LineState, heap),
+                             cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaEventRecord(c->ev_line, c->stream));
+  return QV_OK;
+}
+
+static int wait_state_copy(qv_ctx *c, LineState *h) {
+  QV_CUDA(c, cudaEventSynchronize(c->ev_line));
+  memcpy(h, c->line_host, offsetof(LineState, heap));
+  return QV_OK;
+}
+
 static __global__ void k_line_clear_status(LineState *s) { s->status = 0; }
 
-int qv_line_insert(qv_ctx *c, int *inserted) {
+int qv_line_insert_queue(qv_ctx *c) {
   int rc;
-  if (c->n == 0) { if (inserted) *inserted = 0; return QV_OK; }
+  if (c->n == 0) return QV_OK;
   // pinsert reads the stored ghosts; compute them only if none exist yet
   if (!c->ghosts_stored)
     if ((rc = qv_launch_ghosts(c))) return rc;
@@ -453,20 +508,34 @@ int qv_line_insert(qv_ctx *c, int *inserted) {
   QV_COUNT(c, 1);
   if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
   if ((rc = compact_flags(c, n, a.flag_b, (int *)a.empt, &a.st->ne))) return rc;
+  k_pinsert_seq<<<1, 1, 0, c->stream>>>(a);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return queue_state_copy(c);
+}
+
+int qv_line_insert_finish(qv_ctx *c, int *inserted, bool *resumed) {
+  int rc;
+  if (resumed) *resumed = false;
+  if (c->n == 0) { if (inserted) *inserted = 0; return QV_OK; }
+  LineArgs a = line_args(c);
   LineState h;
   for (int attempt = 0; attempt < 16; attempt++) {
-    k_pinsert_seq<<<1, 1, 0, c->stream>>>(a);
-    QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 1);
-    if ((rc = read_state(c, &h))) return rc;
+    if ((rc = wait_state_copy(c, &h))) return rc;
     if (h.status != 1) break;
     // more slots than allocated: grow the point arrays, keeping every slot in
     // use including those appended so far (the candidate and empty-slot lists
     // keep their size), and resume where the scan stopped
+    if (resumed) *resumed = true;
+    QV_CUDA(c, cudaStreamSynchronize(c->stream));  // work queued behind pinsert is done
     c->n = h.n_cur;
     if ((rc = qv_grow_points(c, c->cap + std::max(4096, c->cap / 4)))) return rc;
     a = line_args(c);
     k_line_clear_status<<<1, 1, 0, c->stream>>>(a.st);
+    k_pinsert_seq<<<1, 1, 0, c->stream>>>(a);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 2);
+    if ((rc = queue_state_copy(c))) return rc;
   }
   if (h.status == 1) return qv_fail(c, QV_ERR_NOMEM, "pinsert: slot growth did not converge");
   if (h.status == 2) return qv_fail(c, QV_ERR_STATE, "pinsert: more than %d re-tests pending", LHEAP);
@@ -474,6 +543,15 @@ int qv_line_insert(qv_ctx *c, int *inserted) {
   if (inserted) *inserted = h.done;
   return QV_OK;
 }
+
+int qv_line_insert(qv_ctx *c, int *inserted) {
+  int rc;
+  if ((rc = qv_line_insert_queue(c))) return rc;
+  return qv_line_insert_finish(c, inserted, nullptr);
+}
+
+const int *qv_line_count_dev(qv_ctx *c) { return &((LineState *)c->line_st)->n_cur; }
+const int *qv_line_status_dev(qv_ctx *c) { return &((LineState *)c->line_st)->status; }
 
 int qv_line_reconnect(qv_ctx *c, int *count) {
   int rc;
@@ -487,7 +565,7 @@ int qv_line_reconnect(qv_ctx *c, int *count) {
   if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
   RecEval *rec = (RecEval *)c->line_rec;
   k_rec_eval<<<nblk(n, 128), 128, 0, c->stream>>>(n, a, rec);
-  k_precon_seq<<<1, 1, 0, c->stream>>>(a, rec);
+  k_precon_seq<<<1, 256, 0, c->stream>>>(a, rec);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 2);
   if (count) {

@@ -247,3 +247,44 @@ def test_step_with_reconnection_equals_the_call_sequence():
     assert np.array_equal(xa[act], xb[act])
     a.close()
     b.close()
+
+
+def test_step_whose_pinsert_outgrows_the_slots_equals_the_call_sequence():
+    """qv_step queues the candidate search behind pinsert before it reads the
+    new slot count; when pinsert stops to have the arrays grown, that search
+    does nothing and runs again after the growth.  Every segment of this ring
+    splits (spacing 1.6e-5 > delta 5e-6), far more insertions than the spare
+    slots, and the step must equal the separate calls."""
+    L, W = _mods()
+    n = 20000
+    w = W.ring(n, 0.05, 0.0, seed=2)
+    prm = dict(w.params, delta=5e-6, box_size=0.3, velocity="Tree", tree_theta=0.4,
+               precision="mixed", dt=1e-9)
+    a = L.Context(L.default_params(**prm, line_ops=2))
+    a.set_points(w.x, w.infront, w.behind)
+    b = L.Context(L.default_params(**prm))
+    b.set_points(w.x, w.infront, w.behind)
+    a.step(1)
+    b.ghosts()
+    b.build_tree()
+    b.velocity(False)
+    b.step_ab()
+    assert b.pinsert() == n
+    cb, _ = b.closest()
+    b.precon()
+    b.premove()
+    b.ghosts()
+    b.enforce_periodic()
+    assert a.n == b.n == 2 * n
+    ia, _ = a.get_links()
+    ib, _ = b.get_links()
+    assert np.array_equal(ia, ib)
+    xa, _ = a.get_points()
+    xb, _ = b.get_points()
+    act = ia != 0
+    assert np.array_equal(xa[act], xb[act])
+    ca, da = a.get_closest()
+    cb2, db = b.get_closest()
+    assert np.array_equal(ca, cb2) and np.array_equal(da, db)
+    a.close()
+    b.close()
