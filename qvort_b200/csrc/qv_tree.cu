@@ -382,6 +382,7 @@ __device__ void build_local(const BuildArgs &a, const int d0, const int n_act, P
 __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
   cg::grid_group grid = cg::this_grid();
   __shared__ Pack2 sh[BT / 32 + 1];
+  __shared__ Pack2 ex1[CH + 1];  // P1: exclusive digit-count prefix at each position of a chunk
   __shared__ int s9[BT / 32][9];
   volatile int *ctl = a.ctl;
   const int n_act = *a.d_nact;
@@ -408,39 +409,82 @@ __global__ void __launch_bounds__(BT) k_build(BuildArgs a) {
     int *cntc = (d & 1) ? a.cnt9B : a.cnt9A;
     int *cntn = (d & 1) ? a.cnt9A : a.cnt9B;
 
-    // ---- P1: digits, node counts, chunk counts
+    // ---- P1: digits, node counts, chunk counts.  The loads of a thread's
+    // positions are issued together; a node's digit counts in this chunk come
+    // from the block scan (prefix at the end of its run of positions minus the
+    // prefix at its start), added to the node's counters once per digit by the
+    // thread holding the run's first position.
     for (int ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+      const int c0 = ch * CH;
+      int ks[PPT], ss[PPT], cs[PPT], st[PPT], gs[PPT];
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        const int p = c0 + threadIdx.x * PPT + j;
+        ks[j] = p < n_act ? nodc[p] : -1;
+        ss[j] = p < n_act ? ordc[p] : 0;
+      }
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        cs[j] = ks[j] >= 0 ? a.count[ks[j]] : 0;
+        st[j] = ks[j] >= 0 ? a.start[ks[j]] : 0;
+      }
+      double X[PPT][3], P[PPT][3], Wd[PPT];
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        const bool sp = cs[j] >= 2;
+        const int sl = sp ? ss[j] : 0, k = sp ? ks[j] : 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          X[j][c] = a.x[3 * sl + c];
+          P[j][c] = a.pos[3 * k + c];
+        }
+        Wd[j] = a.width[k];
+      }
       Pack2 loc{0ull, 0ull};
 #pragma unroll
       for (int j = 0; j < PPT; j++) {
-        int p = ch * CH + threadIdx.x * PPT + j;
-        int g = NOD, key = -1;
-        if (p < n_act) {
-          int k = nodc[p];
-          if (k >= 0 && a.count[k] >= 2) {
-            int s = ordc[p];
-            double X[3] = {a.x[3 * s], a.x[3 * s + 1], a.x[3 * s + 2]};
-            double P[3] = {a.pos[3 * k], a.pos[3 * k + 1], a.pos[3 * k + 2]};
-            g = child_digit(X, P, a.width[k]);
-            key = (k - ls) * 9 + g;
-          }
-          a.dig[p] = (unsigned char)g;
-        }
-        // warp-aggregated node counts
-        unsigned act = __ballot_sync(0xffffffffu, key >= 0);
-        if (key >= 0) {
-          unsigned peers = __match_any_sync(act, key);
-          int leader = __ffs(peers) - 1;
-          if ((int)(threadIdx.x & 31) == leader) atomicAdd(&cntc[key], __popc(peers));
-        }
-        if (g != NOD) {
+        const int p = c0 + threadIdx.x * PPT + j;
+        int g = NOD;
+        if (cs[j] >= 2) {
+          g = child_digit(X[j], P[j], Wd[j]);
           Pack2 o = pk_one(g);
           loc.lo += o.lo; loc.hi += o.hi;
         }
+        gs[j] = g;
+        if (p < n_act) a.dig[p] = (unsigned char)g;
       }
       Pack2 tot;
-      block_scan_pack(loc, &tot, sh);
+      Pack2 run = block_scan_pack(loc, &tot, sh);
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        ex1[threadIdx.x * PPT + j] = run;
+        if (gs[j] != NOD) {
+          Pack2 o = pk_one(gs[j]);
+          run.lo += o.lo; run.hi += o.hi;
+        }
+      }
+      if (threadIdx.x == 0) ex1[CH] = tot;
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < PPT; j++) {
+        const int q = threadIdx.x * PPT + j, p = c0 + q;
+        if (gs[j] != NOD && p == max(st[j], c0)) {
+          // a node's positions end at start + count, except for a root, whose
+          // count includes its empty slots: its positions end where the next
+          // root's begin
+          const int k = ks[j];
+          const int nend = d > 0 ? st[j] + cs[j] : (k + 1 < le ? a.start[k + 1] : n_act);
+          const int e = min(min(nend, c0 + CH), n_act) - c0;
+          const Pack2 b = ex1[q], f = ex1[e];
+          int *cn = cntc + (k - ls) * 9;
+          for (int g = 0; g < 9; g++) {
+            const int v = pk_get(f, g) - pk_get(b, g);
+            if (v > 0) atomicAdd(&cn[g], v);
+          }
+        }
+      }
       if (threadIdx.x < 9) a.chunk9[ch * 9 + threadIdx.x] = pk_get(tot, threadIdx.x);
+      __syncthreads();
     }
     grid.sync();
 
