@@ -144,6 +144,7 @@ extern "C" int qv_destroy(qv_ctx *c) {
       if (q) cudaFree(q);
   }
   if (c->line_host) cudaFreeHost(c->line_host);
+  if (c->h_stat) cudaFreeHost(c->h_stat);
   if (c->ev_line) cudaEventDestroy(c->ev_line);
   if (c->walk_part) cudaFree(c->walk_part);
   for (int k = 0; k < 3; k++) {
@@ -507,12 +508,17 @@ static int velocity_launch(qv_ctx *c) {
 
 // Wait for the stream, read the evaluation counters and the status word.
 static int velocity_collect(qv_ctx *c, long long *eval_count) {
-  unsigned long long dev_ev = 0, dev_far = 0;
-  int st = 0;
-  QV_CUDA(c, cudaMemcpyAsync(&dev_ev, c->evals, sizeof(dev_ev), cudaMemcpyDeviceToHost, c->stream));
-  QV_CUDA(c, cudaMemcpyAsync(&dev_far, c->evals_far, sizeof(dev_far), cudaMemcpyDeviceToHost, c->stream));
-  QV_CUDA(c, cudaMemcpyAsync(&st, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  // the two counters and the status word land in one pinned buffer: three
+  // asynchronous copies and a single wait
+  if (!c->h_stat) QV_CUDA(c, cudaMallocHost((void **)&c->h_stat, 4 * sizeof(unsigned long long)));
+  unsigned long long *hs = c->h_stat;
+  QV_CUDA(c, cudaMemcpyAsync(hs, c->evals, sizeof(*hs), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaMemcpyAsync(hs + 1, c->evals_far, sizeof(*hs), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaMemcpyAsync(hs + 2, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  const unsigned long long dev_ev = hs[0], dev_far = hs[1];
+  int st = 0;
+  memcpy(&st, hs + 2, sizeof(int));
   long long ev = 0;
   if (c->p.velocity == QV_VEL_TREE) {
     ev = 2LL * c->tree.n_act + (long long)dev_ev;

@@ -150,6 +150,7 @@ struct qv_ctx {
   void *line_flags = nullptr, *line_st = nullptr, *line_rec = nullptr;
   void *line_host = nullptr;       // pinned copy of the ordered passes' state
   cudaEvent_t ev_line = nullptr;   // recorded when that copy is queued
+  unsigned long long *h_stat = nullptr;  // pinned: evaluation counters and status word
   size_t line_cap = 0;
   TreeBuf tree;
   int sm_count = 148;
