@@ -423,14 +423,14 @@ def extras(ctx, w, stream, L, torch, itime):
     cur = [n]
     moved = [0, 0]
 
+    inp = dict(x=hx, infront=hinf, behind=hbeh, u1=hist[0], u2=hist[1], u3=hist[2], closest=hcl)
+    outp = dict(x=hx, u=hu, u1=hist[0], u2=hist[1], u3=hist[2], infront=hinf, behind=hbeh,
+                closest=hcl, closestd=hcd)
+
     def e2e_step(it):
-        m = cur[0]
-        c.set_state(m, x=hx, infront=hinf, behind=hbeh, u1=hist[0], u2=hist[1], u3=hist[2],
-                    closest=hcl)
-        c.step(it)
-        m = cur[0] = c.get_state(cap, x=hx, u=hu, u1=hist[0], u2=hist[1], u3=hist[2],
-                                 infront=hinf, behind=hbeh, closest=hcl, closestd=hcd)
-        moved[0] += m * (24 + 8 + 72 + 4)         # x, links, history, closest in
+        n_in = cur[0]
+        m = cur[0] = c.step_exchange(it, n_in, cap, inp, outp)
+        moved[0] += n_in * (24 + 8 + 72 + 4)      # x, links, history, closest in
         moved[1] += m * (24 + 24 + 72 + 4 + 8 + 8)  # x, u, history, closest(d), links out
 
     for it in range(3):
@@ -447,9 +447,9 @@ def extras(ctx, w, stream, L, torch, itime):
     out["e2e"] = {"value": pairs_step / (e2e_ms * 1e-3), "unit": UNIT,
                   "h2d_bytes_per_step": moved[0] // K, "d2h_bytes_per_step": moved[1] // K,
                   "ms_per_step": e2e_ms,
-                  "path": "qv_set_state (pinned host: x, links, AB history, closest) -> "
-                          "qv_step (line_ops 2) -> qv_get_state (pinned host: x, u, history, "
-                          "links, closest, closestd), wall clock"}
+                  "path": "qv_step_exchange (line_ops 2): pinned host in x, links, AB "
+                          "history, closest; out x, u, history, links, closest, closestd; "
+                          "wall clock"}
 
     # ---- gradients/s on the differentiation workload: 16 trefoil rings,
     # N = 50,000, periodic, K = 256 Adams-Bashforth steps checkpointed every 16,

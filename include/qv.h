@@ -119,6 +119,16 @@ typedef struct qv_state {
 } qv_state;
 int qv_set_state(qv_ctx *ctx, int n, const qv_state *s);
 int qv_get_state(qv_ctx *ctx, int cap, qv_state *s, int *n);
+/* One iteration of the run.f90 loop (src/run.f90:41-93) with the host copy of
+ * f(:): the same as qv_set_state(n, in), qv_step(itime), qv_get_state(cap,
+ * out, n_out), with one wait.  The copies overlap the step as far as the data
+ * allows: the AB history and closest go up on a side stream and the update
+ * waits for them; everything but x comes back while the closing ghosts and
+ * wrap run.  in and out may point at the same host arrays; none of them is
+ * read or written after the call returns.  n_out > cap: QV_ERR_ARG with
+ * *n_out set and out untouched (the step itself has run). */
+int qv_step_exchange(qv_ctx *ctx, int itime, int n, const qv_state *in, int cap, qv_state *out,
+                     int *n_out);
 /* Device pointers of the context's arrays (valid until the next set_points). */
 int qv_device_arrays(qv_ctx *ctx, double **x, double **u, int **infront, int **behind);
 

@@ -153,6 +153,7 @@ extern "C" int qv_destroy(qv_ctx *c) {
   }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
+  if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return QV_OK;
@@ -622,8 +623,21 @@ extern "C" int qv_energy(qv_ctx *c, double *energy) {
   return qv_launch_energy(c, energy);
 }
 
-extern "C" int qv_step(qv_ctx *c, int itime) {
-  QV_CHECK_CTX(c);
+// Inputs of qv_step_exchange still in flight on a side stream (the AB history
+// and closest): the update is their first reader, so it waits for them there.
+static int wait_pending_inputs(qv_ctx *c) {
+  if (!c->in_pending) return QV_OK;
+  c->in_pending = false;
+  QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_in, 0));
+  return QV_OK;
+}
+
+typedef int (*step_hook)(qv_ctx *c, void *arg);
+
+// One run.f90 step, queued (the host waits inside only for pinsert's new slot
+// count and the tree's node count); `after_lines`, if given, runs once the
+// line operations are queued, before the closing ghosts and wrap.
+static int step_body(qv_ctx *c, int itime, step_hook after_lines, void *arg) {
   int rc;
   qv_phase_begin(c, PH_GHOSTS);
   if ((rc = qv_launch_ghosts(c))) return rc;                     // run.f90:41
@@ -634,10 +648,12 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
     qv_phase_end(c, PH_BUILD);
   }
   if (c->p.runge_kutta) {                                        // run.f90:50-54
+    if ((rc = wait_pending_inputs(c))) return rc;
     if ((rc = rk3_stages(c))) return rc;
   } else {
     if ((rc = velocity_launch(c))) return rc;
     qv_phase_begin(c, PH_UPDATE);
+    if ((rc = wait_pending_inputs(c))) return rc;
     if ((rc = qv_launch_ab(c))) return rc;
     qv_phase_end(c, PH_UPDATE);
     c->ghosts_valid = false;
@@ -678,12 +694,118 @@ extern "C" int qv_step(qv_ctx *c, int itime) {
       qv_phase_end(c, PH_LINE);
     }
   }
+  if (after_lines)
+    if ((rc = after_lines(c, arg))) return rc;
   qv_phase_begin(c, PH_WRAP);
   if ((rc = qv_launch_ghosts(c))) return rc;                     // run.f90:75
   if ((rc = qv_launch_wrap(c))) return rc;                       // run.f90:82-93
   qv_phase_end(c, PH_WRAP);
   c->ghosts_valid = false;
+  return QV_OK;
+}
+
+extern "C" int qv_step(qv_ctx *c, int itime) {
+  QV_CHECK_CTX(c);
+  int rc;
+  if ((rc = step_body(c, itime, nullptr, nullptr))) return rc;
   return velocity_collect(c, nullptr);  // one wait per step; reports any status
+}
+
+// ------------------------------------------------ step with the host copy
+struct ExchangeOut {
+  int cap;
+  qv_state *out;
+  bool over = false, queued = false;
+};
+
+// After the line operations every array but x is final: copy those out on a
+// side stream while the closing ghosts and wrap run.
+static int exchange_out_hook(qv_ctx *c, void *arg) {
+  ExchangeOut *o = (ExchangeOut *)arg;
+  if (c->n > o->cap) {
+    o->over = true;
+    return QV_OK;
+  }
+  if (c->n == 0) return QV_OK;
+  const size_t v = sizeof(double) * 3 * (size_t)c->n, ni = sizeof(int) * (size_t)c->n;
+  const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
+  cudaStream_t sa = c->aux[2];
+  QV_CUDA(c, cudaEventRecord(c->ev_fork2, c->stream));
+  QV_CUDA(c, cudaStreamWaitEvent(sa, c->ev_fork2, 0));
+  qv_state *s = o->out;
+  double *hd[] = {s->u, s->u1, s->u2, s->u3};
+  const double *dd[] = {c->u, c->u1, c->u2, c->u3};
+  for (int k = 0; k < 4; k++)
+    if (hd[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], dd[k], v, d2h, sa));
+  if (s->infront) QV_CUDA(c, cudaMemcpyAsync(s->infront, c->infront, ni, d2h, sa));
+  if (s->behind) QV_CUDA(c, cudaMemcpyAsync(s->behind, c->behind, ni, d2h, sa));
+  if (s->closest) QV_CUDA(c, cudaMemcpyAsync(s->closest, c->closest, ni, d2h, sa));
+  if (s->closestd)
+    QV_CUDA(c, cudaMemcpyAsync(s->closestd, c->closestd, sizeof(double) * c->n, d2h, sa));
+  QV_CUDA(c, cudaEventRecord(c->ev_join[2], sa));
+  o->queued = true;
+  return QV_OK;
+}
+
+extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in, int cap,
+                                qv_state *out, int *n_out) {
+  QV_CHECK_CTX(c);
+  if (!in || !out || !n_out || n < 0 || (n > 0 && (!in->x || !in->infront || !in->behind)))
+    return qv_fail(c, QV_ERR_ARG, "qv_step_exchange: x, infront and behind are required");
+  int rc;
+  if ((rc = reserve_points(c, std::max(n, 1)))) return rc;
+  if ((rc = qv_aux_streams(c))) return rc;
+  c->n = n;
+  if (n > 0) {
+    const size_t v = sizeof(double) * 3 * (size_t)n;
+    const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    // what the step reads first, here; the AB history and closest on a side
+    // stream, awaited by the update
+    QV_CUDA(c, cudaMemcpyAsync(c->x, in->x, v, h2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->infront, in->infront, sizeof(int) * n, h2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->behind, in->behind, sizeof(int) * n, h2d, c->stream));
+    double *zv[] = {c->u, c->u_li, c->u_bs};
+    for (double *q : zv) QV_CUDA(c, cudaMemsetAsync(q, 0, v, c->stream));
+    QV_CUDA(c, cudaMemsetAsync(c->closestd, 0, sizeof(double) * n, c->stream));
+    cudaStream_t sa = c->aux[2];
+    QV_CUDA(c, cudaEventRecord(c->ev_fork2, c->stream));
+    QV_CUDA(c, cudaStreamWaitEvent(sa, c->ev_fork2, 0));
+    const double *hs[] = {in->u1, in->u2, in->u3};
+    double *hd[] = {c->u1, c->u2, c->u3};
+    for (int k = 0; k < 3; k++) {
+      if (hs[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], hs[k], v, h2d, sa));
+      else QV_CUDA(c, cudaMemsetAsync(hd[k], 0, v, sa));
+    }
+    if (in->closest) QV_CUDA(c, cudaMemcpyAsync(c->closest, in->closest, sizeof(int) * n, h2d, sa));
+    else QV_CUDA(c, cudaMemsetAsync(c->closest, 0, sizeof(int) * n, sa));
+    QV_CUDA(c, cudaEventRecord(c->ev_in, sa));
+    c->in_pending = true;
+  }
+  c->ghosts_valid = false;
+  c->ghosts_stored = false;
+  c->tree.valid = false;
+  ExchangeOut o;
+  o.cap = cap;
+  o.out = out;
+  rc = step_body(c, itime, exchange_out_hook, &o);
+  if (rc) {
+    // nothing may still read the caller's arrays once this returns
+    c->in_pending = false;
+    cudaStreamSynchronize(c->aux[2]);
+    cudaStreamSynchronize(c->stream);
+    return rc;
+  }
+  *n_out = c->n;
+  if (!o.over && out->x && c->n > 0)
+    QV_CUDA(c, cudaMemcpyAsync(out->x, c->x, sizeof(double) * 3 * (size_t)c->n,
+                               cudaMemcpyDeviceToHost, c->stream));
+  if (o.queued) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[2], 0));
+  rc = velocity_collect(c, nullptr);
+  if (rc) return rc;
+  if (o.over)
+    return qv_fail(c, QV_ERR_ARG, "qv_step_exchange: %d slots in use, host arrays hold %d", c->n,
+                   cap);
+  return QV_OK;
 }
 
 // One step of qv_step's sequence for a point set that does not change (no

@@ -151,6 +151,8 @@ struct qv_ctx {
   void *line_host = nullptr;       // pinned copy of the ordered passes' state
   cudaEvent_t ev_line = nullptr;   // recorded when that copy is queued
   unsigned long long *h_stat = nullptr;  // pinned: evaluation counters and status word
+  cudaEvent_t ev_in = nullptr;  // qv_step_exchange: the side-stream inputs are in
+  bool in_pending = false;      // ... and the next update must wait for them
   size_t line_cap = 0;
   TreeBuf tree;
   int sm_count = 148;

@@ -1226,6 +1226,7 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
 int qv_aux_streams(qv_ctx *c) {
   if (c->aux[0]) return QV_OK;
   QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming));
+  QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
   for (int k = 0; k < 3; k++) {
     QV_CUDA(c, cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
     QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));

@@ -120,6 +120,7 @@ _SIGS = {
     "qv_step": [_P, C.c_int],
     "qv_set_state": [_P, C.c_int, C.POINTER(QvState)],
     "qv_get_state": [_P, C.c_int, C.POINTER(QvState), _I],
+    "qv_step_exchange": [_P, C.c_int, C.c_int, C.POINTER(QvState), C.c_int, C.POINTER(QvState), _I],
     "qv_steps": [_P, C.c_int, C.c_int],
     "qv_sync": [_P],
     "qv_profile": [_P, C.c_int],
@@ -267,6 +268,16 @@ class Context:
         the slot count in use."""
         m = C.c_int()
         self._check(_lib.qv_get_state(self._h, cap, C.byref(self._state(arrays)), C.byref(m)))
+        self.n = m.value
+        return m.value
+
+    def step_exchange(self, itime: int, n: int, cap: int, inp: dict, out: dict) -> int:
+        """One step with the host copy of the state: set_state(n, **inp), step,
+        get_state(cap, **out) in one call (inp and out may share arrays); the
+        copies overlap the step where the data allows.  Returns the slot count."""
+        m = C.c_int()
+        self._check(_lib.qv_step_exchange(self._h, itime, n, C.byref(self._state(inp)), cap,
+                                          C.byref(self._state(out)), C.byref(m)))
         self.n = m.value
         return m.value
 

@@ -156,7 +156,6 @@ def test_tree_bit_exact_tangle(L, seed):
     _compare_trees(gt, ot)
 
 
-
 def test_tree_bit_exact_many_ranges(L):
     """~420k points: more block-local ranges of the build than co-resident
     blocks, so blocks take several ranges each."""
@@ -171,6 +170,7 @@ def test_tree_bit_exact_many_ranges(L):
     ot = O.Tree(p, w.x, og[0], w.infront).export()
     _compare_trees(gt, ot)
     c.close()
+
 
 def test_tree_bit_exact_edge_cases(L):
     rng = np.random.default_rng(7)
@@ -588,3 +588,58 @@ def test_field_velocity_tree_matches_oracle(L, bc, theta):
     assert np.array_equal(np.isnan(u), nan)
     ok = ~nan.any(axis=1)
     assert rel_max(u[ok], uo[ok]) < 1e-12, rel_max(u[ok], uo[ok])
+
+
+@pytest.mark.parametrize("delta", [4.5e-4, 4.1e-4])
+def test_step_exchange_equals_set_step_get(delta):
+    """qv_step_exchange (one call, copies overlapping the step) leaves the host
+    copy of f(:) exactly as qv_set_state, qv_step, qv_get_state do, through
+    steps with reconnections (delta 4.5e-4) or insertions (4.1e-4, below the
+    point spacing 4.2e-4); a host copy too small for the slot count is an
+    error that leaves it untouched."""
+    from qvort_b200 import lib as L
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).parent))
+    from test_oracle import _touching_rings
+
+    x, inf, beh = _touching_rings(n=60, R=0.004, gap=4e-5)
+    prm = dict(W.ring(8).params, delta=delta, box_size=0.1, tree_theta=0.4, velocity="Tree",
+               precision="mixed", dt=1e-6, line_ops=2)
+    n0 = len(x)
+    cap = 4 * n0
+
+    def host():
+        h = dict(x=np.zeros((cap, 3)), u=np.zeros((cap, 3)), u1=np.zeros((cap, 3)),
+                 u2=np.zeros((cap, 3)), u3=np.zeros((cap, 3)), infront=np.zeros(cap, np.int32),
+                 behind=np.zeros(cap, np.int32), closest=np.zeros(cap, np.int32),
+                 closestd=np.zeros(cap))
+        h["x"][:n0] = x
+        h["infront"][:n0] = inf
+        h["behind"][:n0] = beh
+        return h
+
+    ha, hb = host(), host()
+    a = L.Context(L.default_params(**prm))
+    b = L.Context(L.default_params(**prm))
+    ins = ("x", "infront", "behind", "u1", "u2", "u3", "closest")
+    na = nb = n0
+    for it in range(1, 6):
+        na = a.step_exchange(it, na, cap, {k: ha[k] for k in ins}, ha)
+        b.set_state(nb, **{k: hb[k] for k in ins})
+        b.step(it)
+        nb = b.get_state(cap, **hb)
+        assert na == nb
+        for k in ha:
+            assert np.array_equal(ha[k][:na], hb[k][:nb]), (it, k)
+    if delta < 4.2e-4:
+        assert na > n0                                      # points were inserted
+    else:
+        assert not np.array_equal(ha["infront"][:n0], inf)  # links were reconnected
+    before = {k: v.copy() for k, v in ha.items()}
+    with pytest.raises(L.QvError):
+        a.step_exchange(6, na, na - 1, {k: ha[k] for k in ins}, ha)
+    for k in ha:
+        assert np.array_equal(ha[k], before[k]), k
+    a.close()
+    b.close()
