@@ -111,6 +111,14 @@ module qv_iface
       type(qv_state_t), intent(in) :: s
       integer(c_int), intent(out) :: n
     end function
+    integer(c_int) function qv_step_exchange(ctx, itime, n, sin, cap, sout, nout) &
+        bind(C, name='qv_step_exchange')
+      import :: c_ptr, c_int, qv_state_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: itime, n, cap
+      type(qv_state_t), intent(in) :: sin, sout
+      integer(c_int), intent(out) :: nout
+    end function
   end interface
 
   type(c_ptr), save :: ctx = c_null_ptr
@@ -173,6 +181,11 @@ contains
   end subroutine
 
   subroutine gather()
+    call gather_arrays()
+    call check(qv_set_state(ctx, int(size(f), c_int), state()), 'qv_iface:qv_set_state')
+  end subroutine
+
+  subroutine gather_arrays()
     integer :: n
     n = size(f)
     if (allocated(xs)) then
@@ -185,7 +198,6 @@ contains
     h2(1,:) = f(:)%u2(1) ; h2(2,:) = f(:)%u2(2) ; h2(3,:) = f(:)%u2(3)
     h3(1,:) = f(:)%u3(1) ; h3(2,:) = f(:)%u3(2) ; h3(3,:) = f(:)%u3(3)
     infs = f(:)%infront ; behs = f(:)%behind ; cls = f(:)%closest
-    call check(qv_set_state(ctx, int(n, c_int), state()), 'qv_iface:qv_set_state')
   end subroutine
 
   function state() result(s)
@@ -199,6 +211,10 @@ contains
   subroutine scatter()
     integer(c_int) :: n
     call check(qv_get_state(ctx, int(size(xs, 2), c_int), state(), n), 'qv_iface:qv_get_state')
+    call scatter_arrays()
+  end subroutine
+
+  subroutine scatter_arrays()
     f(:)%x(1) = xs(1,:) ; f(:)%x(2) = xs(2,:) ; f(:)%x(3) = xs(3,:)
     f(:)%u(1) = us(1,:) ; f(:)%u(2) = us(2,:) ; f(:)%u(3) = us(3,:)
     f(:)%u1(1) = h1(1,:) ; f(:)%u1(2) = h1(2,:) ; f(:)%u1(3) = h1(3,:)
@@ -212,9 +228,12 @@ contains
   !> premove left to the host, see INTEGRATION.md for the ordering)
   subroutine qv_gpu_step(it)
     integer, intent(in) :: it
-    call gather()
-    call check(qv_step(ctx, int(it, c_int)), 'qv_iface:qv_step')
-    call scatter()
+    integer(c_int) :: n
+    call gather_arrays()
+    ! set_state + step + get_state in one call, the copies overlapping the step
+    call check(qv_step_exchange(ctx, int(it, c_int), int(size(f), c_int), state(), &
+                                int(size(xs, 2), c_int), state(), n), 'qv_iface:qv_step_exchange')
+    call scatter_arrays()
   end subroutine
 
   !> replaces the first loop of pmotion (src/timestep.f90:41-47): f(:)%u,

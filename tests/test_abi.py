@@ -40,3 +40,13 @@ def test_default_params_are_run_in_defaults():
     p = L.default_params()
     assert p.quant_circ == 9.97e-4 and p.corea == 8.244023e-9
     assert p.deriv_order == 2 and p.tree_extra_correction == 1 and p.recon_shots == 1
+
+
+def test_fortran_shim_binds_declared_entry_points():
+    """Every bind(C, name=...) of the Fortran interface module names an entry
+    point that include/qv.h declares (and the library exports, above)."""
+    text = (ROOT / "shim" / "qv_iface.f90").read_text()
+    bound = set(re.findall(r"bind\(C,\s*name='(qv_[a-z0-9_]+)'\)", text))
+    assert "qv_step_exchange" in bound and "qv_step" in bound
+    missing = sorted(bound - set(_declared()))
+    assert not missing, missing
