@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
 
 // ---------------------------------------------------------------- mixed walk
 template <int BC>
-__global__ void __launch_bounds__(WW * 32) k_walk32(WalkArgs a) {
+__global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 blocks/SM: measured fastest (5-7 tried)
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   extern __shared__ StkEnt stk_dyn[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
