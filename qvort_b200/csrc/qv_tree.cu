@@ -84,6 +84,7 @@ struct PackArgs {
   WPay32 *p32;
   int *leaf_of;
   int n_leaf;
+  int full;  // also the FP64 walk payload and the search header (a forest needs neither)
 };
 __device__ void pack_one(const PackArgs &P, int k);
 
@@ -693,6 +694,7 @@ __global__ void __launch_bounds__(BT) k_build_local(BuildArgs a) {
 #define MW 8      // warps per block (small nodes: one warp per node)
 #define BIGN LCH  // nodes with more points: a block each, early (all made grid-wide)
 #define MIDN 128  // nodes with more points (up to BIGN): a block each, after the tree
+#define TN 8      // nodes with at most this many points: a thread each
 #define MC 256    // points per shared-memory chunk in the block kernel
 #define MBT 512   // threads of the block kernel: warp 0 runs the chains, the rest gather
 
@@ -724,7 +726,7 @@ __device__ __forceinline__ double chain15(double acc, const double *rows, int st
   return acc;
 }
 
-// One thread per one-point node, then one warp per node of at most MIDN points.
+// One thread per node of at most TN points, then one warp per node of at most MIDN points.
 __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl, int cap_nodes, int k0,
                                                      const int *__restrict__ level,
                                                      const int *__restrict__ start,
@@ -737,36 +739,63 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
   int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
-  // one-point nodes (most of a tree): one thread each, the 15 chains of a
-  // single point with the same roundings as the warp path below
+  // nodes of at most TN points (most of a tree): one thread each, the 15
+  // chains over the node's points in the warp path's order and roundings
+  // (the next point's loads issued before the current point's operations)
   for (int kl = k0 + blockIdx.x * blockDim.x + threadIdx.x; kl < n_nodes;
        kl += gridDim.x * blockDim.x) {
-    if (count[kl] != 1) continue;
-    const int idx = ord[(size_t)level[kl] * cap_pts + start[kl]];
-    double X[3], G[3], cm[3], ci[3];
+    const int n = count[kl];
+    if (n < 1 || n > TN) continue;
+    const int *o = ord + (size_t)level[kl] * cap_pts + start[kl];
+    double ac[3] = {0., 0., 0.}, ai[3] = {0., 0., 0.}, aC[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) aC[q] = 0.;
+    int idx = o[0];
+    const int idx0 = idx;
+    double X[3], G[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) { X[c] = x[3 * idx + c]; G[c] = gi[3 * idx + c]; }
+    for (int q = 0; q < n; q++) {
+      double nX[3], nG[3];
+      if (q + 1 < n) {
+        const int ni = o[q + 1];
+#pragma unroll
+        for (int c = 0; c < 3; c++) { nX[c] = x[3 * ni + c]; nG[c] = gi[3 * ni + c]; }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        ac[c] = __dadd_rn(ac[c], X[c]);
+        ai[c] = __dsub_rn(__dadd_rn(ai[c], G[c]), X[c]);
+      }
+#pragma unroll
+      for (int mm = 0; mm < 3; mm++)
+#pragma unroll
+        for (int kk = 0; kk < 3; kk++)
+          aC[3 * mm + kk] = __dadd_rn(aC[3 * mm + kk], __dmul_rn(X[mm], __dsub_rn(G[kk], X[kk])));
+      if (q + 1 < n) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) { X[c] = nX[c]; G[c] = nG[c]; }
+      }
+    }
+    double cm[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      cm[c] = __ddiv_rn(__dadd_rn(0., X[c]), 1.);
-      ci[c] = __dsub_rn(__dadd_rn(0., G[c]), X[c]);
+      cm[c] = __ddiv_rn(ac[c], (double)n);
       cent[3 * kl + c] = cm[c];
-      circ[3 * kl + c] = ci[c];
+      circ[3 * kl + c] = ai[c];
     }
 #pragma unroll
     for (int mm = 0; mm < 3; mm++)
 #pragma unroll
-      for (int kk = 0; kk < 3; kk++) {
-        double acc = __dadd_rn(0., __dmul_rn(X[mm], __dsub_rn(G[kk], X[kk])));
-        C[9 * kl + 3 * mm + kk] = __dsub_rn(acc, __dmul_rn(cm[mm], ci[kk]));
-      }
-    first[kl] = idx;
+      for (int kk = 0; kk < 3; kk++)
+        C[9 * kl + 3 * mm + kk] = __dsub_rn(aC[3 * mm + kk], __dmul_rn(cm[mm], ai[kk]));
+    first[kl] = idx0;
   }
-  // nodes of 2..MIDN points: one warp per node, the next 32 points' gather
+  // nodes of TN+1..MIDN points: one warp per node, the next 32 points' gather
   // in flight while the chains run over the current 32
   for (int k = k0 + blockIdx.x * MW + wid; k < n_nodes; k += gridDim.x * MW) {
     int s = start[k], n = count[k];
-    if (n < 2 || n > MIDN) continue;
+    if (n <= TN || n > MIDN) continue;
     const int *o = ord + (size_t)level[k] * cap_pts + s;
     double acc = 0.;
     double X[3] = {0., 0., 0.}, G[3] = {0., 0., 0.};
@@ -962,7 +991,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
-                          WPay32 *p32, int *leaf_of, int n_leaf);
+                          WPay32 *p32, int *leaf_of, int n_leaf, int full);
 
 __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
@@ -973,7 +1002,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
-                          WPay32 *p32, int *leaf_of, int n_leaf) {
+                          WPay32 *p32, int *leaf_of, int n_leaf, int full) {
   WNode64 h;
   h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
   h.width = width[k];
@@ -1022,7 +1051,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
     h32.rlo = __double2float_rn(rc2 * (1. - 4e-6));
   }
   w32[k] = h32;
-  {
+  if (full) {  // the candidate search's header
     SNode32 s32;
     for (int c = 0; c < 3; c++) {
       s32.ch[c] = h32.ch[c];
@@ -1064,7 +1093,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
   }
   q.pad = 0.;
   r.pad = 0.f;
-  p64[k] = q;
+  if (full) p64[k] = q;  // the FP64 walk's payload
   p32[k] = r;
 }
 
@@ -1156,7 +1185,7 @@ __global__ void k_forest_init(int nroots, const int4 *__restrict__ roots, double
 __device__ void pack_one(const PackArgs &P, int k) {
   pack_node(k, P.nroots, P.pos, P.width, P.cent, P.circ, P.C, P.count, P.child_first, P.nchild,
             P.cmask, P.first, P.x, P.gi, P.inf, P.beh, P.theta, P.extra, P.w64, P.p64, P.w32,
-            P.c32, P.p32, P.leaf_of, P.n_leaf);
+            P.c32, P.p32, P.leaf_of, P.n_leaf, P.full);
 }
 
 // Walk packs of every node once all moments are in.  root_cent: the single
@@ -1260,6 +1289,7 @@ static PackArgs pack_args(qv_ctx *c, int nroots, int *leaf_of, int n_leaf) {
   pk.theta = c->p.tree_theta; pk.extra = c->p.tree_extra_correction;
   pk.w64 = t.w64; pk.p64 = t.p64; pk.w32 = t.w32; pk.c32 = t.c32; pk.p32 = t.p32;
   pk.leaf_of = leaf_of; pk.n_leaf = n_leaf;
+  pk.full = 1;
   return pk;
 }
 
@@ -1437,7 +1467,8 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->stream));
   k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
                                                       t.ctl + CTL_NBIG, MIDN, INT_MAX, 0);
-  const PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
+  PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
+  pk.full = 0;  // the batch runs the mixed walk only and no candidate search
   k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->stream>>>(
       t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
       t.circ, t.C, t.first);
