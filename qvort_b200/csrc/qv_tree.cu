@@ -1461,24 +1461,42 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  // the roots' centroid chains need only the active slots: a side stream,
+  // from the start (the events fork and join inside a captured graph too)
+  QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+  QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
+  k_forest_root_cent<<<std::min(f.nroots, 2 * c->sm_count), 512, 2 * RC * 3 * sizeof(double),
+                       c->aux[1]>>>(f.nroots, f.roots, f.fact, c->x, t.ctl, t.cent);
+  QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
   QV_CUDA(c, cudaLaunchKernelEx(&cfg, k_build, a));
+  // the chains of the nodes of more than BIGN points (all made by the
+  // grid-wide levels) on another side stream while the local levels run
+  QV_CUDA(c, cudaEventRecord(c->ev_fork2, c->stream));
+  QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork2, 0));
+  QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
+  k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
+                                                      t.ctl + CTL_NBIG, BIGN, INT_MAX, 1);
+  k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
+      t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
+      t.circ, t.C, t.first);
+  QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
   k_build_local<<<std::max(1, std::min(nblk(f.n_fact, LCH), 2 * c->sm_count)), BT, LOCAL_SMEM,
                   c->stream>>>(a);
-  QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->stream));
-  k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
-                                                      t.ctl + CTL_NBIG, MIDN, INT_MAX, 0);
-  PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
-  pk.full = 0;  // the batch runs the mixed walk only and no candidate search
+  QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NMID, 0, sizeof(int), c->stream));
+  k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rs9,
+                                                      t.ctl + CTL_NMID, MIDN, BIGN, 0);
   k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->stream>>>(
-      t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
+      t.rs9, t.ctl + CTL_NMID, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
       t.circ, t.C, t.first);
   k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.level,
                                                          t.start, t.count, t.ord, t.cap_pts, c->x,
                                                          c->gi, t.cent, t.circ, t.C, t.first);
-  k_forest_root_cent<<<std::min(f.nroots, 2 * c->sm_count), 512, 2 * RC * 3 * sizeof(double),
-                       c->stream>>>(f.nroots, f.roots, f.fact, c->x, t.ctl, t.cent);
+  QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
+  QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
+  PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
+  pk.full = 0;  // the batch runs the mixed walk only and no candidate search
   k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent);
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 8);
+  QV_COUNT(c, 10);
   return QV_OK;
 }
