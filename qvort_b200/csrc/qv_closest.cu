@@ -346,12 +346,10 @@ int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_gri
     int nwarps = (n_grid + TPW - 1) / TPW;
     int cap = 7 * (c->tree.depth + 1) + 8;
     size_t smem = sizeof(CStkEnt) * cap * CW;
-    if (smem > 48 * 1024) {
-      static size_t opted = 0;
-      if (smem > opted) {
-        cudaFuncSetAttribute(k_closest_tree, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        opted = smem;
-      }
+    if (smem > 48 * 1024 && smem > c->smem_search) {  // per context: attributes are per device
+      QV_CUDA(c, cudaFuncSetAttribute(k_closest_tree, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+      c->smem_search = smem;
     }
     const TreeBuf &t = c->tree;
     k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, smem, c->stream>>>(

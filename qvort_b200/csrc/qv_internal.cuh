@@ -157,6 +157,7 @@ struct qv_ctx {
   TreeBuf tree;
   int sm_count = 148;
   int build_grid = 0;  // co-resident blocks of the cooperative tree build
+  size_t smem_walk = 0, smem_search = 0;  // dynamic shared memory opted in on this device
   // instrumentation
   bool profile = false;
   cudaEvent_t ev_beg[PH_N] = {}, ev_end[PH_N] = {};

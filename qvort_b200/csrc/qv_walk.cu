@@ -411,13 +411,12 @@ int qv_launch_walk(qv_ctx *c) {
   int nb = (int)std::min<long>((items + WW - 1) / WW, 64L * c->sm_count);
   bool mixed = c->p.precision == QV_PREC_MIXED;
   if (mixed && smem > 48 * 1024) {
-    static size_t opted = 0;
-    if (smem > opted) {
+    if (smem > c->smem_walk) {  // per context: attributes are per device
       cudaFuncSetAttribute(k_walk32<QV_BC_OPEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(k_walk32<QV_BC_PERIODIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(k_walk32<QV_BC_OPENX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       cudaFuncSetAttribute(k_walk32<QV_BC_OPENXY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      opted = smem;
+      c->smem_walk = smem;
     }
   }
   switch (c->p.boundary) {
