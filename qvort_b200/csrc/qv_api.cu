@@ -534,11 +534,13 @@ static int velocity_collect(qv_ctx *c, long long *eval_count) {
     ev = c->n_act;
   }
   if (eval_count) *eval_count = ev;
-  if (st & 1)
+  if (st & QV_STAT_SINGULAR)
     return qv_fail(c, QV_ERR_SINGULAR, "singularity in BS (tree) velocity field - this is normally "
                    "caused by having recon_shots too large");
-  if (st & 2) return qv_fail(c, QV_ERR_TREE_DEPTH, "walk or search stack overflow");
-  if (st & 4) return qv_fail(c, QV_ERR_STATE, "line operation: too many re-tests pending");
+  if (st & QV_STAT_STACK) return qv_fail(c, QV_ERR_TREE_DEPTH, "walk or search stack overflow");
+  if (st & QV_STAT_STAGE)
+    return qv_fail(c, QV_ERR_CUDA, "direct sum: a source-tile copy did not complete");
+  if (st & QV_STAT_HEAP) return qv_fail(c, QV_ERR_STATE, "line operation: too many re-tests pending");
   return QV_OK;
 }
 
@@ -610,7 +612,7 @@ extern "C" int qv_closest(qv_ctx *c, int *closest, double *closestd) {
   int st = 0;
   QV_CUDA(c, cudaMemcpyAsync(&st, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (st & 2) return qv_fail(c, QV_ERR_TREE_DEPTH, "closest-search stack overflow");
+  if (st & QV_STAT_STACK) return qv_fail(c, QV_ERR_TREE_DEPTH, "closest-search stack overflow");
   return QV_OK;
 }
 
@@ -903,8 +905,10 @@ extern "C" int qv_steps(qv_ctx *c, int itime0, int nsteps) {
   cudaGraphExecDestroy(g_search);
   if (g_plain) cudaGraphExecDestroy(g_plain);
   c->ghosts_valid = false;
-  if (st & 1)
+  if (st & QV_STAT_SINGULAR)
     return qv_fail(c, QV_ERR_SINGULAR, "singularity in BS velocity field during qv_steps");
+  if (st & QV_STAT_STAGE)
+    return qv_fail(c, QV_ERR_CUDA, "direct sum: a source-tile copy did not complete");
   return QV_OK;
 }
 

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int 
       closestd[i] = cd;  // 100 for empty slots too (src/tree.f90:225)
       if (live) closest[i] = cl;
     }
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, 2);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, QV_STAT_STACK);
   }
 }
 

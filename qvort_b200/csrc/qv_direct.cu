@@ -241,15 +241,143 @@ __device__ __forceinline__ double shifted(double v, int a, double L) {
   return a == 0 ? v : (a > 0 ? v + L : v - L);
 }
 
+// ------------------------------------------------------------ TMA staging
+// A source tile is a contiguous run of the pack (64 bytes per source in both
+// packs), so one 1-D bulk copy of the TMA engine (cp.async.bulk, no
+// multicast) moves it into shared memory and signals an mbarrier with its
+// byte count.  Two buffers alternate: the copy of tile t+1 runs while tile t
+// is summed.  The pack base is a device allocation (256-byte aligned) and
+// every tile starts at a multiple of 64 bytes with a size that is a multiple
+// of 64 bytes, which the copy's 16-byte rules ask for.  Each wait is bounded
+// (QV_STAGE_WAIT_NS of wall time, and an iteration cap); a wait that runs out
+// sets QV_STAT_STAGE in the status word and the block stops summing, so a
+// copy that never lands ends the launch with an error, not a hang.
+#define QV_STAGE_WAIT_NS 1000000000ull  // 1 s
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+
+// make the initialised barriers visible to the copy engine before first use
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// one thread: arm the barrier for `bytes` and start the copy
+__device__ __forceinline__ void stage_copy(unsigned dst, const void *src, unsigned bytes,
+                                           unsigned bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ unsigned long long wall_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait for the barrier's phase of parity `parity` to complete, giving up
+// after QV_STAGE_WAIT_NS or 2^30 polls
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = wall_ns();
+  for (unsigned it = 0; it < (1u << 30); it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (wall_ns() - t0 > QV_STAGE_WAIT_NS) break;
+  }
+  return false;
+}
+
+// Double-buffered tile pipeline over sources [j0, j1) of a pack with 64-byte
+// rows.  begin() starts tile 0; acquire(t) starts tile t+1 and waits for tile
+// t (every thread of the block calls it; the result is block-uniform);
+// release() ends the use of the current tile; abort(t) drains the copies a
+// failed acquire(t) may have left in flight and reports the failure.
+struct TilePipe {
+  const unsigned char *src;  // pack base
+  int j0, j1, ntile;
+  // shared-memory addresses: stage k's buffer at buf + k * DTILE * 64, its
+  // barrier at bar + 8 k
+  unsigned buf, bar;
+
+  __device__ __forceinline__ unsigned bar_of(int t) const { return bar + 8u * (t & 1); }
+  __device__ __forceinline__ unsigned parity_of(int t) const { return (unsigned)(t >> 1) & 1u; }
+  __device__ __forceinline__ void start(int t) const {
+    const int t0 = j0 + t * DTILE, m = min(DTILE, j1 - t0);
+    stage_copy(buf + (unsigned)(DTILE * 64) * (t & 1), src + (size_t)t0 * 64, (unsigned)m * 64u,
+               bar_of(t));
+  }
+  __device__ __forceinline__ void begin() const {
+    if (threadIdx.x == 0) {
+      mbar_init(bar);
+      mbar_init(bar + 8u);
+      mbar_init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && ntile > 0) start(0);
+  }
+  __device__ __forceinline__ bool acquire(int t) const {
+    // buffer (t+1)&1 was last read in iteration t-1, which release() closed
+    if (threadIdx.x == 0 && t + 1 < ntile) start(t + 1);
+    const bool got = mbar_wait(bar_of(t), parity_of(t));
+    return __syncthreads_and(got) != 0;
+  }
+  __device__ __forceinline__ void release() const { __syncthreads(); }
+  // kept out of line: inlined, its waits made the FP64 kernels spill
+  __device__ __noinline__ void abort(int t, int *status) const {
+    if (threadIdx.x == 0) {
+      mbar_wait(bar_of(t), parity_of(t));
+      if (t + 1 < ntile) mbar_wait(bar_of(t + 1), parity_of(t + 1));
+      if (status) atomicOr(status, QV_STAT_STAGE);
+    }
+  }
+};
+
+// stages: 2 * DTILE * 64 contiguous bytes of shared memory; bars: 2 barriers
+__device__ __forceinline__ TilePipe make_pipe(const void *src, int j0, int j1, const void *stages,
+                                              const unsigned long long *bars) {
+  TilePipe p;
+  p.src = static_cast<const unsigned char *>(src);
+  p.j0 = j0;
+  p.j1 = j1;
+  p.ntile = j1 > j0 ? (j1 - j0 + DTILE - 1) / DTILE : 0;
+  p.buf = smem_u32(stages);
+  p.bar = smem_u32(bars);
+  return p;
+}
+
 // ------------------------------------------------------------ FP64 kernel
 template <int BC>
 __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restrict__ act,
                                                     const double *__restrict__ x,
                                                     const int *__restrict__ beh,
                                                     const double *__restrict__ src, int chunk_len,
-                                                    double L, double *part) {
+                                                    double L, double *part, int *status) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
-  __shared__ double tile[DTILE * 8];
+  __shared__ __align__(128) double tiles[2][DTILE * 8];
+  __shared__ __align__(8) unsigned long long bars[2];
   int q = blockIdx.x * DTILE + threadIdx.x;
   bool live = q < na;
   int i = live ? act[q] : 0;
@@ -257,11 +385,15 @@ __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restric
   int bi = live ? beh[i] : -1, ii = i + 1;
   double a0x = 0., a0y = 0., a0z = 0., a1x = 0., a1y = 0., a1z = 0.;
   int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
-  for (int t0 = j0; t0 < j1; t0 += DTILE) {
-    int m = min(DTILE, j1 - t0);
-    __syncthreads();
-    for (int k = threadIdx.x; k < m * 8; k += DTILE) tile[k] = src[8 * t0 + k];
-    __syncthreads();
+  const TilePipe pipe = make_pipe(src, j0, j1, tiles, bars);
+  pipe.begin();
+  for (int t = 0; t < pipe.ntile; t++) {
+    if (!pipe.acquire(t)) {
+      pipe.abort(t, status);
+      return;
+    }
+    const int m = min(DTILE, j1 - (j0 + t * DTILE));
+    const double *tile = tiles[t & 1];
     for (int k = 0; k < m; k++) {
       const double *s = tile + 8 * k;
       int jj = (int)s[7];
@@ -277,6 +409,7 @@ __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restric
         }
       }
     }
+    pipe.release();
   }
   if (live) {
     double *o = part + ((size_t)blockIdx.y * na + q) * 6;
@@ -322,9 +455,10 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
                                                     const double *__restrict__ x,
                                                     const int *__restrict__ beh,
                                                     const float *__restrict__ src, int chunk_len,
-                                                    double L, double *part) {
+                                                    double L, double *part, int *status) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
-  __shared__ float4 tile[DTILE * 4];
+  __shared__ __align__(128) float4 tiles[2][DTILE * 4];
+  __shared__ __align__(8) unsigned long long bars[2];
   int q = blockIdx.x * DTILE + threadIdx.x;
   bool live = q < na;
   int i = live ? act[q] : 0;
@@ -334,12 +468,15 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
   k0.zero();
   k1.zero();
   int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
-  const float4 *src4 = reinterpret_cast<const float4 *>(src);
-  for (int t0 = j0; t0 < j1; t0 += DTILE) {
-    int m = min(DTILE, j1 - t0);
-    __syncthreads();
-    for (int k = threadIdx.x; k < m * 4; k += DTILE) tile[k] = src4[4 * t0 + k];
-    __syncthreads();
+  const TilePipe pipe = make_pipe(src, j0, j1, tiles, bars);
+  pipe.begin();
+  for (int t = 0; t < pipe.ntile; t++) {
+    if (!pipe.acquire(t)) {
+      pipe.abort(t, status);
+      return;
+    }
+    const int m = min(DTILE, j1 - (j0 + t * DTILE));
+    const float4 *tile = tiles[t & 1];
     seg_tile(tile, m, xi, 0, 0, 0, L, bi, ii, k0);
 #pragma unroll 1
     for (int im = 0; im < NIMG; im++) {
@@ -347,6 +484,7 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
       qv_img_shift(BC, im, &ma, &mb, &mc);
       seg_tile(tile, m, xi, ma, mb, mc, L, bi, -7, k1);
     }
+    pipe.release();
   }
   if (live) {
     double *o = part + ((size_t)blockIdx.y * na + q) * 6;
@@ -412,10 +550,10 @@ int qv_launch_direct(qv_ctx *c) {
   case BCV:                                                                                   \
     if (mixed)                                                                                \
       k_direct32<BCV><<<grid, DTILE, 0, c->stream>>>(na, c->act, c->x, c->behind, c->src32,  \
-                                                     chunk_len, L, part);                     \
+                                                     chunk_len, L, part, c->dstatus);         \
     else                                                                                      \
       k_direct64<BCV><<<grid, DTILE, 0, c->stream>>>(na, c->act, c->x, c->behind, c->src64,  \
-                                                     chunk_len, L, part);                     \
+                                                     chunk_len, L, part, c->dstatus);         \
     break;
     QV_DIRECT_CASE(QV_BC_OPEN)
     QV_DIRECT_CASE(QV_BC_PERIODIC)
@@ -436,9 +574,10 @@ int qv_launch_direct(qv_ctx *c) {
 
 // ------------------------------------------------------ caller-owned scratch
 // The same direct sum with every temporary placed in memory the caller
-// provides (no allocation): act (n ints), blk (n/256+2 ints), src64 (8n
-// doubles), src32 (16n floats), part (max_chunks * 6n doubles).  Writes only
-// u_bs (the non-local velocity, f(:)%u_s_BS of src/timestep.f90:229-240).
+// provides (no allocation): act (n ints), blk (n/256+3 ints: block counts,
+// the active count, a status word), src64 (8n doubles), src32 (16n floats),
+// part (max_chunks * 6n doubles).  Writes only u_bs (the non-local velocity,
+// f(:)%u_s_BS of src/timestep.f90:229-240) and returns after the sum is done.
 __global__ void k_direct_reduce_bs(int na, int nchunk, const int *__restrict__ act,
                                    const double *__restrict__ part, double scale, double *u_bs) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -467,6 +606,8 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
   if (na == 0) return QV_OK;
   int tb = nblk(na, 256);
   bool mixed = p->precision == QV_PREC_MIXED;
+  int *stat = blk + nb + 1;
+  if (cudaMemsetAsync(stat, 0, sizeof(int), s) != cudaSuccess) return QV_ERR_CUDA;
   k_pack_sources<<<tb, 256, 0, s>>>(na, act, x, gi, src64, src32);
   int bx = nblk(na, DTILE);
   int want = (4 * sm_count + bx - 1) / bx;
@@ -480,9 +621,11 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
 #define QV_DIRECT_SCRATCH_CASE(BCV)                                                      \
   case BCV:                                                                              \
     if (mixed)                                                                           \
-      k_direct32<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src32, chunk_len, L, part); \
+      k_direct32<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src32, chunk_len, L, part,  \
+                                             stat);                                      \
     else                                                                                 \
-      k_direct64<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src64, chunk_len, L, part); \
+      k_direct64<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src64, chunk_len, L, part,  \
+                                             stat);                                      \
     break;
     QV_DIRECT_SCRATCH_CASE(QV_BC_OPEN)
     QV_DIRECT_SCRATCH_CASE(QV_BC_PERIODIC)
@@ -494,5 +637,10 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
   }
   double scale = mixed ? p->quant_circ / (4. * QV_PI) : p->quant_circ / (2. * QV_PI);
   k_direct_reduce_bs<<<tb, 256, 0, s>>>(na, nchunk, act, part, scale, u_bs);
-  return cudaGetLastError() == cudaSuccess ? QV_OK : QV_ERR_CUDA;
+  if (cudaGetLastError() != cudaSuccess) return QV_ERR_CUDA;
+  int st = 0;
+  if (cudaMemcpyAsync(&st, stat, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return QV_ERR_CUDA;
+  return st ? QV_ERR_CUDA : QV_OK;
 }

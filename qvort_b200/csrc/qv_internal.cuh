@@ -16,6 +16,12 @@
 #define QV_PI 3.14159265358979324  // src/cdata.f90:176
 #define QV_DEPS 2.220446049250313e-16  // epsilon(0.) under -fdefault-real-8
 
+// Bits of the device status word (qv_ctx::dstatus)
+#define QV_STAT_SINGULAR 1  // a tree leaf closer than epsilon (src/tree.f90:372-376)
+#define QV_STAT_STACK 2     // walk or search stack overflow
+#define QV_STAT_HEAP 4      // a line scan's re-test heap overflowed
+#define QV_STAT_STAGE 8     // a direct-sum source-tile copy did not land in time
+
 // Walk-ready node header, FP64 (64 B).  cent, width and the geometric offset
 // geo = |cent - cell centre| (src/tree.f90:355-357) in FP64 so that every
 // opening decision is taken exactly as the reference takes it.

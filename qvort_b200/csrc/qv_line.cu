@@ -75,7 +75,7 @@ struct LineArgs {
   const int *cand, *empt;
   int *flag_a, *flag_b;
   LineState *st;
-  int *dstatus;  // the context's status word (bit 4: a scan's re-test heap overflowed)
+  int *dstatus;  // the context's status word (QV_STAT_HEAP: a scan's re-test heap overflowed)
 };
 
 // clear_particle, src/general.f90:11-22 (u3 is kept)
@@ -132,7 +132,7 @@ __global__ void k_rem_flags(int n, LineArgs a) {
 __device__ void heap_push(LineState *s, int *dstatus, int v) {
   if (s->heap_n >= LHEAP) {
     s->status = 2;
-    atomicOr(dstatus, 4);
+    atomicOr(dstatus, QV_STAT_HEAP);
     return;
   }
   int k = s->heap_n++;

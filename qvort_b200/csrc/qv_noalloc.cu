@@ -31,7 +31,7 @@ constexpr int kMaxChunks = 8;
 constexpr size_t kOffGi = 0;
 constexpr size_t kOffAct = kOffGi + up(sizeof(double) * 3 * kMaxN);
 constexpr size_t kOffBlk = kOffAct + up(sizeof(int) * kMaxN);
-constexpr size_t kOffSrc64 = kOffBlk + up(sizeof(int) * (kMaxN / 256 + 2));
+constexpr size_t kOffSrc64 = kOffBlk + up(sizeof(int) * (kMaxN / 256 + 3));
 constexpr size_t kOffSrc32 = kOffSrc64 + up(sizeof(double) * 8 * kMaxN);
 constexpr size_t kOffPart = kOffSrc32 + up(sizeof(float) * 16 * kMaxN);
 constexpr size_t kBytes = kOffPart + up(sizeof(double) * 6 * (size_t)kMaxChunks * kMaxN);

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
     }
     if (lane == 0 && ev) atomicAdd(a.evals, ev);
     if (lane == 0 && evf) atomicAdd(a.evals_far, evf);
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, 1);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, QV_STAT_SINGULAR);
   }
 }
 
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 block
     }
     if (lane == 0 && ev) atomicAdd(a.evals, (unsigned long long)ev);
     if (lane == 0 && evf) atomicAdd(a.evals_far, (unsigned long long)evf);
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, 1);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, QV_STAT_SINGULAR);
   }
 }
 
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(GW * 32) k_walk_general(int m, const double *_
     if (live) { u[3 * q] = acc[0]; u[3 * q + 1] = acc[1]; u[3 * q + 2] = acc[2]; }
     for (int o = 16; o > 0; o >>= 1) ev += __shfl_down_sync(0xffffffffu, ev, o);
     if (lane == 0 && ev) atomicAdd(evals, ev);
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, 2);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, QV_STAT_STACK);
   }
 }
 
