@@ -51,9 +51,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--suite", default="tangle",
-                    choices=["tangle", "batch", "gradient", "large", "ring"],
-                    help="tangle: the headline line; batch / gradient / large: only that "
-                         "workload's entry")
+                    choices=["tangle", "batch", "gradient", "large", "ring", "direct"],
+                    help="tangle: the headline line; batch / gradient / large / ring / "
+                         "direct: only that workload's entry")
     ap.add_argument("--quick", action="store_true",
                     help="headline timing only (no comparators, e2e or CPU baseline)")
     return ap.parse_args()
@@ -572,6 +572,40 @@ def large_rate(L, torch, steps: int = 5, warmup: int = 3) -> dict:
     return out
 
 
+def direct_rate(L, torch, steps: int = 3, warmup: int = 1) -> dict:
+    """The direct Biot-Savart sum (velocity BS, every segment against every
+    target in all 27 images) on the tangle's initial state, FP64 and mixed:
+    CUDA-event time of one velocity evaluation (LIA, compaction, source pack,
+    direct kernel, reduction) and the mixed form's error against the FP64 one."""
+    from qvort_b200 import workloads as W
+
+    w = W.tangle(0)
+    out, vel = {}, {}
+    for prec in ("fp64", "mixed"):
+        c = L.Context(L.default_params(**dict(w.params, precision=prec, velocity="BS",
+                                              tree_theta=0.0)))
+        c.set_points(w.x, w.infront, w.behind)
+        for _ in range(max(1, warmup)):
+            vel[prec] = c.velocity(False)[0]
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            c.velocity(False)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        n = w.n  # every slot of the initial tangle is active
+        out[prec] = {"ms_per_velocity": ms, "pairs_per_s": float(n) * n * 27 / (ms * 1e-3)}
+        c.close()
+    rms, mx = _rel(vel["mixed"], vel["fp64"])
+    out["error"] = {"mixed_vs_fp64_direct_rms_rel": rms, "mixed_vs_fp64_direct_max_rel": mx}
+    out["workload"] = (f"tangle N={w.n}, periodic L=0.1 (27 images), direct sum (theta 0); "
+                       "CUDA events around qv_velocity calls")
+    return out
+
+
 def batch_rate(L, torch, steps: int = 20) -> dict:
     """512 independent open systems (rings and leap-frogging pairs, N log-uniform
     in [100, 8000], dt from {5e-8, 1e-7, 2e-7}, direct below 2000 points,
@@ -643,6 +677,8 @@ def main():
             r = large_rate(L, torch, args.steps, args.warmup)
         elif args.suite == "ring":
             r = ring_rate(L, torch)
+        elif args.suite == "direct":
+            r = direct_rate(L, torch, args.steps, args.warmup)
         else:
             r = gradient_rate(L, torch)
         print(json.dumps({"suite": args.suite, **r}), flush=True)
