@@ -24,7 +24,8 @@ extern "C" {
 
 #define QV_OK 0
 #define QV_ERR_ARG (-1)        /* bad argument or size */
-#define QV_ERR_CUDA (-2)       /* a CUDA call failed; see qv_last_error */
+#define QV_ERR_CUDA (-2)       /* a CUDA call failed, or a device-side copy did not complete
+                                  within its bounded wait; see qv_last_error */
 #define QV_ERR_SINGULAR (-3)   /* tree singularity (src/tree.f90:372-376) */
 #define QV_ERR_TREE_DEPTH (-4) /* octree deeper than QV_MAX_DEPTH (coincident points) */
 #define QV_ERR_STATE (-5)      /* call out of order (no points, no tree, ...) */
