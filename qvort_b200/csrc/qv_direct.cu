@@ -243,8 +243,8 @@ __device__ __forceinline__ double shifted(double v, int a, double L) {
 
 // ------------------------------------------------------------ TMA staging
 // A source tile is a contiguous run of the pack (64 bytes per source in both
-// packs), so one 1-D bulk copy of the TMA engine (cp.async.bulk, no
-// multicast) moves it into shared memory and signals an mbarrier with its
+// packs), so one 1-D bulk copy of the TMA engine (cp.async.bulk into this
+// block's own shared memory) moves it there and signals an mbarrier with its
 // byte count.  Two buffers alternate: the copy of tile t+1 runs while tile t
 // is summed.  The pack base is a device allocation (256-byte aligned) and
 // every tile starts at a multiple of 64 bytes with a size that is a multiple
