@@ -268,6 +268,87 @@ def precon(p: QoParams, n: int, st) -> int:
     return lib().qo_precon(C.byref(p), n, C.byref(_qostate(st)))
 
 
+class Loop:
+    """The reference's whole time-loop body (src/run.f90:41-93) on the oracle's
+    copy of f(:), with the line operations:
+
+      ghostp; construct_tree; pmotion; pinsert; every recon_shots steps
+      pclose_tree on the tree built before the move (pclose when
+      tree_theta = 0), precon_original, premove; ghostp; enforce_periodic.
+
+    line_ops: 0 = none, 1 = pinsert and premove, 2 = also precon (the
+    reference's default loop, switch_off_recon F).  Arrays hold `cap` slots;
+    `n` is pcount.  Points inserted this step are searched as targets but
+    cannot be found as partners (the tree predates them), as in the reference.
+    """
+
+    def __init__(self, p: QoParams, x, inf, beh, cap: int | None = None, line_ops: int = 2,
+                 recon_shots: int = 1, nthreads: int = 1):
+        x = _f(x)
+        self.p = p
+        self.n = x.shape[0]
+        self.cap = cap or 2 * self.n + 64
+        self.st = line_state(self.n, self.cap, x=x, infront=_i(inf), behind=_i(beh))
+        self.line_ops = line_ops
+        self.recon_shots = recon_shots
+        self.nthreads = nthreads
+        self.evals = 0
+        self.counts = {}
+
+    def _ghosts(self):
+        n, s = self.n, self.st
+        g = ghosts(self.p, s["x"][:n], s["infront"][:n], s["behind"][:n])
+        for k, a in zip(("gi", "gb", "gii", "gbb"), g):
+            s[k][:n] = a
+
+    def step(self, itime: int) -> int:
+        p, s = self.p, self.st
+        n = self.n
+        self._ghosts()                                            # run.f90:41
+        tree = None
+        if p.tree_theta > 0:                                      # run.f90:43
+            tree = Tree(p, s["x"][:n], s["gi"][:n], s["infront"][:n])
+            if tree.status:
+                return -2
+        g = [s[k][:n] for k in ("gi", "gb", "gii", "gbb")]       # run.f90:50 pmotion
+        u, uli, ubs, ev, st = velocity(p, s["x"][:n], s["infront"][:n], s["behind"][:n], g, tree,
+                                       nthreads=self.nthreads)
+        if st:
+            return st
+        self.evals = ev
+        act = s["infront"][:n] != 0
+        s["u"][:n][act], s["u_li"][:n][act], s["u_bs"][:n][act] = u[act], uli[act], ubs[act]
+        xn, h1, h2, h3 = pmotion_ab(p.dt, s["x"][:n], s["u"][:n], s["u1"][:n], s["u2"][:n],
+                                    s["u3"][:n], s["infront"][:n])
+        s["x"][:n], s["u1"][:n], s["u2"][:n], s["u3"][:n] = xn, h1, h2, h3
+        self.counts = {"inserted": 0, "reconnected": 0, "removed": 0}
+        if self.line_ops:                                         # run.f90:61
+            self.n, self.counts["inserted"] = pinsert(p, self.n, s)
+            n = self.n
+        if itime % self.recon_shots == 0:                         # run.f90:63-72
+            if tree is not None:
+                cl, cd = pclose_tree(tree, s["x"][:n], s["infront"][:n], s["behind"][:n],
+                                     s["closest"][:n], self.nthreads)
+            else:
+                cl, cd = pclose(s["x"][:n], s["infront"][:n], s["behind"][:n], s["closest"][:n],
+                                s["closestd"][:n])
+            s["closest"][:n], s["closestd"][:n] = cl, cd
+            if self.line_ops == 2:
+                self.counts["reconnected"] = precon(p, n, s)
+            if self.line_ops:
+                self.counts["removed"] = premove(p, n, s)
+        if tree is not None:
+            tree.close()
+        self._ghosts()                                            # run.f90:75
+        if p.boundary in (1, 2, 3):                               # run.f90:82-93
+            lib().qo_enforce_periodic(C.byref(p), n, _p(s["x"]), _p(s["infront"]))
+        return 0
+
+    def state(self) -> dict:
+        n = self.n
+        return {k: v[:n].copy() for k, v in self.st.items()}
+
+
 def field_velocity_tree(p: QoParams, tree, pts):
     """tree_walk_general at the points (the Tree arm of mesh_velocity)."""
     pts = _f(pts).reshape(-1, 3)

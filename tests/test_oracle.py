@@ -358,3 +358,37 @@ def test_tree_walk_general_at_tiny_theta_is_the_segment_sum():
         c = a * b * (a * b + (r1 * r2).sum(1))
         ref = (((a + b) / c)[:, None] * np.cross(r1, r2)).sum(0) / (4 * np.pi)
         assert np.abs(u[q] - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def test_loop_without_line_ops_is_the_plain_step():
+    """oracle.Loop with line_ops 0 runs the same body as State.step (ghosts,
+    tree, velocity, AB, search, ghosts, wrap): identical states, bit for bit."""
+    w = W.random_rings(6, 0.006, 0.01, 5e-4, 0.1, seed=5, theta=0.4)
+    p = O.params(**w.params)
+    lp = O.Loop(p, w.x, w.infront, w.behind, line_ops=0)
+    st = O.State(p, w.x, w.infront, w.behind)
+    for it in range(1, 4):
+        assert lp.step(it) == 0 and st.step() == 0
+        s = lp.state()
+        for k in ("x", "u", "u1", "u2", "u3", "closest", "closestd"):
+            np.testing.assert_array_equal(s[k], getattr(st, k), err_msg=k)
+
+
+def test_loop_with_line_ops_keeps_links_consistent():
+    """The default loop (pinsert, pclose_tree, precon, premove) on a tangle whose
+    rings touch: every step reconnects or removes somewhere, and afterwards every
+    active slot's neighbours point back at it and empty slots carry no links."""
+    w = W.random_rings(40, 0.004, 0.012, 5e-4, 0.1, seed=3, theta=0.4, centre_box=0.03)
+    p = O.params(**w.params)
+    lp = O.Loop(p, w.x, w.infront, w.behind, line_ops=2)
+    done = 0
+    for it in range(1, 4):
+        assert lp.step(it) == 0
+        done += lp.counts["reconnected"] + lp.counts["removed"] + lp.counts["inserted"]
+        s = lp.state()
+        inf, beh = s["infront"], s["behind"]
+        act = np.flatnonzero(inf)
+        np.testing.assert_array_equal(beh[inf[act] - 1], act + 1)
+        np.testing.assert_array_equal(inf[beh[act] - 1], act + 1)
+        assert (beh[inf == 0] == 0).all()
+    assert done > 0
