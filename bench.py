@@ -1,13 +1,16 @@
 #!/usr/bin/env python
 """Benchmark of the velocity-and-timestep path on B200.
 
-Workload (one "step"): the loop body of src/run.f90:41-107 restricted to the
-path -- ghost gather, octree build, Biot-Savart velocity (LIA + Barnes-Hut
-walk with 26 periodic images, FP32 pair terms with FP64 recentring and
-compensated sums), Adams-Bashforth update, reconnection candidate search,
-periodic wrap -- on the random-ring tangle: 100 rings, R ~ U(0.008, 0.02) cm,
-delta 5e-4 cm (N ~ 24.7k points), periodic box 0.1 cm, theta 0.4, dt 1e-7 s.
-Inputs are seeded synthetic rings (no dataset).
+Workload (one "step"): the reference's time-loop body (src/run.f90:41-93)
+with its default options -- ghost gather, octree build, Biot-Savart velocity
+(LIA + Barnes-Hut walk with 26 periodic images; FP32 pair terms with FP64
+recentring and compensated sums), Adams-Bashforth update, pinsert, the
+reconnection candidate search on the tree built before the move, precon
+(original), premove, ghost gather and periodic wrap -- on the large isotropic
+tangle: 3000 rings, R ~ U(0.004, 0.015) cm, delta 3e-4 cm (N = 802,906
+points), periodic box 0.1 cm, theta 0.5, dt 1e-7 s.  This is the largest
+configuration of the path that runs on one GPU.  Inputs are seeded synthetic
+rings (no dataset).
 
 Metric: direct-equivalent Biot-Savart pair interactions per second,
 N * N_active * 27 per step / step time (the unit the O(N^2) direct form would
@@ -15,6 +18,7 @@ have to evaluate), whole job over all ranks.  Every rank runs an independent
 replica (the path does not shard; "replicas only").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--suite large|tangle|batch|gradient|ring|direct] [--quick]
 
 Under torchrun each rank drives cuda:LOCAL_RANK; the timed region is bracketed
 by a barrier and a synchronize, and the max over ranks is reported.
@@ -27,7 +31,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from pathlib import Path
 
@@ -50,10 +53,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--suite", default="tangle",
-                    choices=["tangle", "batch", "gradient", "large", "ring", "direct"],
-                    help="tangle: the headline line; batch / gradient / large / ring / "
-                         "direct: only that workload's entry")
+    ap.add_argument("--suite", default="large",
+                    choices=["large", "tangle", "batch", "gradient", "ring", "direct"],
+                    help="large: the headline line; the others print only that workload's "
+                         "entry")
     ap.add_argument("--quick", action="store_true",
                     help="headline timing only (no comparators, e2e or CPU baseline)")
     return ap.parse_args()
@@ -147,15 +150,30 @@ def job_value(units_per_step: float, ms_per_step: float, ws: int) -> float:
 def workload(seed: int):
     from qvort_b200 import workloads as W
 
-    return W.tangle(seed)
+    return W.large_tangle(seed)
+
+
+def workload_config(w, ws: int = 1) -> dict:
+    """The `config` object of the JSON line, identical in both arms."""
+    return {
+        "workload": (f"large tangle: 3000 rings R~U(0.004,0.015) cm, delta 3e-4 cm, "
+                     f"N={w.n}, periodic L=0.1 cm (26 images), Barnes-Hut theta 0.5, AB ladder, "
+                     f"dt 1e-7 s, default loop (pinsert, pclose_tree, precon, premove "
+                     f"every step)"),
+        "n_points": w.n,
+        "l2": "inputs (tree packs ~0.2 GB) larger than L2, and L2 flushed between timed steps",
+        "parallelism": f"replicas x{ws} (the path does not shard)",
+    }
 
 
 # ----------------------------------------------------------------------- CPU
 def cpu_step_rate(w, seconds_budget: float = 12.0, nthreads: int | None = None):
-    """Oracle (the C restatement, OpenMP over targets) on the host cores: time
-    the path's step on a bounded sample -- full ghost gather, tree build, AB
-    update and wrap; velocity and candidate search on a strided subset of
-    targets, scaled to all targets.  Returns (step seconds, sample text, cores)."""
+    """Oracle (the C restatement, OpenMP over targets) on the host cores: one
+    step of the same loop on a bounded sample -- ghost gathers, tree build, AB
+    update, candidate search and the sequential line operations (pinsert,
+    precon, premove) on every point; the velocity on an evenly strided subset
+    of targets sized to `seconds_budget`, scaled to all targets.  Returns
+    (step seconds, sample text, threads used)."""
     from oracle import oracle as O
 
     nthreads = nthreads or os.cpu_count() or 1
@@ -183,21 +201,25 @@ def cpu_step_rate(w, seconds_budget: float = 12.0, nthreads: int | None = None):
     t0 = time.perf_counter()
     xn, *_ = O.pmotion_ab(p.dt, x, uf, *h, inf)
     t_ab = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    cl, cd = O.pclose_tree(tree, xn, inf, beh, np.zeros(w.n, np.int32), nthreads)
-    t_c = time.perf_counter() - t0
-    # line operations (sequential in the reference): pinsert, precon, premove
     st = O.line_state(w.n, 2 * w.n, x=xn, u=uf, infront=inf, behind=beh, gi=g[0], gb=g[1],
-                      gii=g[2], gbb=g[3], closest=cl, closestd=cd)
+                      gii=g[2], gbb=g[3])
     t0 = time.perf_counter()
     n2, _ = O.pinsert(p, w.n, st)
+    t_l = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cl, cd = O.pclose_tree(tree, st["x"][:n2], st["infront"][:n2], st["behind"][:n2],
+                           np.zeros(n2, np.int32), nthreads)
+    t_c = time.perf_counter() - t0
+    st["closest"][:n2], st["closestd"][:n2] = cl, cd
+    t0 = time.perf_counter()
     O.precon(p, n2, st)
     O.premove(p, n2, st)
-    t_l = time.perf_counter() - t0
+    t_l += time.perf_counter() - t0
+    tree.close()
     t_step = t_g * 2 + t_b + t_v + t_ab + t_c + t_l
-    sample = (f"1 step of the same workload: ghosts, tree build, AB, candidate search, "
-              f"pinsert/precon/premove on all {w.n} points; velocity on {m} evenly strided "
-              f"targets scaled by {w.n}/{m}")
+    sample = (f"1 step of the same loop: ghosts, tree build, AB, pinsert, candidate search, "
+              f"precon, premove on all {w.n} points; velocity on {m} evenly strided "
+              f"targets, scaled by {w.n}/{m}")
     return t_step, sample, nthreads
 
 
@@ -208,11 +230,12 @@ def reference_arm(args):
     w = workload(args.seed)
     pairs = float(w.n) * w.n * 27
     for _ in range(args.warmup):
-        cpu_step_rate(w, seconds_budget=1.0)
+        cpu_step_rate(w, seconds_budget=0.5)
     ts = []
     t_wall = time.perf_counter()
+    sample, cores = "", 0
     for _ in range(args.steps):
-        t, sample, cores = cpu_step_rate(w, seconds_budget=4.0)
+        t, sample, cores = cpu_step_rate(w, seconds_budget=1.5)
         ts.append(t)
     wall = time.perf_counter() - t_wall
     t = float(np.mean(ts))
@@ -222,9 +245,7 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded random rings)",
-        "config": {"workload": "tangle: 100 rings R~U(0.008,0.02) cm, delta 5e-4, N=%d, "
-                               "periodic L=0.1, Tree theta 0.4, AB, dt 1e-7" % w.n,
-                   "n_points": w.n},
+        "config": workload_config(w, args.gpus),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample,
                          "note": "no Fortran compiler on this image: the reference's own "
@@ -238,6 +259,26 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------------- GPU
+def time_steps(ctx, stream, torch, itime: int, steps: int, flush=None):
+    """CUDA-event time of `steps` calls of qv_step on `stream` (the context's
+    stream), L2 flushed before each outside the events; returns (ms per step,
+    next itime)."""
+    evs = []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            if flush is not None:
+                flush.fill_(k & 0xFF)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            itime += 1
+            ctx.step(itime)
+            e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs) / steps, itime
+
+
 def our_arm(args):
     import torch
 
@@ -272,46 +313,30 @@ def our_arm(args):
     if ws > 1:
         torch.distributed.barrier()
     launches0 = ctx.counters()["launches"]
-    evs = []
     torch.cuda.synchronize()
     t_wall0 = time.time()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(k & 0xFF)       # L2 flush between timed steps (outside the events)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            itime += 1
-            ctx.step(itime)
-            e1.record(stream)
-        evs.append((e0, e1))
-    torch.cuda.synchronize()
+    ms_local, itime = time_steps(ctx, stream, torch, itime, args.steps, flush)
     clk = clocks.stop(t_wall0, time.time())
     launches = ctx.counters()["launches"] - launches0
-    ms_total = job_time_ms(sum(a.elapsed_time(b) for a, b in evs), ws)
+    ms_step = job_time_ms(ms_local, ws)
     if ws > 1:
         torch.distributed.barrier()
-    ms_step = ms_total / args.steps
     value = job_value(pairs_step, ms_step, ws)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair terms, f64 recentring/LIA/AB",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair terms, f64 recentring/LIA/AB/tree/search",
         "data": "synthetic (seeded random rings)",
-        "config": {"workload": "tangle: 100 rings R~U(0.008,0.02) cm, delta 5e-4, N=%d, "
-                               "periodic L=0.1 (26 images), Tree theta 0.4, mixed precision, "
-                               "AB ladder, dt 1e-7, reconnections on" % n,
-                   "n_points": n, "n_points_end": ctx.n,
-                   "line_ops": "pinsert, candidate search, precon (original), premove each step",
-                   "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"replicas x{ws} (path does not shard)"},
+        "config": workload_config(w, ws),
+        "n_points_end": ctx.n,
         "steps_per_s": 1e3 / ms_step * ws,
         "clocks": clk,
         "gpu_launches": int(launches),
     }
     if not args.quick and rank == 0:
-        line.update(extras(ctx, w, stream, L, torch, itime))
+        line.update(extras(ctx, w, stream, L, torch, itime, flush))
     ctx.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -326,18 +351,14 @@ def _rel(a, b):
             float((np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-300)).max()))
 
 
-def extras(ctx, w, stream, L, torch, itime):
-    out = {}
-    n = w.n
-    pairs_step = float(n) * n * 27
-    sp = stream.cuda_stream
-
-    # ---- phase breakdown and the dominant kernel (the tree walk)
+def walk_roofline(ctx, L, stream, nprof: int = 3, traffic_file: str = "walk_large_traffic.json"):
+    """Phase times over nprof profiled steps and the roofline of the dominant
+    kernel, the mixed Barnes-Hut walk: algorithmic FLOPs counted on the device
+    (38 per leaf pair, 50 per far cell) over its CUDA-event time."""
+    itime = 10_000
     ctx.profile(True)
-    itime += 1
-    ctx.step(itime)          # first profiled step creates the events; not counted
+    ctx.step(itime)          # the first profiled step creates the events; not counted
     ctx.phase_times(reset=True)
-    nprof = 5
     for _ in range(nprof):
         itime += 1
         ctx.step(itime)
@@ -346,70 +367,69 @@ def extras(ctx, w, stream, L, torch, itime):
     cnt = ctx.counters()
     walk_ms = ph["nonlocal"] / nprof
     flops = cnt["leaf_evals"] * FLOP_LEAF + cnt["far_evals"] * FLOP_FAR
-    peak = L.probe_fp32(sp)
+    peak = L.probe_fp32(stream.cuda_stream)
     achieved = flops / (walk_ms * 1e-3) / 1e12
-    traffic = None
-    prof = ROOT / "profiles" / "walk_tangle_traffic.json"
+    traffic, traffic_src = None, None
+    prof = ROOT / "profiles" / traffic_file
     if prof.exists():
-        traffic = json.loads(prof.read_text()).get("bytes_per_launch")
-    out["phases_ms_per_step"] = {k: v / nprof for k, v in ph.items()}
-    out["roofline"] = {
+        d = json.loads(prof.read_text())
+        traffic, traffic_src = d.get("bytes_per_launch"), d.get("source")
+    roof = {
         "kernel": "k_walk32 (Barnes-Hut walk, mixed)", "bound": "fp32",
         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
         "traffic": traffic,
+        "traffic_source": traffic_src or "no capture committed",
         "peak_source": "measured FP32 FMA throughput on this GPU (qv_probe_fp32); "
                        "MEASURED_PEAKS.json has no FP32-pipe figure",
         "flop_model": f"{FLOP_LEAF:.0f} FLOP/leaf pair + {FLOP_FAR:.0f} FLOP/far cell "
                       "(algorithmic; theta tests, recentring and Kahan excluded)",
-        "leaf_evals": cnt["leaf_evals"], "far_evals": cnt["far_evals"],
-        "walk_ms": walk_ms,
+        "leaf_evals": cnt["leaf_evals"], "far_evals": cnt["far_evals"], "walk_ms": walk_ms,
     }
-    # the same kernel against HBM: its DRAM traffic (one ncu capture, per launch)
-    # over its time, against the measured copy bandwidth -- far from the bound
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     if traffic and peaks_file.exists():
         hbm = json.loads(peaks_file.read_text()).get("hbm_gbs")
         if hbm:
             gbs = traffic / (walk_ms * 1e-3) / 1e9
-            out["roofline"]["hbm"] = {"achieved": gbs, "peak": hbm, "unit": "GB/s",
-                                      "frac": gbs / hbm,
-                                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
-    out["evals_per_step"] = cnt["leaf_evals"] + cnt["far_evals"] + 2 * n
+            roof["hbm"] = {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
+    return {k: v / nprof for k, v in ph.items()}, roof
 
-    # ---- accuracy at the initial state: mixed BH vs FP64 BH vs FP64 direct
+
+def precision_pair(L, torch, w, stream, flush, steps: int = 3, warmup: int = 2):
+    """The same workload in FP64 (the reference's arithmetic, same Barnes-Hut
+    algorithm): CUDA-event step time, and the mixed velocity's error against the
+    FP64 velocity on every target of the initial state."""
+    sp = stream.cuda_stream
     vel = {}
-    for key, prm in (("bh_mixed", dict(precision="mixed")), ("bh_fp64", dict(precision="fp64")),
-                     ("direct_fp64", dict(precision="fp64", velocity="BS", tree_theta=0.0))):
-        pr = dict(w.params)
-        pr.update(prm)
-        c = L.Context(L.default_params(**pr), stream=sp)
+    out = {}
+    for prec in ("mixed", "fp64"):
+        c = L.Context(L.default_params(**dict(w.params, precision=prec, line_ops=2)), stream=sp)
         c.set_points(w.x, w.infront, w.behind)
-        vel[key] = c.velocity(False)[0]
-        if key == "direct_fp64":
-            # time the FP64 direct form: velocity + step
-            c.step(1)
+        vel[prec] = c.velocity(False)[0]
+        if prec == "fp64":
+            it = 0
+            for _ in range(warmup):
+                it += 1
+                c.step(it)
             torch.cuda.synchronize()
-            ts = []
-            for k in range(2):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                c.step(2 + k)
-                e1.record(stream)
-                e1.synchronize()
-                ts.append(e0.elapsed_time(e1))
-            ms = float(np.mean(ts))
-            out["fp64_direct"] = {"ms_per_step": ms, "pairs_per_s": pairs_step / (ms * 1e-3)}
+            ms, _ = time_steps(c, stream, torch, it, steps, flush)
+            out["fp64_bh"] = {"ms_per_step": ms, "pairs_per_s": float(w.n) * w.n * 27 / (ms * 1e-3),
+                              "steps": steps, "timing": "CUDA events, L2 flushed between steps"}
         c.close()
-    rms, mx = _rel(vel["bh_mixed"], vel["bh_fp64"])
-    rms_a, mx_a = _rel(vel["bh_fp64"], vel["direct_fp64"])
+    rms, mx = _rel(vel["mixed"], vel["fp64"])
     out["error"] = {"mixed_vs_fp64_bh_rms_rel": rms, "mixed_vs_fp64_bh_max_rel": mx,
-                    "bh_vs_fp64_direct_rms_rel": rms_a, "bh_vs_fp64_direct_max_rel": mx_a}
+                    "targets": w.n, "state": "initial"}
+    return out
 
-    # ---- end to end through the C ABI with pinned host buffers (the Fortran
-    # shim's per-step pattern: gather f(:) in, step, scatter f(:) out)
+
+def e2e_rate(L, torch, w, stream, steps: int = 10):
+    """The same step end to end through the C ABI with pinned host buffers
+    (the Fortran shim's per-step pattern: gather f(:) in, step, scatter f(:)
+    out in one qv_step_exchange call); wall clock around the calls."""
+    n = w.n
+    pairs_step = float(n) * n * 27
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
-    cap = 2 * n  # room for insertions (the host grows f(:) when pcount grows)
+    cap = n + n // 4  # room for insertions (the host grows f(:) when pcount grows)
     hx = pin((cap, 3), torch.float64); hx[:n] = w.x
     hinf = pin((cap,), torch.int32); hinf[:n] = w.infront
     hbeh = pin((cap,), torch.int32); hbeh[:n] = w.behind
@@ -419,10 +439,10 @@ def extras(ctx, w, stream, L, torch, itime):
     hcl = pin((cap,), torch.int32); hcl[:] = 0
     hu = pin((cap, 3), torch.float64)
     hcd = pin((cap,), torch.float64)
-    c = L.Context(L.default_params(**w.params, precision="mixed", line_ops=2), stream=sp)
+    c = L.Context(L.default_params(**w.params, precision="mixed", line_ops=2),
+                  stream=stream.cuda_stream)
     cur = [n]
     moved = [0, 0]
-
     inp = dict(x=hx, infront=hinf, behind=hbeh, u1=hist[0], u2=hist[1], u3=hist[2], closest=hcl)
     outp = dict(x=hx, u=hu, u1=hist[0], u2=hist[1], u3=hist[2], infront=hinf, behind=hbeh,
                 closest=hcl, closestd=hcd)
@@ -436,29 +456,42 @@ def extras(ctx, w, stream, L, torch, itime):
     for it in range(3):
         e2e_step(it + 1)
     torch.cuda.synchronize()
-    K = 10
     moved[0] = moved[1] = 0
     t0 = time.perf_counter()
-    for it in range(K):
+    for it in range(steps):
         e2e_step(it + 4)
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / K
+    ms = (time.perf_counter() - t0) * 1e3 / steps
     c.close()
-    out["e2e"] = {"value": pairs_step / (e2e_ms * 1e-3), "unit": UNIT,
-                  "h2d_bytes_per_step": moved[0] // K, "d2h_bytes_per_step": moved[1] // K,
-                  "ms_per_step": e2e_ms,
-                  "path": "qv_step_exchange (line_ops 2): pinned host in x, links, AB "
-                          "history, closest; out x, u, history, links, closest, closestd; "
-                          "wall clock"}
+    return {"value": pairs_step / (ms * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": moved[0] // steps, "d2h_bytes_per_step": moved[1] // steps,
+            "ms_per_step": ms,
+            "path": "qv_step_exchange (line_ops 2): pinned host in x, links, AB history, "
+                    "closest; out x, u, history, links, closest, closestd; wall clock"}
 
-    # ---- gradients/s on the differentiation workload: 16 trefoil rings,
-    # N = 50,000, periodic, K = 256 Adams-Bashforth steps checkpointed every 16,
-    # mixed Barnes-Hut forward (theta 0.4) and the FP64 adjoint backward
+
+def extras(ctx, w, stream, L, torch, itime, flush):
+    out = {}
+    n = w.n
+    pairs_step = float(n) * n * 27
+    # ---- phase breakdown and the dominant kernel (the tree walk)
+    ph, roof = walk_roofline(ctx, L, stream)
+    out["phases_ms_per_step"] = ph
+    out["roofline"] = roof
+    out["evals_per_step"] = roof["leaf_evals"] + roof["far_evals"] + 2 * n
+    # ---- mixed against FP64 on the same algorithm: time and error
+    pp = precision_pair(L, torch, w, stream, flush)
+    out["fp64_bh"] = pp["fp64_bh"]
+    out["error"] = pp["error"]
+    # ---- end to end through the C ABI with pinned host buffers
+    out["e2e"] = e2e_rate(L, torch, w, stream)
+    # ---- the random-ring tangle (N = 24.7k): mixed and FP64 Barnes-Hut steps,
+    # the FP64 direct form (the >= 5x comparison), errors
+    out["tangle"] = tangle_rate(L, torch, stream, flush)
+    # ---- gradients/s on the differentiation workload
     out["gradient"] = gradient_rate(L, torch)
-
     # ---- batched ensemble: 512 independent open systems in one graph per step
     out["batch"] = batch_rate(L, torch)
-
     # ---- CPU baseline (oracle port on this host's cores), bounded sample
     t, sample, cores = cpu_step_rate(w)
     out["cpu_baseline"] = {"value": pairs_step / t, "unit": UNIT, "cores": cores, "kind": "port",
@@ -466,12 +499,53 @@ def extras(ctx, w, stream, L, torch, itime):
     return out
 
 
+def tangle_rate(L, torch, stream, flush, steps: int = 10, warmup: int = 3) -> dict:
+    """The random-ring tangle: 100 rings, R ~ U(0.008, 0.02) cm, delta 5e-4 cm
+    (N = 24,707), periodic L = 0.1, theta 0.4, the default loop.  Mixed and FP64
+    Barnes-Hut steps and the FP64 direct form's step, CUDA events; errors of
+    the mixed velocity against FP64 Barnes-Hut and of FP64 Barnes-Hut against
+    the FP64 direct sum at the initial state."""
+    from qvort_b200 import workloads as W
+
+    w = W.tangle(0)
+    n = w.n
+    pairs_step = float(n) * n * 27
+    sp = stream.cuda_stream
+    out = {"workload": f"tangle: 100 rings R~U(0.008,0.02) cm, delta 5e-4 cm, N={n}, periodic "
+                       f"L=0.1, theta 0.4, default loop", "n_points": n}
+    vel = {}
+    for key, prm, k in (("mixed", dict(precision="mixed"), steps),
+                        ("fp64_bh", dict(precision="fp64"), steps),
+                        ("fp64_direct", dict(precision="fp64", velocity="BS", tree_theta=0.0), 2)):
+        pr = dict(w.params, line_ops=2)
+        pr.update(prm)
+        c = L.Context(L.default_params(**pr), stream=sp)
+        c.set_points(w.x, w.infront, w.behind)
+        vel[key] = c.velocity(False)[0]
+        it = 0
+        for _ in range(warmup if k > 2 else 1):
+            it += 1
+            c.step(it)
+        torch.cuda.synchronize()
+        ms, _ = time_steps(c, stream, torch, it, k, flush)
+        out[key] = {"ms_per_step": ms, "pairs_per_s": pairs_step / (ms * 1e-3)}
+        c.close()
+    out["mixed_speedup_vs_fp64_bh"] = out["fp64_bh"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed_speedup_vs_fp64_direct"] = (out["fp64_direct"]["ms_per_step"] /
+                                           out["mixed"]["ms_per_step"])
+    rms, mx = _rel(vel["mixed"], vel["fp64_bh"])
+    rms_a, mx_a = _rel(vel["fp64_bh"], vel["fp64_direct"])
+    out["error"] = {"mixed_vs_fp64_bh_rms_rel": rms, "mixed_vs_fp64_bh_max_rel": mx,
+                    "bh_vs_fp64_direct_rms_rel": rms_a, "bh_vs_fp64_direct_max_rel": mx_a}
+    return out
+
+
 def gradient_rate(L, torch, steps: int = 256, reps: int = 2) -> dict:
     from qvort_b200 import adjoint as A
     from qvort_b200 import workloads as W
 
-    w = W.trefoil_rings()
-    prm = dict(w.params, velocity="Tree", tree_theta=0.4, precision="mixed")
+    w = W.trefoil_rings(smooth=True)
+    prm = dict(w.params, velocity="Tree", tree_theta=0.4, precision="mixed", dt=1e-8)
     s = A.FilamentSystem(L.default_params(**prm), w.infront, w.behind)
     A.gradient(w.x, s, 16, 16)          # warm-up: buffers, tree capacity
     torch.cuda.synchronize()
@@ -482,9 +556,12 @@ def gradient_rate(L, torch, steps: int = 256, reps: int = 2) -> dict:
     sec = (time.perf_counter() - t0) / reps
     s.close()
     return {"value": 1.0 / sec, "unit": "gradients/s", "s_per_gradient": sec,
-            "workload": f"16 trefoil rings, N={w.n}, periodic L=0.1, K={steps} AB steps, "
-                        "checkpoint every 16, Tree theta 0.4 mixed forward, FP64 adjoint; "
-                        "loss = E(x_K) + sum |x_K - x_0|^2; wall clock"}
+            "workload": f"16 trefoil rings, N={w.n}, smooth seeded 1e-5 cm displacement, "
+                        f"periodic L=0.1, K={steps} AB steps at dt 1e-8 s (below the "
+                        f"timestep_check bound {W.dt_max(w):.2e} s at the actual spacing), "
+                        "checkpoint every 16, Tree theta 0.4 mixed forward, FP64 adjoint "
+                        "(velocity, energy and AB step, all CUDA); loss = E(x_K) + "
+                        "sum |x_K - x_0|^2; wall clock"}
 
 
 def ring_rate(L, torch, steps: int = 1000) -> dict:
@@ -527,49 +604,6 @@ def ring_rate(L, torch, steps: int = 1000) -> dict:
             "ring_speed_cm_s": float(abs(np.mean(u[:, 2]))), "formula_speed_cm_s": float(v_ref),
             "timing": "wall clock around qv_steps (1000 steps, graph replay, one wait); "
                       "qv_step called per step (one wait each) for comparison"}
-
-
-def large_rate(L, torch, steps: int = 5, warmup: int = 3) -> dict:
-    """The large isotropic tangle: 3000 random rings, R ~ U(0.004, 0.015) cm,
-    delta 3e-4 cm, periodic L = 0.1, Barnes-Hut theta 0.5, candidate search every
-    step.  Mixed and FP64 steps timed with CUDA events (inputs far above L2), and
-    the mixed velocity's error against the FP64 velocity on every target."""
-    from qvort_b200 import workloads as W
-
-    w = W.large_tangle()
-    n = w.n
-    out = {"workload": f"3000 rings, N={n}, periodic L=0.1, Tree theta 0.5, AB, dt 1e-7",
-           "n_points": n}
-    stream = torch.cuda.Stream()
-    vel = {}
-    for prec in ("mixed", "fp64"):
-        c = L.Context(L.default_params(**dict(w.params, precision=prec)), stream=stream.cuda_stream)
-        c.set_points(w.x, w.infront, w.behind)
-        vel[prec] = c.velocity(False)[0]
-        it = 0
-        for _ in range(max(1, warmup)):
-            it += 1
-            c.step(it)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            for _ in range(steps):
-                it += 1
-                c.step(it)
-            e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        cnt = c.counters()
-        out[prec] = {"ms_per_step": ms, "pairs_per_s": float(n) * n * 27 / (ms * 1e-3),
-                     "leaf_evals": cnt["leaf_evals"], "far_evals": cnt["far_evals"]}
-        c.close()
-    rms, mx = _rel(vel["mixed"], vel["fp64"])
-    out["error"] = {"mixed_vs_fp64_bh_rms_rel": rms, "mixed_vs_fp64_bh_max_rel": mx,
-                    "targets": n}
-    out["mixed_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
-    return out
 
 
 def direct_rate(L, torch, steps: int = 3, warmup: int = 1) -> dict:
@@ -666,15 +700,17 @@ def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
-    if args.suite != "tangle":
+    if args.suite != "large":
         import torch
 
         from qvort_b200 import lib as L
 
         if args.suite == "batch":
             r = batch_rate(L, torch, args.steps)
-        elif args.suite == "large":
-            r = large_rate(L, torch, args.steps, args.warmup)
+        elif args.suite == "tangle":
+            s = torch.cuda.Stream()
+            r = tangle_rate(L, torch, s, torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8,
+                                                   device="cuda"), args.steps, args.warmup)
         elif args.suite == "ring":
             r = ring_rate(L, torch)
         elif args.suite == "direct":

@@ -25,13 +25,15 @@ extern "C" {
 #define QV_OK 0
 #define QV_ERR_ARG (-1)        /* bad argument or size */
 #define QV_ERR_CUDA (-2)       /* a CUDA call failed, or a device-side copy did not complete
-                                  within its bounded wait; see qv_last_error */
+                                  within its bounded wait (the outputs of that call are then
+                                  undefined); see qv_last_error */
 #define QV_ERR_SINGULAR (-3)   /* tree singularity (src/tree.f90:372-376) */
 #define QV_ERR_TREE_DEPTH (-4) /* octree deeper than QV_MAX_DEPTH (coincident points) */
 #define QV_ERR_STATE (-5)      /* call out of order (no points, no tree, ...) */
 #define QV_ERR_NOMEM (-6)      /* device allocation failed */
 #define QV_ERR_UNSUPPORTED (-7)/* a run.in option outside this path (mirror, forcing, ...) */
-#define QV_ERR_NAN (-8)        /* NaN in positions (NAN_finder, src/general.f90:253-280) */
+#define QV_ERR_NAN (-8)        /* NaN in the positions of any slot at the end of a step
+                                  (NAN_finder, src/general.f90:253-280; run.f90:168) */
 #define QV_ERR_NOALLOC_LIMIT (-9) /* more slots than QV_NOALLOC_MAX_POINTS */
 
 #define QV_MAX_DEPTH 64
@@ -91,9 +93,14 @@ int qv_set_params(qv_ctx *ctx, const qv_params *p);
 const char *qv_last_error(const qv_ctx *ctx);
 
 /* Gather of f(:)%x, f(:)%infront, f(:)%behind into the context (host
- * pointers).  Resets the AB history and closest to zero. */
+ * pointers).  Resets the AB history and closest to zero.  The links are
+ * checked on the host before anything is uploaded (this, qv_set_state and
+ * qv_step_exchange): every infront/behind (and closest, where given) in 0..n,
+ * and an active slot linking forwards and backwards to active slots;
+ * otherwise QV_ERR_ARG and nothing runs. */
 int qv_set_points(qv_ctx *ctx, int n, const double *x, const int *infront, const int *behind);
-/* The same from device pointers (the torch harness). */
+/* The same from device pointers (the torch harness); the links are the
+ * caller's device arrays and are not checked. */
 int qv_set_points_device(qv_ctx *ctx, int n, const double *x, const int *infront,
                          const int *behind);
 /* f(:)%u1..u3 in/out (host; NULL means zero on set, skip on get). */
@@ -199,6 +206,20 @@ int qv_velocity_vjp(qv_ctx *ctx, const double *u_bar, double *x_bar);
  * device velocities u, with dE/dx (explicit, through s' and the segment
  * lengths) and dE/du, device pointers (3n); energy on the host. */
 int qv_energy_grad(qv_ctx *ctx, const double *u, double *energy, double *x_bar, double *u_bar);
+/* One position update of pmotion (src/timestep.f90:48-71: the Adams-Bashforth
+ * ladder, rung chosen per point by exact-zero tests of the history) followed by
+ * enforce_periodic (src/periodic.f90:188-214), from device arrays x, u, u1, u2,
+ * u3 (3n each, n = the context's slot count, its infront marking empty slots)
+ * into x_out; the same operations as qv_step's update, so x_out is bitwise what
+ * qv_step would store.  Queued on the context's stream. */
+int qv_ab_step_device(qv_ctx *ctx, int n, const double *x, const double *u, const double *u1,
+                      const double *u2, const double *u3, double *x_out);
+/* Its adjoint: given x_out_bar, x_bar = x_out_bar and u_bar, u1_bar, u2_bar,
+ * u3_bar = the rung's coefficients times x_out_bar (zero for empty slots);
+ * u1..u3 select the rung.  Device pointers (3n each). */
+int qv_ab_vjp_device(qv_ctx *ctx, int n, const double *u1, const double *u2, const double *u3,
+                     const double *x_out_bar, double *x_bar, double *u_bar, double *u1_bar,
+                     double *u2_bar, double *u3_bar);
 /* biot_savart_general(_shift) (src/timestep.f90:516-563) at m host points and
  * the exact gradient du_i/dx_k (9 per point, row-major) -- the derivative that
  * velocity_quasip takes by central differences (src/hamiltonian.f90:65-89).
@@ -232,6 +253,42 @@ int qv_read_var_file(const char *path, int cap, int *n, double *t, double *x, in
 /* printf (src/output.f90:116-143): the var%04d.log stream snapshot. */
 int qv_write_var_file(const char *path, int n, double t, const double *x, const int *infront,
                       const double *u);
+/* The point fields of a restart file (host arrays of at least n slots: 3 per
+ * slot for vectors, 1 for links and closest/closestd; NULL skips a field on
+ * either side, x/infront/behind are required to write). */
+typedef struct qv_restart {
+  double *x, *u, *u1, *u2, *u3, *u_li, *u_bs, *gi, *gb, *gii, *gbb, *closestd;
+  int *infront, *behind, *closest;
+} qv_restart;
+/* data_dump (src/output.f90:272-285): ./data/var.dat as gfortran writes it --
+ * sequential unformatted records framed by 4-byte length markers: pcount,
+ * recon_count, itime, t, f(:) (pcount records of type qvort,
+ * src/cdata.f90:20-39, under -fdefault-real-8: 464 bytes each in declaration
+ * order with natural alignment), quasi_pcount = 0, part_count = 0.  Fields of
+ * qvort outside this path (x_interp, acc, u_mf, f_mf, stretch, curv,
+ * closestd_loop, pinned flags, t_recon) are written as zero, u_sup as u and
+ * the resolution factor delta as 1.  Files of 2 GiB or more (above ~4.6M
+ * slots) are refused with QV_ERR_ARG. */
+int qv_write_restart_file(const char *path, int n, int recon_count, int itime, double t,
+                          const qv_restart *s);
+/* data_restore (src/initial.f90:501-538): *n = pcount, recon_count, itime and
+ * t, and, when s and s->x are given, the fields of the first *n <= cap slots.
+ * A file whose f(:) record is not pcount * 464 bytes returns QV_ERR_ARG. */
+int qv_read_restart_file(const char *path, int cap, int *n, int *recon_count, int *itime,
+                         double *t, qv_restart *s);
+/* data_dump of the context's state, from its device buffers: positions,
+ * velocities (u, u_s_LI, u_s_BS), history, ghosts, links, closest and closestd
+ * as the last step left them. */
+int qv_dump(qv_ctx *ctx, const char *path, int recon_count, int itime, double t);
+/* data_restore into the context: the positions, links, history and closest of
+ * the file (as qv_set_state), its pcount in the context; itime, t and
+ * recon_count returned.  The run resumes with qv_step(itime + 1): a resumed
+ * run is bitwise the run that was never interrupted. */
+int qv_restore(qv_ctx *ctx, const char *path, int *recon_count, int *itime, double *t);
+/* printf (src/output.f90:116-143) from the context's device buffers: the
+ * var%04d.log stream snapshot of the current positions, links and u. */
+int qv_write_snapshot(qv_ctx *ctx, const char *path, double t);
+
 /* setup_single_loop / setup_leap_frog (src/initial_loop.f90:11-38, 206-245). */
 int qv_setup_loops(const char *initf, int pcount, double delta, double *x, int *infront,
                    int *behind);
@@ -278,6 +335,13 @@ int qv_counters(qv_ctx *ctx, long long *launches, long long *leaf_evals, long lo
 /* Measured FP32 FMA throughput of the current device (TFLOP/s), the
  * denominator of the FP32-pipe roofline. */
 int qv_probe_fp32(void *stream, double *tflops);
+
+/* Test hook, no counterpart in the reference: enable != 0 makes every
+ * source-tile wait of the direct-sum kernels report that it ran out, without
+ * waiting, so the bounded-wait error path (drain the copies in flight, flag
+ * the status word, return QV_ERR_CUDA) can be exercised while every copy
+ * still lands; 0 restores normal waits.  Process-wide. */
+int qv_test_stage_timeout(int enable);
 
 /* Non-local direct Biot-Savart velocity without any device allocation.
  * No counterpart in the reference: it exists for hosts that cannot call

@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
         _lib.qo_precon.argtypes = [P, C.c_int, C.POINTER(QoState)]
         _lib.qo_field_velocity_tree.argtypes = [P, v, C.c_int, v, v]
         _lib.qo_field_velocity_tree.restype = C.c_longlong
+        _lib.qo_field_velocity.argtypes = [P, C.c_int, v, v, v, C.c_int, v, v]
     return _lib
 
 
@@ -355,6 +356,17 @@ def field_velocity_tree(p: QoParams, tree, pts):
     u = np.zeros_like(pts)
     ev = lib().qo_field_velocity_tree(C.byref(p), tree.h, pts.shape[0], _p(pts), _p(u))
     return u, ev
+
+
+def field_velocity(p: QoParams, x, inf, gi, pts):
+    """biot_savart_general with the boundary's images at the points (the BS arm
+    of mesh_velocity)."""
+    x, inf, gi = _f(x), _i(inf), _f(gi)
+    pts = _f(pts).reshape(-1, 3)
+    u = np.zeros_like(pts)
+    lib().qo_field_velocity(C.byref(p), x.shape[0], _p(x), _p(gi), _p(inf), pts.shape[0],
+                            _p(pts), _p(u))
+    return u
 
 
 def dt_max(p: QoParams) -> float:

@@ -1058,3 +1058,43 @@ long long qo_field_velocity_tree(const qo_params *p, const qo_tree *T, int m, co
   }
   return evals;
 }
+
+/* ------------------------------------------------ biot_savart_general */
+/* biot_savart_general (shift == NULL) and biot_savart_general_shift,
+ * src/timestep.f90:516-563: the velocity at an arbitrary point x from every
+ * active segment j -> ghosti(j) (no skip rule), added into u, in the
+ * reference's operation order. */
+static void bs_general(const qo_params *p, int n, const double *xs, const double *gi,
+                       const int *infront, const double *x, const double *shift, double *u) {
+  for (int i = 0; i < n; i++) {
+    if (infront[i] == 0) continue;
+    const double *xi = xs + 3 * i, *gj = gi + 3 * i;
+    double xsh[3], d[3], s[3], ub[3];
+    for (int k = 0; k < 3; k++) xsh[k] = shift ? xi[k] + shift[k] : xi[k];
+    double a = dist_gen_sq(x, xsh);
+    for (int k = 0; k < 3; k++) { d[k] = xsh[k] - x[k]; s[k] = gj[k] - xi[k]; }
+    double b = 2. * dot3(d, s);
+    double c = dist_gen_sq(gj, xi);
+    if ((4 * a * c - b * b) == 0) continue;
+    cross(d, s, ub);
+    for (int k = 0; k < 3; k++) ub[k] = ub[k] * p->quant_circ / ((2 * QO_PI) * (4 * a * c - b * b));
+    double fac = (2 * c + b) / sqrt(a + b + c) - (b / sqrt(a));
+    for (int k = 0; k < 3; k++) ub[k] = ub[k] * fac;
+    for (int k = 0; k < 3; k++) u[k] = u[k] + ub[k];
+  }
+}
+
+/* The BS arm of mesh_velocity (src/timestep.f90:393-416) at m points: the
+ * unshifted sum, then the boundary's images in the reference's loop order,
+ * into one running sum per point. */
+void qo_field_velocity(const qo_params *p, int n, const double *xs, const double *gi,
+                       const int *infront, int m, const double *pts, double *u) {
+  double sh[27 * 3];
+  int ns = image_shifts(p, sh);
+  for (int q = 0; q < m; q++) {
+    double *uq = u + 3 * q;
+    uq[0] = uq[1] = uq[2] = 0.;
+    bs_general(p, n, xs, gi, infront, pts + 3 * q, NULL, uq);
+    for (int s = 0; s < ns; s++) bs_general(p, n, xs, gi, infront, pts + 3 * q, sh + 3 * s, uq);
+  }
+}

@@ -1,11 +1,12 @@
 """Differentiable filament dynamics on top of the C ABI's hand-written derivatives.
 
-The velocity u = calc_velocity(x) (src/timestep.f90:180-309) and the energy
-E = energy_info(x, u) (src/diagnostic.f90:259-280) are torch.autograd.Functions
-whose backward passes call qv_velocity_vjp and qv_energy_grad (CUDA).  The
-Adams-Bashforth ladder of pmotion (src/timestep.f90:48-71) and the periodic
-wrap (src/periodic.f90:188-214) are a few lines of torch, so autograd chains
-them; torch.utils.checkpoint keeps one state every `checkpoint_every` steps
+The velocity u = calc_velocity(x) (src/timestep.f90:180-309), the energy
+E = energy_info(x, u) (src/diagnostic.f90:259-280) and the position update of
+pmotion with the periodic wrap (src/timestep.f90:48-71, src/periodic.f90:
+188-214) are torch.autograd.Functions whose forward and backward passes are
+CUDA kernels of the C ABI (qv_velocity_device / qv_velocity_vjp,
+qv_energy_grad, qv_ab_step_device / qv_ab_vjp_device); torch only chains
+them.  torch.utils.checkpoint keeps one state every `checkpoint_every` steps
 and recomputes the steps in between during the backward pass.
 
 With velocity Tree the topology of each step's octree is frozen in its
@@ -91,40 +92,46 @@ def energy(x: torch.Tensor, u: torch.Tensor, system: FilamentSystem) -> torch.Te
     return EnergyFn.apply(x, u, system)
 
 
-def _allzero(h):
-    return (h == 0).all(dim=1, keepdim=True)
+class ABStepFn(torch.autograd.Function):
+    """pmotion's position update (src/timestep.f90:48-71) and enforce_periodic
+    (src/periodic.f90:188-214) as one CUDA kernel each way: the forward takes
+    the update kernel's operations (bitwise the positions qv_step stores), the
+    backward is the hand-written adjoint qv_ab_vjp_device."""
+
+    @staticmethod
+    def forward(ctx, x, u, u1, u2, u3, system: FilamentSystem):
+        x, u, u1, u2, u3 = (t.detach().contiguous() for t in (x, u, u1, u2, u3))
+        xo = torch.empty_like(x)
+        system.ctx.ab_step_device(x.data_ptr(), u.data_ptr(), u1.data_ptr(), u2.data_ptr(),
+                                  u3.data_ptr(), xo.data_ptr())
+        ctx.save_for_backward(u1, u2, u3)
+        ctx.system = system
+        return xo
+
+    @staticmethod
+    def backward(ctx, xob):
+        u1, u2, u3 = ctx.saved_tensors
+        xob = xob.contiguous()
+        out = [torch.empty_like(xob) for _ in range(5)]
+        ctx.system.ctx.ab_vjp_device(u1.data_ptr(), u2.data_ptr(), u3.data_ptr(), xob.data_ptr(),
+                                     *[t.data_ptr() for t in out])
+        return (*out, None)
 
 
-def ab_step(x, u, u1, u2, u3, dt: float):
-    """One rung of the Adams-Bashforth ladder per point (exact-zero history tests)."""
-    z1, z2, z3 = _allzero(u1), _allzero(u2), _allzero(u3)
-    ab4 = dt * (55.0 * u - 59.0 * u1 + 37.0 * u2 - 9.0 * u3) / 24.0
-    ab3 = (23.0 / 12.0) * dt * u - (4.0 / 3.0) * dt * u1 + (5.0 / 12.0) * dt * u2
-    ab2 = 1.5 * dt * u - 0.5 * dt * u1
-    dx = torch.where(z1, dt * u, torch.where(z2, ab2, torch.where(z3, ab3, ab4)))
-    return x + dx
-
-
-def wrap(x, system: FilamentSystem):
-    bc, L_ = system.params.boundary, system.params.box_size
-    lo = {1: 0, 2: 1, 3: 2}.get(bc)
-    if lo is None:
-        return x
-    h = L_ / 2.0
-    cols = torch.arange(3, device=x.device) >= lo
-    shift = (x.detach() > h).double() - (x.detach() < -h).double()
-    return x - L_ * shift * cols
+def ab_step(x, u, u1, u2, u3, system: FilamentSystem):
+    """One Adams-Bashforth rung per point (exact-zero history tests) and the
+    periodic wrap."""
+    return ABStepFn.apply(x, u, u1, u2, u3, system)
 
 
 def run(x0: torch.Tensor, system: FilamentSystem, nsteps: int, checkpoint_every: int = 16):
     """x_K after nsteps Adams-Bashforth steps from x0 with zero history."""
-    dt = system.params.dt
     zero = torch.zeros_like(x0)
 
     def segment(x, u1, u2, u3, k):
         for _ in range(k):
             u = velocity(x, system)
-            x = wrap(ab_step(x, u, u1, u2, u3, dt), system)
+            x = ab_step(x, u, u1, u2, u3, system)
             u1, u2, u3 = u, u1, u2
         return x, u1, u2, u3
 

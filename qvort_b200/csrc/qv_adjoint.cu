@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "qv_internal.cuh"
+#include "qv_ab.cuh"
 #include "qv_lia.cuh"
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
@@ -612,6 +613,93 @@ static int adj_reserve(qv_ctx *c) {
   return QV_OK;
 }
 
+// ------------------------------------------------------ Adams-Bashforth step
+// The position update of pmotion (src/timestep.f90:48-71) followed by the wrap
+// of enforce_periodic (src/periodic.f90:188-214), from device arrays, and its
+// adjoint.  The forward takes the update kernel's operations (qv_ab.cuh), so a
+// differentiable trajectory is bitwise the trajectory qv_step would make from
+// the same velocities.  The rung is chosen by exact-zero tests of the history,
+// piecewise constant in every input, and the wrap moves a point by a constant:
+// the adjoint is x_bar = x_out_bar and (u, u1, u2, u3)_bar = the rung's
+// coefficients times x_out_bar.  Empty slots (infront = 0) do not move.
+__global__ void k_ab_fwd(int n, double dt, const double *__restrict__ x,
+                         const double *__restrict__ u, const double *__restrict__ u1,
+                         const double *__restrict__ u2, const double *__restrict__ u3,
+                         const int *__restrict__ inf, int lo_axis, double L, double *xo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (inf[i] == 0) {
+    for (int c = 0; c < 3; c++) xo[3 * i + c] = x[3 * i + c];
+    return;
+  }
+  double U1[3], U2[3], U3[3];
+  for (int c = 0; c < 3; c++) {
+    U1[c] = u1[3 * i + c]; U2[c] = u2[3 * i + c]; U3[c] = u3[3 * i + c];
+  }
+  const int rung = ab_rung(U1, U2, U3);
+  for (int c = 0; c < 3; c++) {
+    const double r = ab_update(rung, dt, x[3 * i + c], u[3 * i + c], U1[c], U2[c], U3[c]);
+    xo[3 * i + c] = c >= lo_axis ? wrap_coord(r, L) : r;
+  }
+}
+
+__global__ void k_ab_vjp(int n, double dt, const double *__restrict__ u1,
+                         const double *__restrict__ u2, const double *__restrict__ u3,
+                         const int *__restrict__ inf, const double *__restrict__ xob, double *xb,
+                         double *ub, double *u1b, double *u2b, double *u3b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double k[4] = {0., 0., 0., 0.};
+  if (inf[i] != 0) {
+    double U1[3], U2[3], U3[3];
+    for (int c = 0; c < 3; c++) {
+      U1[c] = u1[3 * i + c]; U2[c] = u2[3 * i + c]; U3[c] = u3[3 * i + c];
+    }
+    ab_coef(ab_rung(U1, U2, U3), dt, k);
+  }
+  for (int c = 0; c < 3; c++) {
+    const double g = xob[3 * i + c];
+    xb[3 * i + c] = g;
+    ub[3 * i + c] = k[0] * g;
+    u1b[3 * i + c] = k[1] * g;
+    u2b[3 * i + c] = k[2] * g;
+    u3b[3 * i + c] = k[3] * g;
+  }
+}
+
+static int ab_lo_axis(int bc) {
+  return bc == QV_BC_PERIODIC ? 0 : bc == QV_BC_OPENX ? 1 : bc == QV_BC_OPENXY ? 2 : 3;
+}
+
+extern "C" int qv_ab_step_device(qv_ctx *c, int n, const double *x, const double *u,
+                                 const double *u1, const double *u2, const double *u3,
+                                 double *x_out) {
+  if (!c) return QV_ERR_ARG;
+  if (n != c->n) return qv_fail(c, QV_ERR_STATE, "qv_ab_step_device: %d slots, context holds %d", n, c->n);
+  if (n == 0) return QV_OK;
+  if (!x || !u || !u1 || !u2 || !u3 || !x_out) return qv_fail(c, QV_ERR_ARG, "null array");
+  k_ab_fwd<<<nblk(n, 256), 256, 0, c->stream>>>(n, c->p.dt, x, u, u1, u2, u3, c->infront,
+                                                ab_lo_axis(c->p.boundary), c->p.box_size, x_out);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
+extern "C" int qv_ab_vjp_device(qv_ctx *c, int n, const double *u1, const double *u2,
+                                const double *u3, const double *xbar_out, double *xbar,
+                                double *ubar, double *u1bar, double *u2bar, double *u3bar) {
+  if (!c) return QV_ERR_ARG;
+  if (n != c->n) return qv_fail(c, QV_ERR_STATE, "qv_ab_vjp_device: %d slots, context holds %d", n, c->n);
+  if (n == 0) return QV_OK;
+  if (!u1 || !u2 || !u3 || !xbar_out || !xbar || !ubar || !u1bar || !u2bar || !u3bar)
+    return qv_fail(c, QV_ERR_ARG, "null array");
+  k_ab_vjp<<<nblk(n, 256), 256, 0, c->stream>>>(n, c->p.dt, u1, u2, u3, c->infront, xbar_out,
+                                                xbar, ubar, u1bar, u2bar, u3bar);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
+}
+
 extern "C" int qv_velocity_vjp(qv_ctx *c, const double *ubar, double *xbar) {
   if (!c || !ubar || !xbar) return QV_ERR_ARG;
   if (c->n == 0) return QV_OK;
@@ -654,6 +742,7 @@ extern "C" int qv_velocity_vjp(qv_ctx *c, const double *ubar, double *xbar) {
   } else if (p.velocity == QV_VEL_TREE) {
     if (!c->tree.valid)
       if ((rc = qv_launch_tree_build(c))) return rc;
+    if ((rc = qv_tree_finalize_root(c))) return rc;
     TreeBuf &t = c->tree;
     size_t nbytes = sizeof(double) * 15 * (size_t)t.n_nodes;
     if (nbytes > c->adj_nb_bytes) {

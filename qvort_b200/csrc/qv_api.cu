@@ -100,7 +100,8 @@ static void free_tree(TreeBuf &t) {
   if (t.ev_ctl) cudaEventDestroy(t.ev_ctl);
   void *ps[] = {t.pos, t.width, t.cent, t.circ, t.C, t.count, t.start, t.parent, t.child_first,
                 t.nchild, t.first, t.level, t.digit, t.cmask, t.w64, t.p64, t.w32, t.c32, t.p32, t.leaf_of,
-                t.ord, t.nodeA, t.nodeB, t.dig, t.rnk, t.cnt9, t.rs9, t.chunk9, t.ctl, t.permb};
+                t.ord, t.nodeA, t.nodeB, t.dig, t.rnk, t.cnt9, t.rs9, t.chunk9, t.ctl, t.permb,
+                t.root_est, t.root_ctl, t.root_unc, t.root_part, t.root_xc};
   for (void *q : ps)
     if (q) cudaFree(q);
   t = TreeBuf();
@@ -237,9 +238,41 @@ int qv_grow_points(qv_ctx *c, int new_cap) {
   return QV_OK;
 }
 
+// The links of a host copy of f(:), checked before anything is uploaded: every
+// link lies in 0..n; an active slot (infront != 0) links forwards and backwards
+// to active slots; closest, when given, lies in 0..n.  The kernels index
+// f(infront)/f(behind) (ghosts, derivatives, tree leaves, line operations) and
+// f(closest) (reconnection) without further checks, so an input that breaks
+// these rules is refused here with QV_ERR_ARG and nothing runs.
+static int check_links(qv_ctx *c, int n, const int *inf, const int *beh, const int *closest,
+                       const char *who) {
+  for (int i = 0; i < n; i++) {
+    const int a = inf[i], b = beh[i];
+    if (a < 0 || a > n || b < 0 || b > n)
+      return qv_fail(c, QV_ERR_ARG, "%s: slot %d has infront %d, behind %d, outside 0..%d", who,
+                     i + 1, a, b, n);
+  }
+  for (int i = 0; i < n; i++) {
+    const int a = inf[i], b = beh[i];
+    if (a != 0 && (b == 0 || inf[a - 1] == 0 || inf[b - 1] == 0))
+      return qv_fail(c, QV_ERR_ARG, "%s: active slot %d links to an empty slot (infront %d, behind %d)",
+                     who, i + 1, a, b);
+  }
+  if (closest)
+    for (int i = 0; i < n; i++)
+      if (closest[i] < 0 || closest[i] > n)
+        return qv_fail(c, QV_ERR_ARG, "%s: slot %d has closest %d, outside 0..%d", who, i + 1,
+                       closest[i], n);
+  return QV_OK;
+}
+
 static int set_points_impl(qv_ctx *c, int n, const double *x, const int *inf, const int *beh,
                            cudaMemcpyKind kind) {
   if (n < 0 || (n > 0 && (!x || !inf || !beh))) return qv_fail(c, QV_ERR_ARG, "bad points");
+  if (kind == cudaMemcpyHostToDevice && n > 0) {
+    int rc0 = check_links(c, n, inf, beh, nullptr, "qv_set_points");
+    if (rc0) return rc0;
+  }
   int rc = reserve_points(c, std::max(n, 1));
   if (rc) return rc;
   c->n = n;
@@ -329,7 +362,9 @@ extern "C" int qv_set_state(qv_ctx *c, int n, const qv_state *s) {
   QV_CHECK_CTX(c);
   if (!s || n < 0 || (n > 0 && (!s->x || !s->infront || !s->behind)))
     return qv_fail(c, QV_ERR_ARG, "qv_set_state: x, infront and behind are required");
-  int rc = reserve_points(c, std::max(n, 1));
+  int rc = n > 0 ? check_links(c, n, s->infront, s->behind, s->closest, "qv_set_state") : QV_OK;
+  if (rc) return rc;
+  rc = reserve_points(c, std::max(n, 1));
   if (rc) return rc;
   c->n = n;
   if (n > 0) {
@@ -376,6 +411,76 @@ extern "C" int qv_get_state(qv_ctx *c, int cap, qv_state *s, int *n) {
   if (s->closestd)
     QV_CUDA(c, cudaMemcpyAsync(s->closestd, c->closestd, sizeof(double) * c->n, d2h, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  return QV_OK;
+}
+
+// ------------------------------------------------------------ restart file
+extern "C" int qv_dump(qv_ctx *c, const char *path, int recon_count, int itime, double t) {
+  QV_CHECK_CTX(c);
+  if (!path) return qv_fail(c, QV_ERR_ARG, "qv_dump: no path");
+  const int n = c->n;
+  const size_t n3 = 3 * (size_t)n;
+  std::vector<double> v[11];
+  for (auto &a : v) a.resize(std::max<size_t>(n3, 1));
+  std::vector<double> cd(std::max(n, 1));
+  std::vector<int> inf(std::max(n, 1)), beh(std::max(n, 1)), cl(std::max(n, 1));
+  const double *dv[11] = {c->x, c->u, c->u1, c->u2, c->u3, c->u_li, c->u_bs,
+                          c->gi, c->gb, c->gii, c->gbb};
+  const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
+  if (n > 0) {
+    for (int k = 0; k < 11; k++)
+      QV_CUDA(c, cudaMemcpyAsync(v[k].data(), dv[k], sizeof(double) * n3, d2h, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(inf.data(), c->infront, sizeof(int) * n, d2h, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(beh.data(), c->behind, sizeof(int) * n, d2h, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(cl.data(), c->closest, sizeof(int) * n, d2h, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(cd.data(), c->closestd, sizeof(double) * n, d2h, c->stream));
+  }
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  qv_restart r;
+  r.x = v[0].data(); r.u = v[1].data(); r.u1 = v[2].data(); r.u2 = v[3].data();
+  r.u3 = v[4].data(); r.u_li = v[5].data(); r.u_bs = v[6].data(); r.gi = v[7].data();
+  r.gb = v[8].data(); r.gii = v[9].data(); r.gbb = v[10].data(); r.closestd = cd.data();
+  r.infront = inf.data(); r.behind = beh.data(); r.closest = cl.data();
+  const int rc = qv_write_restart_file(path, n, recon_count, itime, t, &r);
+  if (rc) return qv_fail(c, rc, "qv_dump: cannot write %s", path);
+  return QV_OK;
+}
+
+extern "C" int qv_restore(qv_ctx *c, const char *path, int *recon_count, int *itime, double *t) {
+  QV_CHECK_CTX(c);
+  if (!path) return qv_fail(c, QV_ERR_ARG, "qv_restore: no path");
+  int n = 0;
+  int rc = qv_read_restart_file(path, 0, &n, recon_count, itime, t, nullptr);
+  if (rc) return qv_fail(c, rc, "qv_restore: cannot read %s", path);
+  std::vector<double> x(3 * (size_t)std::max(n, 1)), h1(x.size()), h2(x.size()), h3(x.size());
+  std::vector<int> inf(std::max(n, 1)), beh(std::max(n, 1)), cl(std::max(n, 1));
+  qv_restart r = {};
+  r.x = x.data(); r.u1 = h1.data(); r.u2 = h2.data(); r.u3 = h3.data();
+  r.infront = inf.data(); r.behind = beh.data(); r.closest = cl.data();
+  rc = qv_read_restart_file(path, n, &n, recon_count, itime, t, &r);
+  if (rc) return qv_fail(c, rc, "qv_restore: %s is not a restart file of this layout", path);
+  qv_state s = {};
+  s.x = r.x; s.u1 = r.u1; s.u2 = r.u2; s.u3 = r.u3;
+  s.infront = r.infront; s.behind = r.behind; s.closest = r.closest;
+  return qv_set_state(c, n, &s);
+}
+
+extern "C" int qv_write_snapshot(qv_ctx *c, const char *path, double t) {
+  QV_CHECK_CTX(c);
+  if (!path) return qv_fail(c, QV_ERR_ARG, "qv_write_snapshot: no path");
+  const int n = c->n;
+  std::vector<double> x(3 * (size_t)std::max(n, 1)), u(x.size());
+  std::vector<int> inf(std::max(n, 1));
+  if (n > 0) {
+    const size_t v = sizeof(double) * 3 * (size_t)n;
+    QV_CUDA(c, cudaMemcpyAsync(x.data(), c->x, v, cudaMemcpyDeviceToHost, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(u.data(), c->u, v, cudaMemcpyDeviceToHost, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(inf.data(), c->infront, sizeof(int) * n, cudaMemcpyDeviceToHost,
+                               c->stream));
+  }
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int rc = qv_write_var_file(path, n, t, x.data(), inf.data(), u.data());
+  if (rc) return qv_fail(c, rc, "qv_write_snapshot: cannot write %s", path);
   return QV_OK;
 }
 
@@ -430,6 +535,9 @@ extern "C" int qv_tree_export(qv_ctx *c, int cap, int *parent, int *digit, int *
   QV_CHECK_CTX(c);
   TreeBuf &t = c->tree;
   if (!t.valid) return qv_fail(c, QV_ERR_STATE, "no tree");
+  int rc = qv_tree_finalize_root(c);
+  if (rc) return rc;
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
   int m = t.n_nodes;
   if (m > cap) return -m;
   std::vector<double> hp(3 * m), hw(m), hc(3 * m), hci(3 * m), hC(9 * m);
@@ -541,6 +649,9 @@ static int velocity_collect(qv_ctx *c, long long *eval_count) {
   if (st & QV_STAT_STAGE)
     return qv_fail(c, QV_ERR_CUDA, "direct sum: a source-tile copy did not complete");
   if (st & QV_STAT_HEAP) return qv_fail(c, QV_ERR_STATE, "line operation: too many re-tests pending");
+  // NAN_finder (src/general.f90:253-280), after the step's closing wrap
+  if (st & QV_STAT_NAN)
+    return qv_fail(c, QV_ERR_NAN, "there is a NaN in the (filament) f%%x array");
   return QV_OK;
 }
 
@@ -755,6 +866,8 @@ extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in,
   if (!in || !out || !n_out || n < 0 || (n > 0 && (!in->x || !in->infront || !in->behind)))
     return qv_fail(c, QV_ERR_ARG, "qv_step_exchange: x, infront and behind are required");
   int rc;
+  if (n > 0 && (rc = check_links(c, n, in->infront, in->behind, in->closest, "qv_step_exchange")))
+    return rc;
   if ((rc = reserve_points(c, std::max(n, 1)))) return rc;
   if ((rc = qv_aux_streams(c))) return rc;
   c->n = n;
@@ -909,6 +1022,8 @@ extern "C" int qv_steps(qv_ctx *c, int itime0, int nsteps) {
     return qv_fail(c, QV_ERR_SINGULAR, "singularity in BS velocity field during qv_steps");
   if (st & QV_STAT_STAGE)
     return qv_fail(c, QV_ERR_CUDA, "direct sum: a source-tile copy did not complete");
+  if (st & QV_STAT_NAN)
+    return qv_fail(c, QV_ERR_NAN, "there is a NaN in the (filament) f%%x array");
   return QV_OK;
 }
 

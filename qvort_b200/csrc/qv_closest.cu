@@ -343,6 +343,8 @@ int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_gri
   if (n_grid == 0) return QV_OK;
   if (c->p.tree_theta > 0) {
     if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
+    int rc = qv_tree_finalize_root(c);
+    if (rc) return rc;
     int nwarps = (n_grid + TPW - 1) / TPW;
     int cap = 7 * (c->tree.depth + 1) + 8;
     size_t smem = sizeof(CStkEnt) * cap * CW;

@@ -22,6 +22,8 @@
 // Work split: blockIdx.x = tile of 128 targets, blockIdx.y = chunk of sources;
 // per-chunk partial sums go to a buffer and are added in fixed chunk order,
 // so results are deterministic.
+#include <cstdlib>
+
 #include "qv_internal.cuh"
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
@@ -254,6 +256,17 @@ __device__ __forceinline__ double shifted(double v, int a, double L) {
 // copy that never lands ends the launch with an error, not a hang.
 #define QV_STAGE_WAIT_NS 1000000000ull  // 1 s
 
+// Test hook (qv_test_stage_timeout): nonzero makes every tile acquire report
+// a wait that ran out, without waiting, so that the error path -- drain the
+// copies in flight, set QV_STAT_STAGE, return QV_ERR_CUDA -- runs while every
+// copy still lands.  Process-wide; read when a direct-sum kernel is launched.
+static int g_stage_fail = 0;
+
+extern "C" int qv_test_stage_timeout(int enable) {
+  g_stage_fail = enable ? 1 : 0;
+  return QV_OK;
+}
+
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
@@ -318,6 +331,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
 struct TilePipe {
   const unsigned char *src;  // pack base
   int j0, j1, ntile;
+  int fail;  // test hook: acquire() reports a wait that ran out without waiting
   // shared-memory addresses: stage k's buffer at buf + k * DTILE * 64, its
   // barrier at bar + 8 k
   unsigned buf, bar;
@@ -341,7 +355,7 @@ struct TilePipe {
   __device__ __forceinline__ bool acquire(int t) const {
     // buffer (t+1)&1 was last read in iteration t-1, which release() closed
     if (threadIdx.x == 0 && t + 1 < ntile) start(t + 1);
-    const bool got = mbar_wait(bar_of(t), parity_of(t));
+    const bool got = fail ? false : mbar_wait(bar_of(t), parity_of(t));
     return __syncthreads_and(got) != 0;
   }
   __device__ __forceinline__ void release() const { __syncthreads(); }
@@ -357,8 +371,9 @@ struct TilePipe {
 
 // stages: 2 * DTILE * 64 contiguous bytes of shared memory; bars: 2 barriers
 __device__ __forceinline__ TilePipe make_pipe(const void *src, int j0, int j1, const void *stages,
-                                              const unsigned long long *bars) {
+                                              const unsigned long long *bars, int fail) {
   TilePipe p;
+  p.fail = fail;
   p.src = static_cast<const unsigned char *>(src);
   p.j0 = j0;
   p.j1 = j1;
@@ -374,7 +389,8 @@ __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restric
                                                     const double *__restrict__ x,
                                                     const int *__restrict__ beh,
                                                     const double *__restrict__ src, int chunk_len,
-                                                    double L, double *part, int *status) {
+                                                    double L, double *part, int *status,
+                                                    int stage_fail) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   __shared__ __align__(128) double tiles[2][DTILE * 8];
   __shared__ __align__(8) unsigned long long bars[2];
@@ -385,7 +401,7 @@ __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restric
   int bi = live ? beh[i] : -1, ii = i + 1;
   double a0x = 0., a0y = 0., a0z = 0., a1x = 0., a1y = 0., a1z = 0.;
   int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
-  const TilePipe pipe = make_pipe(src, j0, j1, tiles, bars);
+  const TilePipe pipe = make_pipe(src, j0, j1, tiles, bars, stage_fail);
   pipe.begin();
   for (int t = 0; t < pipe.ntile; t++) {
     if (!pipe.acquire(t)) {
@@ -417,58 +433,76 @@ __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restric
   }
 }
 
-// One tile of sources against one target and one image.  The target is
-// recentred per image: t = x_i - shift as a hi/lo float pair.  skip2 is the
-// extra slot skipped by the unshifted sum (i itself), -7 for images.
-__device__ __forceinline__ void seg_tile(const float4 *tile, int m, const double *xi, int ma,
-                                         int mb, int mc, double L, int bi, int skip2,
-                                         Kahan3 &acc) {
-  float th[3], tl[3];
-  int mm[3] = {ma, mb, mc};
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    double t = shifted(xi[c], -mm[c], L);
-    th[c] = __double2float_rn(t);
-    tl[c] = __double2float_rn(t - (double)th[c]);
-  }
-  for (int k = 0; k < m; k++) {
-    float4 A = tile[4 * k], B = tile[4 * k + 1], Cc = tile[4 * k + 2], D = tile[4 * k + 3];
-    int jj = __float_as_int(D.x);
-    if (jj == bi || jj == skip2) continue;
-    // A = (xh0 xh1 xh2 xl0) B = (xl1 xl2 gh0 gh1) C = (gh2 gl0 gl1 gl2) D = (slot s0 s1 s2)
-    float r1x = (A.x - th[0]) + (A.w - tl[0]);
-    float r1y = (A.y - th[1]) + (B.x - tl[1]);
-    float r1z = (A.z - th[2]) + (B.y - tl[2]);
-    float r2x = (B.z - th[0]) + (Cc.y - tl[0]);
-    float r2y = (B.w - th[1]) + (Cc.z - tl[1]);
-    float r2z = (Cc.x - th[2]) + (Cc.w - tl[2]);
-    float ox, oy, oz;
-    float r1s = fmaf(r1x, r1x, fmaf(r1y, r1y, r1z * r1z));
-    qv_seg32(r1x, r1y, r1z, r2x, r2y, r2z, D.y, D.z, D.w, r1s, ox, oy, oz);
-    acc.add(ox, oy, oz);
-  }
+// ------------------------------------------------------------ mixed kernel
+// Every staged source is read from shared memory once and summed against the
+// thread's NT targets in all images.  An image (a, b, c) shifts the source by
+// (a L, b L, c L), so its R1 = x_j + shift - x_i and R2 = gi_j + shift - x_i
+// take, per axis, one of at most three values: the target recentred per axis
+// and shift (t = x_i - m L as a hi/lo float pair, made once per thread) gives
+// those values with two FP32 adds each, and their squares, the products
+// R1.R2 and the partial products of R1 x s are formed per axis too.  Each of
+// the 27 pair terms then costs a few adds besides its two rsqrt and one
+// reciprocal.  Per source, the 26 image terms are summed in plain FP32 and
+// that sum, like the main-image term, goes into a Kahan-compensated sum.
+//
+// Pair term: the straight-segment form of qv_seg32 (src/tree.f90:380-390),
+// (1/|R1| + 1/|R2|) q / (1 + cos) (R1 x s), q = 1/(|R1||R2|), cos = R1.R2 q,
+// with 1 + cos taken from sin^2 / (1 - cos) when cos < 0.
+__device__ __forceinline__ void seg_terms(float r1s, float r2s, float dd, float cx, float cy,
+                                          float cz, float &ox, float &oy, float &oz) {
+  const float ra = rsqrtf(r1s), rb = rsqrtf(r2s);
+  const float q = ra * rb;
+  const float cs = dd * q;
+  float den = 1.f + cs;
+  if (cs < 0.f) den = fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
+  float f = (ra + rb) * q;
+  f = den > 0.f ? __fdividef(f, den) : 0.f;
+  ox = f * cx;
+  oy = f * cy;
+  oz = f * cz;
 }
 
-// ------------------------------------------------------------ mixed kernel
-template <int BC>
+template <int BC, int NT>
 __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restrict__ act,
                                                     const double *__restrict__ x,
                                                     const int *__restrict__ beh,
                                                     const float *__restrict__ src, int chunk_len,
-                                                    double L, double *part, int *status) {
-  constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
+                                                    double L, double *part, int *status,
+                                                    int stage_fail) {
+  // shifts per axis (the reference's image loops, src/timestep.f90:235-257)
+  constexpr int PX = BC == QV_BC_PERIODIC ? 3 : 1;
+  constexpr int PY = (BC == QV_BC_PERIODIC || BC == QV_BC_OPENX) ? 3 : 1;
+  constexpr int PZ = BC == QV_BC_OPEN ? 1 : 3;
   __shared__ __align__(128) float4 tiles[2][DTILE * 4];
   __shared__ __align__(8) unsigned long long bars[2];
-  int q = blockIdx.x * DTILE + threadIdx.x;
-  bool live = q < na;
-  int i = live ? act[q] : 0;
-  double xi[3] = {live ? x[3 * i] : 0., live ? x[3 * i + 1] : 0., live ? x[3 * i + 2] : 0.};
-  int bi = live ? beh[i] : -1, ii = i + 1;
-  Kahan3 k0, k1;
-  k0.zero();
-  k1.zero();
-  int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
-  const TilePipe pipe = make_pipe(src, j0, j1, tiles, bars);
+  // per target: slot, skip slots, the recentred target per axis and shift
+  int qk[NT], bi[NT], ii[NT];
+  float th[NT][3][3], tl[NT][3][3];
+  Kahan3 k0[NT], k1[NT];
+#pragma unroll
+  for (int k = 0; k < NT; k++) {
+    const int q = (blockIdx.x * NT + k) * DTILE + threadIdx.x;
+    const bool live = q < na;
+    const int i = live ? act[q] : 0;
+    qk[k] = q;
+    bi[k] = live ? beh[i] : -1;
+    ii[k] = live ? i + 1 : -7;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double xc = live ? x[3 * i + c] : 0.;
+      const int P = c == 0 ? PX : c == 1 ? PY : PZ;
+#pragma unroll
+      for (int m = 0; m < 3; m++) {
+        const double t = P == 3 ? shifted(xc, 1 - m, L) : xc;  // x_i - (m-1) L
+        th[k][c][m] = __double2float_rn(t);
+        tl[k][c][m] = __double2float_rn(t - (double)th[k][c][m]);
+      }
+    }
+    k0[k].zero();
+    k1[k].zero();
+  }
+  const int j0 = blockIdx.y * chunk_len, j1 = min(na, j0 + chunk_len);
+  const TilePipe pipe = make_pipe(src, j0, j1, tiles, bars, stage_fail);
   pipe.begin();
   for (int t = 0; t < pipe.ntile; t++) {
     if (!pipe.acquire(t)) {
@@ -477,19 +511,98 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
     }
     const int m = min(DTILE, j1 - (j0 + t * DTILE));
     const float4 *tile = tiles[t & 1];
-    seg_tile(tile, m, xi, 0, 0, 0, L, bi, ii, k0);
 #pragma unroll 1
-    for (int im = 0; im < NIMG; im++) {
-      int ma, mb, mc;
-      qv_img_shift(BC, im, &ma, &mb, &mc);
-      seg_tile(tile, m, xi, ma, mb, mc, L, bi, -7, k1);
+    for (int e = 0; e < m; e++) {
+      // A = (xh0 xh1 xh2 xl0) B = (xl1 xl2 gh0 gh1) C = (gh2 gl0 gl1 gl2) D = (slot s0 s1 s2)
+      const float4 A = tile[4 * e], B = tile[4 * e + 1], Cc = tile[4 * e + 2], D = tile[4 * e + 3];
+      const int jj = __float_as_int(D.x);
+      const float sx = D.y, sy = D.z, sz = D.w;
+#pragma unroll
+      for (int k = 0; k < NT; k++) {
+        if (jj == bi[k]) continue;  // src/timestep.f90:471, 496
+        float r1x[3], r2x[3], r1y[3], r2y[3], r1z[3], r2z[3];
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+          r1x[s] = (A.x - th[k][0][s]) + (A.w - tl[k][0][s]);
+          r2x[s] = (B.z - th[k][0][s]) + (Cc.y - tl[k][0][s]);
+          r1y[s] = (A.y - th[k][1][s]) + (B.x - tl[k][1][s]);
+          r2y[s] = (B.w - th[k][1][s]) + (Cc.z - tl[k][1][s]);
+          r1z[s] = (A.z - th[k][2][s]) + (B.y - tl[k][2][s]);
+          r2z[s] = (Cc.x - th[k][2][s]) + (Cc.w - tl[k][2][s]);
+        }
+        // per axis: |R1|^2, |R2|^2 and R1.R2 parts, and the parts of R1 x s
+        float a1x[3], a2x[3], pdx[3], xsz[3], xsy[3];
+        float a1y[3], a2y[3], pdy[3], ysz[3], ysx[3];
+        float a1z[3], a2z[3], pdz[3], zsy[3], zsx[3];
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+          a1x[s] = r1x[s] * r1x[s]; a2x[s] = r2x[s] * r2x[s]; pdx[s] = r1x[s] * r2x[s];
+          xsz[s] = r1x[s] * sz; xsy[s] = r1x[s] * sy;
+          a1y[s] = r1y[s] * r1y[s]; a2y[s] = r2y[s] * r2y[s]; pdy[s] = r1y[s] * r2y[s];
+          ysz[s] = r1y[s] * sz; ysx[s] = r1y[s] * sx;
+          a1z[s] = r1z[s] * r1z[s]; a2z[s] = r2z[s] * r2z[s]; pdz[s] = r1z[s] * r2z[s];
+          zsy[s] = r1z[s] * sy; zsx[s] = r1z[s] * sx;
+        }
+        float ix = 0.f, iy = 0.f, iz = 0.f;
+#pragma unroll
+        for (int a = 0; a < PX; a++) {
+          const int sa = PX == 3 ? a : 1;  // index of the x shift (1 = none)
+#pragma unroll
+          for (int b = 0; b < PY; b++) {
+            const int sb = PY == 3 ? b : 1;
+#pragma unroll
+            for (int cc = 0; cc < PZ; cc++) {
+              const int sc = PZ == 3 ? cc : 1;
+              const bool main_img = sa == 1 && sb == 1 && sc == 1;
+              if (main_img && jj == ii[k]) continue;
+              float ox, oy, oz;
+              seg_terms(a1x[sa] + a1y[sb] + a1z[sc], a2x[sa] + a2y[sb] + a2z[sc],
+                        pdx[sa] + pdy[sb] + pdz[sc], ysz[sb] - zsy[sc], zsx[sc] - xsz[sa],
+                        xsy[sa] - ysx[sb], ox, oy, oz);
+              if (main_img) {
+                k0[k].add(ox, oy, oz);
+              } else {
+                ix += ox;
+                iy += oy;
+                iz += oz;
+              }
+            }
+          }
+        }
+        if (PX * PY * PZ > 1) k1[k].add(ix, iy, iz);
+      }
     }
     pipe.release();
   }
-  if (live) {
-    double *o = part + ((size_t)blockIdx.y * na + q) * 6;
-    for (int c = 0; c < 3; c++) { o[c] = k0.get(c); o[3 + c] = k1.get(c); }
+#pragma unroll
+  for (int k = 0; k < NT; k++) {
+    if (qk[k] < na) {
+      double *o = part + ((size_t)blockIdx.y * na + qk[k]) * 6;
+      for (int c = 0; c < 3; c++) { o[c] = k0[k].get(c); o[3 + c] = k1[k].get(c); }
+    }
   }
+}
+
+// Targets per thread of the mixed kernel.
+static int direct_nt() {
+  static int nt = 0;
+  if (!nt) {
+    const char *e = getenv("QV_DIRECT_NT");
+    nt = (e && atoi(e) == 2) ? 2 : 1;
+  }
+  return nt;
+}
+
+template <int BC>
+static void launch_direct32(int nt, dim3 grid, cudaStream_t s, int na, const int *act,
+                            const double *x, const int *beh, const float *src, int chunk_len,
+                            double L, double *part, int *status, int stage_fail) {
+  if (nt == 2)
+    k_direct32<BC, 2><<<grid, DTILE, 0, s>>>(na, act, x, beh, src, chunk_len, L, part, status,
+                                             stage_fail);
+  else
+    k_direct32<BC, 1><<<grid, DTILE, 0, s>>>(na, act, x, beh, src, chunk_len, L, part, status,
+                                             stage_fail);
 }
 
 // u_bs = s0 + s1, u = (u_li + s0) + s1, in fixed chunk order.
@@ -528,7 +641,9 @@ int qv_launch_direct(qv_ctx *c) {
   k_pack_sources<<<tb, 256, 0, c->stream>>>(na, c->act, c->x, c->gi, c->src64, c->src32);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
-  int bx = nblk(na, DTILE);
+  bool mixed = c->p.precision == QV_PREC_MIXED;
+  const int nt = mixed ? direct_nt() : 1;  // targets per thread
+  int bx = nblk(na, DTILE * nt);
   // enough chunks to fill ~4 blocks per SM, each chunk at least 4 tiles
   int want = (4 * c->sm_count + bx - 1) / bx;
   int maxch = max(1, na / (4 * DTILE));
@@ -544,16 +659,17 @@ int qv_launch_direct(qv_ctx *c) {
   double *part = c->dpart;
   dim3 grid(bx, nchunk);
   double L = c->p.box_size;
-  bool mixed = c->p.precision == QV_PREC_MIXED;
   switch (c->p.boundary) {
 #define QV_DIRECT_CASE(BCV)                                                                   \
   case BCV:                                                                                   \
     if (mixed)                                                                                \
-      k_direct32<BCV><<<grid, DTILE, 0, c->stream>>>(na, c->act, c->x, c->behind, c->src32,  \
-                                                     chunk_len, L, part, c->dstatus);         \
+      launch_direct32<BCV>(nt, grid, c->stream, na, c->act, c->x, c->behind, c->src32,       \
+                                                     chunk_len, L, part, c->dstatus,          \
+                                                     g_stage_fail);                           \
     else                                                                                      \
       k_direct64<BCV><<<grid, DTILE, 0, c->stream>>>(na, c->act, c->x, c->behind, c->src64,  \
-                                                     chunk_len, L, part, c->dstatus);         \
+                                                     chunk_len, L, part, c->dstatus,          \
+                                                     g_stage_fail);                           \
     break;
     QV_DIRECT_CASE(QV_BC_OPEN)
     QV_DIRECT_CASE(QV_BC_PERIODIC)
@@ -609,7 +725,8 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
   int *stat = blk + nb + 1;
   if (cudaMemsetAsync(stat, 0, sizeof(int), s) != cudaSuccess) return QV_ERR_CUDA;
   k_pack_sources<<<tb, 256, 0, s>>>(na, act, x, gi, src64, src32);
-  int bx = nblk(na, DTILE);
+  const int nt = mixed ? direct_nt() : 1;
+  int bx = nblk(na, DTILE * nt);
   int want = (4 * sm_count + bx - 1) / bx;
   int maxch = max(1, na / (4 * DTILE));
   int nchunk = max(1, min(min(want, maxch), max_chunks));
@@ -621,11 +738,11 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
 #define QV_DIRECT_SCRATCH_CASE(BCV)                                                      \
   case BCV:                                                                              \
     if (mixed)                                                                           \
-      k_direct32<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src32, chunk_len, L, part,  \
-                                             stat);                                      \
+      launch_direct32<BCV>(nt, grid, s, na, act, x, beh, src32, chunk_len, L, part,      \
+                                             stat, g_stage_fail);                        \
     else                                                                                 \
       k_direct64<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src64, chunk_len, L, part,  \
-                                             stat);                                      \
+                                             stat, g_stage_fail);                        \
     break;
     QV_DIRECT_SCRATCH_CASE(QV_BC_OPEN)
     QV_DIRECT_SCRATCH_CASE(QV_BC_PERIODIC)

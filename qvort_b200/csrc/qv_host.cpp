@@ -5,6 +5,7 @@
 // benchmark configurations (setup_single_loop / setup_leap_frog,
 // src/initial_loop.f90:11-38, 206-245).
 #include <cctype>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -228,4 +229,125 @@ extern "C" int qv_setup_loops(const char *initf, int pcount, double delta, doubl
     return QV_OK;
   }
   return QV_ERR_UNSUPPORTED;
+}
+
+// ------------------------------------------------------------ restart file
+// data_dump / data_restore (src/output.f90:272-285, src/initial.f90:501-538):
+// ./data/var.dat, an unformatted sequential file -- each write is one record
+// framed by its byte length as a 4-byte integer before and after (gfortran's
+// record markers) -- holding pcount, recon_count, itime, t, the whole f(:)
+// array, quasi_pcount (and g), part_count (and p).  An element of f is the
+// reference's type qvort (src/cdata.f90:20-39) under -fdefault-real-8, laid
+// out in declaration order with natural alignment, 464 bytes:
+namespace {
+enum : size_t {
+  F_X = 0, F_X_INTERP = 24, F_U = 48, F_U1 = 72, F_U2 = 96, F_U3 = 120, F_ACC = 144,
+  F_U_SUP = 168, F_U_MF = 192, F_U_S_LI = 216, F_U_S_BS = 240, F_GHOSTI = 264, F_GHOSTB = 288,
+  F_GHOSTII = 312, F_GHOSTBB = 336, F_F_MF = 360, F_STRETCH = 384, F_CURV = 392,
+  F_INFRONT = 400, F_BEHIND = 404, F_CLOSEST = 408, F_CLOSESTD = 416, F_CLOSESTD_LOOP = 424,
+  F_PINNEDI = 432, F_PINNEDB = 436, F_DELTA = 440, F_T_RECON = 448, F_SIZE = 464
+};
+// one record of gfortran's sequential unformatted layout; records of 2 GiB
+// and more would be split into subrecords, which this writer does not do
+bool put_rec(std::FILE *f, const void *p, size_t bytes) {
+  if (bytes > 0x7fffffffu - 8) return false;
+  const int32_t m = (int32_t)bytes;
+  return std::fwrite(&m, 4, 1, f) == 1 && (bytes == 0 || std::fwrite(p, bytes, 1, f) == 1) &&
+         std::fwrite(&m, 4, 1, f) == 1;
+}
+bool get_rec(std::FILE *f, std::vector<unsigned char> &buf) {
+  int32_t m = 0, m2 = 0;
+  if (std::fread(&m, 4, 1, f) != 1 || m < 0) return false;
+  buf.resize((size_t)m);
+  if (m > 0 && std::fread(buf.data(), (size_t)m, 1, f) != 1) return false;
+  return std::fread(&m2, 4, 1, f) == 1 && m2 == m;
+}
+template <class T> bool get_scalar(std::FILE *f, T *out) {
+  std::vector<unsigned char> b;
+  if (!get_rec(f, b) || b.size() != sizeof(T)) return false;
+  std::memcpy(out, b.data(), sizeof(T));
+  return true;
+}
+}  // namespace
+
+extern "C" int qv_write_restart_file(const char *path, int n, int recon_count, int itime,
+                                     double t, const qv_restart *s) {
+  if (!path || !s || n < 0 || (n > 0 && (!s->x || !s->infront || !s->behind))) return QV_ERR_ARG;
+  if ((size_t)n * F_SIZE > 0x7fffffffu - 8) return QV_ERR_ARG;
+  std::vector<unsigned char> fa((size_t)n * F_SIZE, 0);
+  auto put3 = [&](size_t off, const double *a, int i) {
+    if (a) std::memcpy(&fa[(size_t)i * F_SIZE + off], a + 3 * (size_t)i, 24);
+  };
+  for (int i = 0; i < n; i++) {
+    unsigned char *e = &fa[(size_t)i * F_SIZE];
+    put3(F_X, s->x, i);
+    put3(F_U, s->u, i);
+    put3(F_U1, s->u1, i);
+    put3(F_U2, s->u2, i);
+    put3(F_U3, s->u3, i);
+    put3(F_U_SUP, s->u, i);  // superfluid velocity = u with no normal fluid
+    put3(F_U_S_LI, s->u_li, i);
+    put3(F_U_S_BS, s->u_bs, i);
+    put3(F_GHOSTI, s->gi, i);
+    put3(F_GHOSTB, s->gb, i);
+    put3(F_GHOSTII, s->gii, i);
+    put3(F_GHOSTBB, s->gbb, i);
+    std::memcpy(e + F_INFRONT, s->infront + i, 4);
+    std::memcpy(e + F_BEHIND, s->behind + i, 4);
+    if (s->closest) std::memcpy(e + F_CLOSEST, s->closest + i, 4);
+    if (s->closestd) std::memcpy(e + F_CLOSESTD, s->closestd + i, 8);
+    const double one = 1.;  // the per-point resolution factor (delta_adapt off)
+    std::memcpy(e + F_DELTA, &one, 8);
+  }
+  std::FILE *f = std::fopen(path, "wb");
+  if (!f) return QV_ERR_ARG;
+  const int zero = 0;
+  bool ok = put_rec(f, &n, 4) && put_rec(f, &recon_count, 4) && put_rec(f, &itime, 4) &&
+            put_rec(f, &t, 8) && put_rec(f, fa.data(), fa.size()) &&
+            put_rec(f, &zero, 4) /* quasi_pcount */ && put_rec(f, &zero, 4) /* part_count */;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? QV_OK : QV_ERR_ARG;
+}
+
+extern "C" int qv_read_restart_file(const char *path, int cap, int *n, int *recon_count,
+                                    int *itime, double *t, qv_restart *s) {
+  if (!path || !n) return QV_ERR_ARG;
+  std::FILE *f = std::fopen(path, "rb");
+  if (!f) return QV_ERR_ARG;
+  int pc = 0, rc_ = 0, it = 0;
+  double tt = 0.;
+  std::vector<unsigned char> fa;
+  bool ok = get_scalar(f, &pc) && get_scalar(f, &rc_) && get_scalar(f, &it) &&
+            get_scalar(f, &tt) && pc >= 0;
+  if (ok && s && s->x) ok = get_rec(f, fa) && fa.size() == (size_t)pc * F_SIZE;
+  std::fclose(f);
+  if (!ok) return QV_ERR_ARG;
+  *n = pc;
+  if (recon_count) *recon_count = rc_;
+  if (itime) *itime = it;
+  if (t) *t = tt;
+  if (!s || !s->x) return QV_OK;
+  if (pc > cap) return QV_ERR_ARG;
+  auto get3 = [&](size_t off, double *a, int i) {
+    if (a) std::memcpy(a + 3 * (size_t)i, &fa[(size_t)i * F_SIZE + off], 24);
+  };
+  for (int i = 0; i < pc; i++) {
+    const unsigned char *e = &fa[(size_t)i * F_SIZE];
+    get3(F_X, s->x, i);
+    get3(F_U, s->u, i);
+    get3(F_U1, s->u1, i);
+    get3(F_U2, s->u2, i);
+    get3(F_U3, s->u3, i);
+    get3(F_U_S_LI, s->u_li, i);
+    get3(F_U_S_BS, s->u_bs, i);
+    get3(F_GHOSTI, s->gi, i);
+    get3(F_GHOSTB, s->gb, i);
+    get3(F_GHOSTII, s->gii, i);
+    get3(F_GHOSTBB, s->gbb, i);
+    if (s->infront) std::memcpy(s->infront + i, e + F_INFRONT, 4);
+    if (s->behind) std::memcpy(s->behind + i, e + F_BEHIND, 4);
+    if (s->closest) std::memcpy(s->closest + i, e + F_CLOSEST, 4);
+    if (s->closestd) std::memcpy(s->closestd + i, e + F_CLOSESTD, 8);
+  }
+  return QV_OK;
 }

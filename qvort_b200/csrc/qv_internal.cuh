@@ -21,6 +21,7 @@
 #define QV_STAT_STACK 2     // walk or search stack overflow
 #define QV_STAT_HEAP 4      // a line scan's re-test heap overflowed
 #define QV_STAT_STAGE 8     // a direct-sum source-tile copy did not land in time
+#define QV_STAT_NAN 16      // a NaN in the positions at the end of a step
 
 // Walk-ready node header, FP64 (64 B).  cent, width and the geometric offset
 // geo = |cent - cell centre| (src/tree.f90:355-357) in FP64 so that every
@@ -111,7 +112,20 @@ struct TreeBuf {
   int *h_ctl = nullptr;                    // pinned copy of the control block
   cudaEvent_t ev_ctl = nullptr;
   std::vector<int> lvl_start;
+  // Root centroid.  The exact value (the reference's sequential sum, a chain
+  // of n dependent FP64 adds) runs on a side stream; until it is joined the
+  // root's headers hold an estimate whose distance from it is bounded:
+  // root_est = [estimate (3), bound, exact (3), spare].  root_ctl = [count of
+  // root decisions left undecided by the bound, spare, redo flag, ticket].
+  double *root_est = nullptr;
+  int *root_ctl = nullptr;
+  int4 *root_unc = nullptr;  // the undecided (target, task slot, evals, far evals)
+  double *root_part = nullptr;  // per-block partial sums of the estimate
+  double *root_xc = nullptr;    // the active positions in active order (the chain's input)
+  bool root_pending = false;    // headers hold the estimate
 };
+#define QV_ROOT_UNC_CAP 8192
+#define QV_ROOT_EST_BLOCKS 296
 
 // Phases timed with CUDA events when profiling is on (qv_profile).
 enum {
@@ -200,6 +214,9 @@ int qv_launch_ghosts(qv_ctx *c);
 int qv_launch_lia(qv_ctx *c);
 int qv_launch_direct(qv_ctx *c);
 int qv_launch_tree_build(qv_ctx *c);
+// Join the exact root centroid and re-pack the root with it (no-op when it is
+// in already).  Every reader of the tree other than the velocity walk calls it.
+int qv_tree_finalize_root(qv_ctx *c);
 int qv_launch_walk(qv_ctx *c);
 int qv_launch_ab(qv_ctx *c);
 int qv_launch_rk3_stage(qv_ctx *c, int stage);

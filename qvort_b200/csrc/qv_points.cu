@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "qv_internal.cuh"
+#include "qv_ab.cuh"
 #include "qv_lia.cuh"
 
 int qv_fail(qv_ctx *c, int code, const char *fmt, ...) {
@@ -142,30 +143,10 @@ __global__ void k_ab(int n, double dt, double *x, const double *__restrict__ u, 
     X[c] = x[3 * i + c]; U[c] = u[3 * i + c]; U1[c] = u1[3 * i + c];
     U2[c] = u2[3 * i + c]; U3[c] = u3[3 * i + c];
   }
-  bool z1 = fabs(U1[0]) == 0 && fabs(U1[1]) == 0 && fabs(U1[2]) == 0;
-  bool z2 = fabs(U2[0]) == 0 && fabs(U2[1]) == 0 && fabs(U2[2]) == 0;
-  bool z3 = fabs(U3[0]) == 0 && fabs(U3[1]) == 0 && fabs(U3[2]) == 0;
-  const double three_twos = 3. / 2., one_half = 1. / 2., c23_12 = 23. / 12.,
-               c4_3 = 4. / 3., c5_12 = 5. / 12.;
+  const int rung = ab_rung(U1, U2, U3);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    double r;
-    if (z1) {
-      r = __dadd_rn(X[c], __dmul_rn(dt, U[c]));
-    } else if (z2) {
-      r = __dadd_rn(X[c], __dmul_rn(__dmul_rn(three_twos, dt), U[c]));
-      r = __dsub_rn(r, __dmul_rn(__dmul_rn(one_half, dt), U1[c]));
-    } else if (z3) {
-      r = __dadd_rn(X[c], __dmul_rn(__dmul_rn(c23_12, dt), U[c]));
-      r = __dsub_rn(r, __dmul_rn(__dmul_rn(c4_3, dt), U1[c]));
-      r = __dadd_rn(r, __dmul_rn(__dmul_rn(c5_12, dt), U2[c]));
-    } else {
-      double s = __dsub_rn(__dmul_rn(55., U[c]), __dmul_rn(59., U1[c]));
-      s = __dadd_rn(s, __dmul_rn(37., U2[c]));
-      s = __dsub_rn(s, __dmul_rn(9., U3[c]));
-      r = __dadd_rn(X[c], __ddiv_rn(__dmul_rn(dt, s), 24.));
-    }
-    x[3 * i + c] = r;
+    x[3 * i + c] = ab_update(rung, dt, X[c], U[c], U1[c], U2[c], U3[c]);
     u3[3 * i + c] = U2[c];
     u2[3 * i + c] = U1[c];
     u1[3 * i + c] = U[c];
@@ -217,8 +198,15 @@ int qv_launch_rk3_stage(qv_ctx *c, int stage) {
 
 // ---------------------------------------------------------------- wrap
 // enforce_periodic, src/periodic.f90:188-214 (and its yz / z variants).
-__global__ void k_wrap(int n, double *x, const int *__restrict__ inf, int lo_axis, double L) {
+// enforce_periodic (src/periodic.f90:188-214) on the axes lo_axis..2, and the
+// end-of-step NaN test of NAN_finder (src/general.f90:253-280, called at
+// src/run.f90:168): a NaN in any coordinate of any slot below n, empty slots
+// included, sets QV_STAT_NAN.  lo_axis = 3 (open boundaries): the test only.
+__global__ void k_wrap(int n, double *x, const int *__restrict__ inf, int lo_axis, double L,
+                       int *status) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool nan = i < n && (isnan(x[3 * i]) || isnan(x[3 * i + 1]) || isnan(x[3 * i + 2]));
+  if (__any_sync(0xffffffffu, nan) && (threadIdx.x & 31) == 0) atomicOr(status, QV_STAT_NAN);
   if (i >= n) return;
   if (inf[i] == 0) return;
   double h = L / 2.;
@@ -233,8 +221,9 @@ __global__ void k_wrap(int n, double *x, const int *__restrict__ inf, int lo_axi
 
 int qv_launch_wrap(qv_ctx *c) {
   int lo = lo_axis_of(c->p.boundary);
-  if (c->n == 0 || lo > 2) return QV_OK;
-  k_wrap<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->x, c->infront, lo, c->p.box_size);
+  if (c->n == 0) return QV_OK;
+  k_wrap<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->n, c->x, c->infront, std::min(lo, 3),
+                                                 c->p.box_size, c->dstatus);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
   return QV_OK;

@@ -924,7 +924,7 @@ __device__ __forceinline__ void root_cent_chain(const int n_act, const int *__re
   auto produce = [&](int ch, double *dst) {
     int base = ch * RC, m = min(RC, n_act - base);
     for (int q = threadIdx.x - 32; q < m; q += blockDim.x - 32) {
-      int i = act[base + q];
+      int i = act ? act[base + q] : base + q;
       dst[3 * q] = x[3 * i];
       dst[3 * q + 1] = x[3 * i + 1];
       dst[3 * q + 2] = x[3 * i + 2];
@@ -959,6 +959,82 @@ __global__ void __launch_bounds__(512) k_root_cent(const int *__restrict__ d_nac
                                                    const int *__restrict__ act,
                                                    const double *__restrict__ x, double *cent) {
   root_cent_chain(*d_nact, act, x, cent);
+}
+
+// The estimate of the same centroid the walk starts from while the chain runs:
+// a parallel sum S of the active positions and, per component, the bound
+//   |exact - estimate| <= 2 gamma_n sum|x| / n + 4 u |estimate|,
+// gamma_n = n u / (1 - n u), u = 2^-53.  Any order of summing n terms is within
+// gamma_(n-1) sum|x| of the true sum (the reference's sequential sum
+// included), and each of the two divisions by n rounds once.  est[3] is the
+// Euclidean norm of the three component bounds, widened by a relative 1e-6
+// (which also covers the rounding of sum|x| itself).  The same pass copies the
+// active positions, in active order, to xc for the exact chain, so that the
+// chain reads nothing another kernel may write before it is joined.  The last
+// block to finish (ticket ctl[3]) reduces the block sums in block order and
+// clears the counters of the walk's fix-up.
+__global__ void __launch_bounds__(256) k_root_est(const int *__restrict__ d_nact,
+                                                  const int *__restrict__ act,
+                                                  const double *__restrict__ x, double *xc,
+                                                  double *part, int *ctl, double *est) {
+  const int n = *d_nact;
+  double v[6] = {0., 0., 0., 0., 0., 0.};
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int i = act[q];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double y = x[3 * i + c];
+      xc[3 * (size_t)q + c] = y;
+      v[c] += y;
+      v[3 + c] += fabs(y);
+    }
+  }
+  __shared__ double red[6][8];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane == 0) red[k][w] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double t = 0.;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[threadIdx.x][k];
+    part[6 * blockIdx.x + threadIdx.x] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&ctl[3], 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double S[6] = {0., 0., 0., 0., 0., 0.};
+    for (int b = 0; b < (int)gridDim.x; b++)
+      for (int k = 0; k < 6; k++) S[k] += part[6 * b + k];
+    const double u = 1.1102230246251565e-16, nu = n * u;
+    const double gam = nu / (1. - nu);
+    double e2 = 0.;
+    for (int c = 0; c < 3; c++) {
+      est[c] = S[c] / n;
+      const double e = 2. * gam * S[3 + c] / n + 4. * u * fabs(est[c]);
+      e2 += e * e;
+    }
+    est[3] = sqrt(e2) * (1. + 1e-6) + 1e-300;
+    ctl[0] = 0;
+    ctl[2] = 0;
+    ctl[3] = 0;
+  }
+}
+
+// Put the exact root centroid in (cent[0..2] and the root's headers) once its
+// chain has been joined.
+__global__ void k_root_pack(PackArgs pk, const double *__restrict__ exact, double *cent) {
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < 3; c++) cent[c] = exact[c];
+    pack_one(pk, 0);
+  }
 }
 
 // The same centroid for every root of a forest: block r takes root r, whose
@@ -1218,6 +1294,7 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
       if ((rc = qv_grow(c, (void **)&t.rnk, sizeof(int) * np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.leaf_of, sizeof(int) * np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.permb, sizeof(int) * np))) return rc;
+      if ((rc = qv_grow(c, (void **)&t.root_xc, sizeof(double) * 3 * (size_t)np))) return rc;
       if ((rc = qv_grow(c, (void **)&t.cnt9, sizeof(int) * 9 * (size_t)(2 * np + 2)))) return rc;
       if ((rc = qv_grow(c, (void **)&t.rs9, sizeof(int) * 9 * (size_t)(np + 1)))) return rc;
       if ((rc = qv_grow(c, (void **)&t.chunk9, sizeof(int) * 9 * (size_t)(np / CH + 2)))) return rc;
@@ -1303,16 +1380,32 @@ int qv_launch_tree_build(qv_ctx *c) {
   // sized by the slot count n, so the host does not wait for the compaction.
   if ((rc = qv_compact_active_async(c))) return rc;
   const int n = c->n;
-  // the root centroid chain needs only the active list: start it now on a side
-  // stream so that it overlaps the level-synchronous build
   if ((rc = qv_aux_streams(c))) return rc;
-  QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
-  QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
-  k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(c->d_nact, c->act, c->x,
-                                                                   c->dscalar);
+  // a chain of an earlier build that no reader joined still reads root_xc
+  if (t.root_pending) {
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
+    t.root_pending = false;
+  }
+  if (!t.root_est) {
+    QV_CUDA(c, cudaMalloc((void **)&t.root_est, 8 * sizeof(double)));
+    QV_CUDA(c, cudaMalloc((void **)&t.root_ctl, 4 * sizeof(int)));
+    QV_CUDA(c, cudaMalloc((void **)&t.root_unc, QV_ROOT_UNC_CAP * sizeof(int4)));
+    QV_CUDA(c, cudaMalloc((void **)&t.root_part, 6 * QV_ROOT_EST_BLOCKS * sizeof(double)));
+    QV_CUDA(c, cudaMemsetAsync(t.root_ctl, 0, 4 * sizeof(int), c->stream));
+  }
+  if ((rc = tree_reserve(c, n, std::max(t.cap_nodes, 4 * n + 64),
+                         std::max(t.cap_levels, std::min(QV_MAX_DEPTH + 1, 40)))))
+    return rc;
+  // The root centroid (the reference's sequential sum, src/tree.f90:53-55)
+  // is a chain of n dependent FP64 adds.  It runs on a side stream over a
+  // private copy of the active positions and is joined only by the first
+  // reader of the tree after the walk's launch; the build and the walk use the
+  // bounded estimate k_root_est makes here (see root_open).
+  k_root_est<<<QV_ROOT_EST_BLOCKS, 256, 0, c->stream>>>(c->d_nact, c->act, c->x, t.root_xc,
+                                                        t.root_part, t.root_ctl, t.root_est);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
-  QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
+  bool chain_started = false;
   if (!t.h_ctl) {
     QV_CUDA(c, cudaMallocHost((void **)&t.h_ctl, sizeof(int) * CTL_SIZE));
     QV_CUDA(c, cudaEventCreateWithFlags(&t.ev_ctl, cudaEventDisableTiming));
@@ -1344,6 +1437,19 @@ int qv_launch_tree_build(qv_ctx *c) {
     // side stream while the block-local levels finish the tree
     QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
     QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork, 0));
+    if (!chain_started) {
+      // the root centroid's chain starts behind the cooperative kernel, whose
+      // blocks must all be resident at once: a one-block kernel holding an
+      // SM's shared memory would delay it until the chain ended
+      QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
+      k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(c->d_nact, nullptr,
+                                                                       t.root_xc, t.root_est + 4);
+      QV_LAUNCH_CHECK(c);
+      QV_COUNT(c, 1);
+      QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
+      t.root_pending = true;
+      chain_started = true;
+    }
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
     k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rnk,
                                                         t.ctl + CTL_NBIG, BIGN, INT_MAX, 1);
@@ -1382,8 +1488,9 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
-    for (int k = 0; k < 3; k++) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[k], 0));
-    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, c->dscalar,
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[2], 0));
+    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, t.root_est,
                                                           t.cent);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
@@ -1415,6 +1522,18 @@ int qv_launch_tree_build(qv_ctx *c) {
     return QV_OK;
   }
   return qv_fail(c, QV_ERR_NOMEM, "tree build did not fit after repeated growth");
+}
+
+int qv_tree_finalize_root(qv_ctx *c) {
+  TreeBuf &t = c->tree;
+  if (!t.root_pending) return QV_OK;
+  t.root_pending = false;
+  QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
+  if (!t.valid) return QV_OK;
+  k_root_pack<<<1, 32, 0, c->stream>>>(pack_args(c, 1, t.leaf_of, c->n), t.root_est + 4, t.cent);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  return QV_OK;
 }
 
 // ------------------------------------------------------------------ forest

@@ -48,7 +48,24 @@ struct WalkArgs {
   int extra, ngroups, stk_cap;
   unsigned long long *evals, *evals_far;
   int *status;
+  // Root header speculation (see root_open): root_est[3] bounds the distance
+  // of the header's centroid from the exact one (nullptr: the header is
+  // exact); undecided root tests go to unc (capacity unc_cap, count in
+  // *unc_count).  gate non-null: the launch does nothing unless *gate != 0.
+  const double *root_est;
+  int4 *unc;
+  int *unc_count;
+  int unc_cap;
+  const int *gate;
 };
+
+// Record a lane whose root test the bound left undecided, with the
+// evaluations its walk of this task counted.
+__device__ __forceinline__ void note_undecided(const WalkArgs &a, int q, int sl, unsigned ev,
+                                               unsigned evf) {
+  const int k = atomicAdd(a.unc_count, 1);
+  if (k < a.unc_cap) a.unc[k] = make_int4(q, sl, (int)ev, (int)evf);
+}
 
 // Task slot s: s < NSPLIT -> unshifted image, root child s; else image s-NSPLIT.
 __device__ __forceinline__ void slot_image(int bc, int s, int &ma, int &mb, int &mc) {
@@ -61,6 +78,8 @@ template <int BC>
 __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   __shared__ int2 stk[WW][STK];
+  if (a.gate && *a.gate == 0) return;
+  const double rdelta = a.root_est ? a.root_est[3] : 0.;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int2 *st = stk[wid];
   const int items = a.ngroups * (NSPLIT + NIMG);
@@ -77,7 +96,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
     }
     double acc[3] = {0., 0., 0.};
     unsigned long long ev = 0, evf = 0;
-    bool bad = false;
+    bool bad = false, runc = false;
     int ma, mb, mc;
     slot_image(BC, sl, ma, mb, mc);
     const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
@@ -96,7 +115,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
         top = (sl == 0 && live_mask) ? 1 : 0;
       } else {
         if (live) {
-          ropen = exact_open(exact_dist(xi, r, s), r, a.theta, a.extra);
+          ropen = root_open(xi, r, s, a.theta, a.extra, rdelta, runc);
           if (!ropen && sl == 0) { ev++; evf++; }  // root far field: zero moments
         }
         const unsigned om = __ballot_sync(0xffffffffu, ropen);
@@ -144,7 +163,8 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
         bool open = false;
         if (in) {
           double dist = exact_dist(xi, h, s);
-          if (exact_open(dist, h, a.theta, a.extra)) {
+          if (node == 0 ? root_open(xi, h, s, a.theta, a.extra, rdelta, runc)
+                        : exact_open(dist, h, a.theta, a.extra)) {
             open = true;
           } else {
             ev++;
@@ -182,6 +202,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
       double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
       o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2];
     }
+    if (runc) note_undecided(a, q, sl, (unsigned)ev, (unsigned)evf);
     for (int o = 16; o > 0; o >>= 1) {
       ev += __shfl_down_sync(0xffffffffu, ev, o);
       evf += __shfl_down_sync(0xffffffffu, evf, o);
@@ -197,6 +218,8 @@ template <int BC>
 __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 blocks/SM: measured fastest (5-7 tried)
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   extern __shared__ StkEnt stk_dyn[];
+  if (a.gate && *a.gate == 0) return;
+  const double rdelta = a.root_est ? a.root_est[3] : 0.;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   StkEnt *st = stk_dyn + wid * a.stk_cap;
   const int items = a.ngroups * (NSPLIT + NIMG);
@@ -214,7 +237,7 @@ __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 block
     Kahan3w k0;
     k0.zero();
     unsigned ev = 0, evf = 0;  // per task: far below 2^32
-    bool bad = false;
+    bool bad = false, runc = false;
     int ma, mb, mc;
     slot_image(BC, sl, ma, mb, mc);
     const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
@@ -249,7 +272,7 @@ __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 block
         top = (sl == 0 && live_mask) ? 1 : 0;
       } else {
         if (live) {
-          ropen = exact_open(exact_dist(xi, r, s), r, a.theta, a.extra);
+          ropen = root_open(xi, r, s, a.theta, a.extra, rdelta, runc);
           if (!ropen && sl == 0) { ev++; evf++; }  // root far field: zero moments
         }
         const unsigned om = __ballot_sync(0xffffffffu, ropen);
@@ -307,7 +330,8 @@ __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 block
             open = d2 < h.rlo;
           } else {
             const WNode64 h64 = a.w64[node];
-            open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+            open = node == 0 ? root_open(xi, h64, s, a.theta, a.extra, rdelta, runc)
+                             : exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
           }
           if (!open) {
             ev++;
@@ -353,6 +377,7 @@ __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 block
       double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
       o[0] = k0.get(0); o[1] = k0.get(1); o[2] = k0.get(2);
     }
+    if (runc) note_undecided(a, q, sl, ev, evf);
     for (int o = 16; o > 0; o >>= 1) {
       ev += __shfl_down_sync(0xffffffffu, ev, o);
       evf += __shfl_down_sync(0xffffffffu, evf, o);
@@ -384,6 +409,40 @@ __global__ void k_walk_reduce(int n_act, int nimg, const int *__restrict__ perm,
   }
 }
 
+// Root tests the centroid bound left undecided (see root_open), once the
+// exact root header is in: a lane that walked an image whose root is in fact
+// far drops that image's sum (the root's moments are zero) and counts the one
+// far-field evaluation the reference counts instead of its walk's.  More
+// undecided tests than the list holds: zero the counters and raise the redo
+// flag, and the gated second walk recomputes every task with the exact root.
+__global__ void k_root_fix(WalkArgs a, int bc, const int4 *__restrict__ unc, int *ctl) {
+  const int cnt = ctl[0];
+  if (cnt > QV_ROOT_UNC_CAP) {
+    if (threadIdx.x == 0) {
+      *a.evals = 0;
+      *a.evals_far = 0;
+      ctl[2] = 1;
+    }
+    return;
+  }
+  if (threadIdx.x == 0) ctl[2] = 0;
+  const WNode64 r = a.w64[0];
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+    const int4 u = unc[e];
+    const int q = u.x, sl = u.y, i = a.perm[q];
+    const double xi[3] = {a.x[3 * i], a.x[3 * i + 1], a.x[3 * i + 2]};
+    int ma, mb, mc;
+    slot_image(bc, sl, ma, mb, mc);
+    const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
+    if (exact_open(exact_dist(xi, r, s), r, a.theta, a.extra)) continue;
+    double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
+    o[0] = o[1] = o[2] = 0.;
+    const unsigned long long one = (sl == 0 || sl >= NSPLIT) ? 1ull : 0ull;
+    atomicAdd(a.evals, one - (unsigned long long)(unsigned)u.z);
+    atomicAdd(a.evals_far, one - (unsigned long long)(unsigned)u.w);
+  }
+}
+
 int qv_launch_walk(qv_ctx *c) {
   TreeBuf &t = c->tree;
   if (!t.valid) return qv_fail(c, QV_ERR_STATE, "tree walk without a built tree");
@@ -402,6 +461,12 @@ int qv_launch_walk(qv_ctx *c) {
   a.L = c->p.box_size; a.theta = c->p.tree_theta; a.gfac = c->p.quant_circ / 4. / QV_PI;
   a.extra = c->p.tree_extra_correction; a.evals = c->evals; a.evals_far = c->evals_far;
   a.status = c->dstatus;
+  a.root_est = nullptr; a.unc = nullptr; a.unc_count = nullptr; a.unc_cap = 0; a.gate = nullptr;
+  const bool spec = t.root_pending;
+  if (spec) {
+    a.root_est = t.root_est; a.unc = t.root_unc; a.unc_count = t.root_ctl;
+    a.unc_cap = QV_ROOT_UNC_CAP;
+  }
   a.ngroups = (t.n_act + 31) / 32;
   // a depth-first stack over a tree of depth D never holds more than 7 D + 1
   // entries (each open pushes at most 8 and pops 1)
@@ -419,25 +484,44 @@ int qv_launch_walk(qv_ctx *c) {
       c->smem_walk = smem;
     }
   }
-  switch (c->p.boundary) {
+  auto launch = [&](const WalkArgs &w, int grid) -> int {
+    switch (c->p.boundary) {
 #define QV_WALK_CASE(BCV)                                                        \
   case BCV:                                                                      \
-    if (mixed) k_walk32<BCV><<<nb, WW * 32, smem, c->stream>>>(a);               \
-    else k_walk64<BCV><<<nb, WW * 32, 0, c->stream>>>(a);                        \
+    if (mixed) k_walk32<BCV><<<grid, WW * 32, smem, c->stream>>>(w);             \
+    else k_walk64<BCV><<<grid, WW * 32, 0, c->stream>>>(w);                      \
     break;
-    QV_WALK_CASE(QV_BC_OPEN)
-    QV_WALK_CASE(QV_BC_PERIODIC)
-    QV_WALK_CASE(QV_BC_OPENX)
-    QV_WALK_CASE(QV_BC_OPENXY)
+      QV_WALK_CASE(QV_BC_OPEN)
+      QV_WALK_CASE(QV_BC_PERIODIC)
+      QV_WALK_CASE(QV_BC_OPENX)
+      QV_WALK_CASE(QV_BC_OPENXY)
 #undef QV_WALK_CASE
-    default:
-      return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
+      default:
+        return qv_fail(c, QV_ERR_UNSUPPORTED, "boundary %d not supported", c->p.boundary);
+    }
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    return QV_OK;
+  };
+  int rc = launch(a, nb);
+  if (rc) return rc;
+  if (spec) {
+    // the exact root centroid (joined now, long after it finished), the fix-up
+    // of undecided root tests, and the second walk that runs only if the
+    // fix-up's list overflowed
+    if ((rc = qv_tree_finalize_root(c))) return rc;
+    k_root_fix<<<1, 256, 0, c->stream>>>(a, c->p.boundary, t.root_unc, t.root_ctl);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    WalkArgs b = a;
+    b.root_est = nullptr; b.unc = nullptr; b.unc_count = nullptr; b.unc_cap = 0;
+    b.gate = t.root_ctl + 2;
+    if ((rc = launch(b, std::min(nb, 2 * c->sm_count)))) return rc;
   }
-  QV_LAUNCH_CHECK(c);
   k_walk_reduce<<<(t.n_act + 255) / 256, 256, 0, c->stream>>>(t.n_act, nimg, t.perm, c->walk_part,
                                                                 a.gfac, c->u_li, c->u, c->u_bs);
   QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 2);
+  QV_COUNT(c, 1);
   return QV_OK;
 }
 
@@ -592,6 +676,7 @@ extern "C" int qv_field_velocity_tree(qv_ctx *c, int m, const double *pts, doubl
   int rc;
   if (!c->tree.valid)
     if ((rc = qv_launch_tree_build(c))) return rc;
+  if ((rc = qv_tree_finalize_root(c))) return rc;
   TreeBuf &t = c->tree;
   double *dp = nullptr;
   QV_CUDA(c, cudaMalloc((void **)&dp, sizeof(double) * 6 * (size_t)m));

@@ -30,6 +30,38 @@ __device__ __forceinline__ bool exact_open(double dist, const WNode64 &h, double
   return !(th < theta_tree);
 }
 
+// The root's opening test while its header holds the centroid estimate of
+// k_root_est, whose distance from the exact (sequentially summed) centroid is
+// at most delta.  Moving the centroid by delta moves dist and geo by at most
+// delta each, so the test is decided for every centroid in that ball when
+// width/(dist - geo) stays on one side of tree_theta over dist - geo +- 2 delta
+// (and width/dist over dist +- delta where dist <= geo is possible); the margin
+// also carries a relative 1e-14 for the rounding of the test itself.  A decided
+// test returns its answer.  An undecided one returns "open" (the lane walks the
+// image) and sets `unc`; the fix-up after the walk takes the exact decision and
+// drops the image's sum if the root was in fact far.  delta = 0: the header
+// holds the exact centroid and this is the reference's test.
+__device__ __forceinline__ bool root_open(const double *xi, const WNode64 &r, const double *s,
+                                          double theta, int extra, double delta, bool &unc) {
+  const double dist = exact_dist(xi, r, s);
+  const bool open = exact_open(dist, r, theta, extra);
+  if (!(delta > 0.)) return open;
+  const double m = delta + 1e-14 * (dist + r.geo + r.width);
+  bool cfar, copen;
+  if (extra) {
+    const double rl = dist - r.geo - 2. * m, rh = dist - r.geo + 2. * m;
+    cfar = rl > 0. && r.width < theta * rl;
+    copen = (rh <= 0. || r.width >= theta * rh) && (rl > 0. || r.width >= theta * (dist + m));
+  } else {
+    cfar = r.width < theta * (dist - m);
+    copen = r.width >= theta * (dist + m);
+  }
+  if (cfar) return false;
+  if (copen) return true;
+  unc = true;
+  return true;
+}
+
 __device__ __forceinline__ void cross3(const double *a, const double *b, double *c) {
   c[0] = a[1] * b[2] - a[2] * b[1];
   c[1] = a[2] * b[0] - a[0] * b[2];

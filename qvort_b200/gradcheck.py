@@ -96,15 +96,22 @@ def main(argv=None):
     ap.add_argument("--dt", type=float, default=1e-7)
     ap.add_argument("--checkpoint-every", type=int, default=16)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--smooth", action="store_true",
+                    help="smooth seeded displacement (the spacing stays near its mean)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-vs-FP64 gradient")
     a = ap.parse_args(argv)
-    w = W.trefoil_rings(seed=a.seed, n_rings=a.rings, pts_per_ring=a.pts)
+    w = W.trefoil_rings(seed=a.seed, n_rings=a.rings, pts_per_ring=a.pts, smooth=a.smooth)
     over = dict(velocity=a.velocity, tree_theta=a.theta, dt=a.dt)
-    out = {"system": f"{a.rings} trefoil rings x {a.pts} points (N={w.n})", "steps": a.steps,
-           "checkpoint_every": a.checkpoint_every, **over}
+    dtm = W.dt_max(w)
+    out = {"system": f"{a.rings} trefoil rings x {a.pts} points (N={w.n}), "
+                     f"{'smooth' if a.smooth else 'per-point'} seeded displacement",
+           "steps": a.steps, "checkpoint_every": a.checkpoint_every, **over,
+           "dt_max_at_actual_spacing": dtm, "dt_passes_timestep_check": a.dt < dtm}
     r = fd_check(w, a.steps, a.dirs, tuple(a.h), a.seed, a.checkpoint_every, **over)
     r.pop("gradient")
     out["fd"] = r
-    out["mixed_vs_fp64"] = mixed_vs_fp64(w, a.steps, a.checkpoint_every, **over)
+    if not a.no_mixed:
+        out["mixed_vs_fp64"] = mixed_vs_fp64(w, a.steps, a.checkpoint_every, **over)
     print(json.dumps(out))
 
 

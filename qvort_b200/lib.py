@@ -74,6 +74,16 @@ class QvState(C.Structure):
                                           "closest", "closestd")]
 
 
+class QvRestart(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("x", "u", "u1", "u2", "u3", "u_li", "u_bs", "gi", "gb",
+                                          "gii", "gbb", "closestd", "infront", "behind",
+                                          "closest")]
+
+
+RESTART_VEC = ("x", "u", "u1", "u2", "u3", "u_li", "u_bs", "gi", "gb", "gii", "gbb")
+RESTART_INT = ("infront", "behind", "closest")
+
+
 class QvError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"qv error {code}: {msg}")
@@ -128,15 +138,23 @@ _SIGS = {
     "qv_counters": [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                     C.POINTER(C.c_longlong)],
     "qv_probe_fp32": [_P, _D],
+    "qv_test_stage_timeout": [C.c_int],
     "qv_velocity_direct_noalloc": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, _P],
     "qv_velocity_device": [_P, _P],
     "qv_velocity_vjp": [_P, _P, _P],
     "qv_energy_grad": [_P, _P, _D, _P, _P],
+    "qv_ab_step_device": [_P, C.c_int, _P, _P, _P, _P, _P, _P],
+    "qv_ab_vjp_device": [_P, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "qv_field_velocity": [_P, C.c_int, _P, C.c_int, _P, _P],
     "qv_field_velocity_tree": [_P, C.c_int, _P, _P, C.POINTER(C.c_longlong)],
     "qv_read_run_file": [C.c_char_p, C.POINTER(QvRun)],
     "qv_read_var_file": [C.c_char_p, C.c_int, _I, _D, _P, _P, _P],
     "qv_write_var_file": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
+    "qv_write_restart_file": [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, _P],
+    "qv_read_restart_file": [C.c_char_p, C.c_int, _I, _I, _I, _D, _P],
+    "qv_dump": [_P, C.c_char_p, C.c_int, C.c_int, C.c_double],
+    "qv_restore": [_P, C.c_char_p, _I, _I, _D],
+    "qv_write_snapshot": [_P, C.c_char_p, C.c_double],
     "qv_setup_loops": [C.c_char_p, C.c_int, C.c_double, _P, _P, _P],
     "qv_pinsert": [_P, _I],
     "qv_premove": [_P, _I],
@@ -412,6 +430,20 @@ class Context:
         if self.params.line_ops:
             self._sync_count()
 
+    def dump(self, path, itime: int, t: float, recon_count: int = 0):
+        self._check(_lib.qv_dump(self._h, str(path).encode(), recon_count, itime, t))
+
+    def restore(self, path):
+        """Returns (itime, t, recon_count) of the file; the state is loaded."""
+        rcn, it, t = C.c_int(), C.c_int(), C.c_double()
+        self._check(_lib.qv_restore(self._h, str(path).encode(), C.byref(rcn), C.byref(it),
+                                    C.byref(t)))
+        self._sync_count()
+        return it.value, t.value, rcn.value
+
+    def write_snapshot(self, path, t: float):
+        self._check(_lib.qv_write_snapshot(self._h, str(path).encode(), t))
+
     def sync(self):
         self._check(_lib.qv_sync(self._h))
 
@@ -426,6 +458,16 @@ class Context:
         e = C.c_double()
         self._check(_lib.qv_energy_grad(self._h, u_ptr, C.byref(e), xbar_ptr, ubar_ptr))
         return e.value
+
+    def ab_step_device(self, x_ptr: int, u_ptr: int, u1_ptr: int, u2_ptr: int, u3_ptr: int,
+                       xo_ptr: int):
+        self._check(_lib.qv_ab_step_device(self._h, self.n, x_ptr, u_ptr, u1_ptr, u2_ptr, u3_ptr,
+                                           xo_ptr))
+
+    def ab_vjp_device(self, u1_ptr: int, u2_ptr: int, u3_ptr: int, xob_ptr: int, xb_ptr: int,
+                      ub_ptr: int, u1b_ptr: int, u2b_ptr: int, u3b_ptr: int):
+        self._check(_lib.qv_ab_vjp_device(self._h, self.n, u1_ptr, u2_ptr, u3_ptr, xob_ptr, xb_ptr,
+                                          ub_ptr, u1b_ptr, u2b_ptr, u3b_ptr))
 
     def field_velocity_tree(self, pts):
         """tree_walk_general at the given points (the mesh_velocity Tree arm)."""
@@ -495,6 +537,36 @@ def write_var_file(path, t, x, infront, u=None):
         raise QvError(rc, f"cannot write {path}")
 
 
+def write_restart_file(path, t: float, itime: int, recon_count: int = 0, **fields):
+    """data_dump's var.dat from host arrays (x, infront, behind required)."""
+    arrs = {k: (_f64(v) if k in RESTART_VEC or k == "closestd" else _i32(v))
+            for k, v in fields.items() if v is not None}
+    n = arrs["x"].shape[0]
+    r = QvRestart(*[_ptr(arrs.get(k)) for k, _ in QvRestart._fields_])
+    rc = _lib.qv_write_restart_file(str(path).encode(), n, recon_count, itime, t, C.byref(r))
+    if rc < 0:
+        raise QvError(rc, f"cannot write {path}")
+
+
+def read_restart_file(path):
+    """data_restore's read of var.dat: (t, itime, recon_count, fields)."""
+    n, rcn, it, t = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+    rc = _lib.qv_read_restart_file(str(path).encode(), 0, C.byref(n), C.byref(rcn), C.byref(it),
+                                   C.byref(t), None)
+    if rc < 0:
+        raise QvError(rc, f"cannot read {path}")
+    m = n.value
+    arrs = {k: np.empty((m, 3)) for k in RESTART_VEC}
+    arrs["closestd"] = np.empty(m)
+    arrs.update({k: np.empty(m, np.int32) for k in RESTART_INT})
+    r = QvRestart(*[_ptr(arrs[k]) for k, _ in QvRestart._fields_])
+    rc = _lib.qv_read_restart_file(str(path).encode(), m, C.byref(n), C.byref(rcn), C.byref(it),
+                                   C.byref(t), C.byref(r))
+    if rc < 0:
+        raise QvError(rc, f"{path} is not a restart file of this layout")
+    return t.value, it.value, rcn.value, arrs
+
+
 def setup_loops(initf: str, pcount: int, delta: float):
     x = np.empty((pcount, 3))
     inf = np.empty(pcount, np.int32)
@@ -503,6 +575,12 @@ def setup_loops(initf: str, pcount: int, delta: float):
     if rc < 0:
         raise QvError(rc, f"initf {initf} is outside this path")
     return x, inf, beh
+
+
+def test_stage_timeout(enable: bool) -> None:
+    """Test hook: every direct-sum source-tile wait reports that it ran out
+    (the copies still land and are drained); False restores normal waits."""
+    _lib.qv_test_stage_timeout(int(bool(enable)))
 
 
 def probe_fp32(stream: int | None = None) -> float:

@@ -118,10 +118,19 @@ def large_tangle(seed: int = 0, n_rings: int = 3000) -> Workload:
 
 def trefoil_rings(seed: int = 0, n_rings: int = 16, pts_per_ring: int = 3125,
                   radius: float = 0.01, amp: float = 5e-4, noise: float = 1e-5,
-                  box: float = 0.1) -> Workload:
+                  box: float = 0.1, smooth: bool = False) -> Workload:
     """Configuration 4: rings of radius 0.01 with an azimuthal mode-3 radial
     perturbation of amplitude amp and a seeded displacement of noise, random
-    centres and orientations in a periodic box (N = n_rings * pts_per_ring)."""
+    centres and orientations in a periodic box (N = n_rings * pts_per_ring).
+
+    smooth=False: every point is displaced independently by noise*U(-1,1) per
+    coordinate.  At 3125 points per ring (spacing 2e-5 cm) that leaves segments
+    down to ~1e-6 cm, and dt = 1e-7 s is then far beyond the reference's
+    timestep_check bound (src/initial.f90:606-622) evaluated at that spacing.
+    smooth=True: the seeded displacement is a sum of random Fourier modes 4..16
+    along each ring, scaled to a largest displacement of noise, so the spacing
+    stays within a few percent of its mean and the bound evaluated at the
+    smallest actual spacing (dt_max of this module) is ~1.8e-8 s."""
     rng = np.random.default_rng(seed)
     xs, infs, behs = [], [], []
     start = 0
@@ -132,7 +141,14 @@ def trefoil_rings(seed: int = 0, n_rings: int = 16, pts_per_ring: int = 3125,
         ang = np.pi * (2 * k - 1) / pts_per_ring
         r = radius + amp * np.cos(3 * ang)
         pts = c + r[:, None] * (np.sin(ang)[:, None] * e1 + np.cos(ang)[:, None] * e2)
-        pts = pts + noise * rng.uniform(-1.0, 1.0, pts.shape)
+        if smooth:
+            disp = np.zeros_like(pts)
+            for m in range(4, 17):
+                coef = rng.normal(size=(2, 3))
+                disp += np.cos(m * ang)[:, None] * coef[0] + np.sin(m * ang)[:, None] * coef[1]
+            pts = pts + noise * disp / np.abs(disp).max()
+        else:
+            pts = pts + noise * rng.uniform(-1.0, 1.0, pts.shape)
         xs.append(pts)
         inf, beh = _ring_links(start, pts_per_ring)
         infs.append(inf)
@@ -186,3 +202,15 @@ def batch_systems(n_systems: int = 512, seed: int = 0, nmin: int = 100, nmax: in
         w.name = f"sys{s}"
         out.append(w)
     return out
+
+
+def dt_max(w: Workload) -> float:
+    """timestep_check (src/initial.f90:606-622) with delta taken as the smallest
+    actual segment length of the system: dt_max = d^2 / |G ln(d / (pi a))|,
+    d = min segment / 2."""
+    act = np.flatnonzero(w.infront)
+    seg = np.linalg.norm(w.x[w.infront[act] - 1] - w.x[act], axis=1)
+    box = w.params.get("box_size", 0.1)
+    seg = seg[seg < box / 2]  # a segment that crosses a periodic face is short once unwrapped
+    d = seg.min() / 2.0
+    return float(d * d / abs(w.params["quant_circ"] * np.log(d / (np.pi * w.params["corea"]))))

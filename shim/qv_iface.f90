@@ -1,7 +1,8 @@
 !> ISO_C_BINDING interface to the B200 velocity-and-timestep path
 !> (include/qv.h).  A maintainer adds this module to the reference's
-!> src/Makefile and links libqvort_b200.so; the calls that replace the
-!> reference's own routines are listed in INTEGRATION.md.
+!> src/Makefile and links libqvort_b200.so.  Each wrapper below names the
+!> reference routine (file:line) whose call it replaces in src/run.f90 or
+!> src/timestep.f90.
 !>
 !> f(:) is not bind(C), so every call gathers the fields it needs into
 !> contiguous arrays and scatters results back; it never aliases the AoS.
@@ -224,8 +225,10 @@ contains
   end subroutine
 
   !> replaces ghostp + construct_tree + pmotion|pmotion_RK3 + pclose_tree|pclose
-  !> + ghostp + enforce_periodic of src/run.f90:41-84 (with pinsert, precon and
-  !> premove left to the host, see INTEGRATION.md for the ordering)
+  !> + ghostp + enforce_periodic of src/run.f90:41-84.  The parameters leave
+  !> line_ops at 0, so pinsert, precon and premove stay with the host, called
+  !> in the reference's order (pinsert after this step's update; precon and
+  !> premove after the candidate search, on recon_shots steps)
   subroutine qv_gpu_step(it)
     integer, intent(in) :: it
     integer(c_int) :: n

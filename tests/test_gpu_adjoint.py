@@ -173,3 +173,52 @@ def test_trefoil_trajectory_gradient_fd_check():
     assert r["by_h"]["1e-07"]["rel_max"] < 1e-5, r["by_h"]
     m = G.mixed_vs_fp64(w, steps=32, velocity="Tree", tree_theta=0.4)
     assert m["rel"] < 1e-5, m
+
+
+def test_ab_step_is_the_step_update_bitwise_and_its_vjp_is_the_transpose():
+    """qv_ab_step_device takes the update kernel's operations: from the same
+    positions, velocities and history it gives the positions qv_step_ab +
+    qv_enforce_periodic store, bit for bit, on every rung of the ladder.  Its
+    adjoint is the transpose of the (piecewise linear) map: <xo_bar, J d> =
+    <J^T xo_bar, d> for random directions d in (x, u, u1, u2, u3)."""
+    torch, A, L, W = _mods()
+    w, sysm = _system(W, L, A, "BS", "periodic", 0.0)
+    n = w.n
+    rng = np.random.default_rng(8)
+    hist = [rng.normal(size=(n, 3)) for _ in range(3)]
+    rung = rng.integers(1, 5, n)         # 1: Euler ... 4: AB4
+    for k in range(3):
+        hist[k][rung <= k + 1] = 0.0     # u1 = 0 for Euler, u2 = 0 for AB2, u3 = 0 for AB3
+    # the context's own update and wrap, from its own velocities
+    c = L.Context(sysm.params)
+    c.set_points(w.x, w.infront, w.behind)
+    c.set_history(*hist)
+    u = c.velocity(False)[0]
+    c.step_ab()
+    c.enforce_periodic()
+    x_ref, _ = c.get_points()
+    c.close()
+    # the differentiable step from the same inputs
+    xt = torch.tensor(w.x, device="cuda")
+    ut = torch.tensor(u, device="cuda")
+    ht = [torch.tensor(h, device="cuda") for h in hist]
+    sysm.load(xt)
+    xo = A.ab_step(xt, ut, *ht, sysm)
+    assert np.array_equal(xo.cpu().numpy(), x_ref)
+    # adjoint = transpose (steps small enough that no point crosses the box)
+    ins = [xt.clone().requires_grad_(True), ut.clone().requires_grad_(True)] + \
+          [h.clone().requires_grad_(True) for h in ht]
+    xob = torch.tensor(rng.normal(size=(n, 3)), device="cuda")
+    out = A.ab_step(*ins, sysm)
+    grads = torch.autograd.grad((out * xob).sum(), ins)
+    # a zero history entry selects the rung: perturb only the nonzero ones
+    masks = [torch.ones(n, 3, device="cuda")] * 2 + [(h != 0).double() for h in ht]
+    for _ in range(3):
+        ds = [torch.tensor(rng.normal(size=(n, 3)), device="cuda") * 1e-9 * m for m in masks]
+        with torch.no_grad():
+            jd = (A.ab_step(*[a + d for a, d in zip(ins, ds)], sysm) -
+                  A.ab_step(*[a - d for a, d in zip(ins, ds)], sysm)) / 2
+        lhs = float((xob * jd).sum())
+        rhs = float(sum((g * d).sum() for g, d in zip(grads, ds)))
+        assert abs(lhs - rhs) <= 1e-6 * abs(rhs), (lhs, rhs)
+    sysm.close()

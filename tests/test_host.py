@@ -106,3 +106,74 @@ def test_qvort_run_driver_matches_oracle(tmp_path):
         st.step()
     d = np.abs(x - st.x).max() / np.abs(st.x - x0).max()
     assert d < 1e-8, d
+
+
+def _gfortran_records(path):
+    """An independent reader of gfortran's sequential unformatted layout: the
+    payloads of the records, each checked for equal leading and trailing
+    4-byte length markers."""
+    raw = Path(path).read_bytes()
+    recs, k = [], 0
+    while k < len(raw):
+        m = int(np.frombuffer(raw[k:k + 4], np.int32)[0])
+        recs.append(raw[k + 4:k + 4 + m])
+        assert int(np.frombuffer(raw[k + 4 + m:k + 8 + m], np.int32)[0]) == m
+        k += 8 + m
+    return recs
+
+
+def test_restart_file_layout_and_round_trip(tmp_path):
+    """data_dump's var.dat (src/output.f90:272-285): seven records (pcount,
+    recon_count, itime, t, f(:), quasi_pcount, part_count) with gfortran's
+    4-byte markers, f(:) as pcount records of the 464-byte type qvort under
+    -fdefault-real-8; the reader returns every field written, bit for bit."""
+    from qvort_b200 import lib as L
+
+    rng = np.random.default_rng(4)
+    n = 37
+    f = {k: rng.normal(size=(n, 3)) for k in L.RESTART_VEC}
+    f["closestd"] = rng.uniform(size=n)
+    f["infront"] = rng.integers(0, n + 1, n).astype(np.int32)
+    f["behind"] = rng.integers(0, n + 1, n).astype(np.int32)
+    f["closest"] = rng.integers(0, n + 1, n).astype(np.int32)
+    path = tmp_path / "var.dat"
+    L.write_restart_file(path, t=1.25e-4, itime=1250, recon_count=17, **f)
+    recs = _gfortran_records(path)
+    assert len(recs) == 7
+    assert np.frombuffer(recs[0], np.int32)[0] == n
+    assert np.frombuffer(recs[1], np.int32)[0] == 17
+    assert np.frombuffer(recs[2], np.int32)[0] == 1250
+    assert np.frombuffer(recs[3], np.float64)[0] == 1.25e-4
+    assert len(recs[4]) == n * 464
+    assert np.frombuffer(recs[5], np.int32)[0] == 0 and np.frombuffer(recs[6], np.int32)[0] == 0
+    # the record type by offset: x at 0, u at 48, ghosti at 264, infront at
+    # 400, behind at 404, closest at 408, closestd at 416, delta at 440
+    e = np.frombuffer(recs[4], np.uint8).reshape(n, 464)
+    np.testing.assert_array_equal(e[:, 0:24].copy().view(np.float64), f["x"])
+    np.testing.assert_array_equal(e[:, 48:72].copy().view(np.float64), f["u"])
+    np.testing.assert_array_equal(e[:, 264:288].copy().view(np.float64), f["gi"])
+    np.testing.assert_array_equal(e[:, 400:404].copy().view(np.int32)[:, 0], f["infront"])
+    np.testing.assert_array_equal(e[:, 404:408].copy().view(np.int32)[:, 0], f["behind"])
+    np.testing.assert_array_equal(e[:, 408:412].copy().view(np.int32)[:, 0], f["closest"])
+    np.testing.assert_array_equal(e[:, 416:424].copy().view(np.float64)[:, 0], f["closestd"])
+    assert (e[:, 440:448].copy().view(np.float64) == 1.0).all()
+    t, itime, rcn, g = L.read_restart_file(path)
+    assert (t, itime, rcn) == (1.25e-4, 1250, 17)
+    for k, v in f.items():
+        np.testing.assert_array_equal(g[k], v, err_msg=k)
+
+
+def test_restart_file_rejects_a_foreign_layout(tmp_path):
+    """A var.dat whose f(:) record is not pcount * 464 bytes (another compiler
+    layout or another type) is refused."""
+    from qvort_b200 import lib as L
+
+    path = tmp_path / "var.dat"
+    with open(path, "wb") as fh:
+        for payload in (np.int32(3).tobytes(), np.int32(0).tobytes(), np.int32(5).tobytes(),
+                        np.float64(0.5).tobytes(), bytes(3 * 456), np.int32(0).tobytes(),
+                        np.int32(0).tobytes()):
+            m = np.int32(len(payload)).tobytes()
+            fh.write(m + payload + m)
+    with pytest.raises(L.QvError):
+        L.read_restart_file(path)

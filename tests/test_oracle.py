@@ -392,3 +392,18 @@ def test_loop_with_line_ops_keeps_links_consistent():
         np.testing.assert_array_equal(inf[beh[act] - 1], act + 1)
         assert (beh[inf == 0] == 0).all()
     assert done > 0
+
+
+def test_field_velocity_on_the_ring_axis_known_answer():
+    """biot_savart_general on the axis of a ring of N = 200 straight segments
+    against the circular ring's field G R^2 / (2 (R^2 + z^2)^(3/2)); the
+    polygon differs from the circle at ~(pi/N)^2."""
+    w = W.ring(200, 0.01, 0.0)
+    p = O.params(**w.params)
+    g = O.ghosts(p, w.x, w.infront, w.behind)
+    G, R = w.params["quant_circ"], 0.01
+    for z in (0.0, 0.003, -0.02):
+        u = O.field_velocity(p, w.x, w.infront, g[0], np.array([[0.0, 0.0, z]]))[0]
+        ref = G * R * R / (2 * (R * R + z * z) ** 1.5)
+        assert abs(abs(u[2]) / ref - 1) < 1e-3, (z, u, ref)
+        assert abs(u[0]) < 1e-12 * ref and abs(u[1]) < 1e-12 * ref
