@@ -356,9 +356,11 @@ int qv_test_stage_timeout(int enable);
  * device array sized for QV_NOALLOC_MAX_POINTS slots (about 9 MB, held by
  * every GPU that loads the library until exit); n above that returns
  * QV_ERR_NOALLOC_LIMIT.  The first call on a device looks up that array's
- * address (cudaGetSymbolAddress) and should come before any stream capture.
- * All calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. */
+ * address (cudaGetSymbolAddress) and should come before any stream capture;
+ * the address is kept for the life of the process, so the library must not be
+ * used on a device across a cudaDeviceReset.  Each call waits for its stream
+ * before it returns.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
 #define QV_NOALLOC_MAX_POINTS 16384
 int qv_velocity_direct_noalloc(const qv_params *p, int n, const double *x, const int *infront,
                                const int *behind, double *u_bs, void *stream);

@@ -520,6 +520,23 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
 #pragma unroll
       for (int k = 0; k < NT; k++) {
         if (jj == bi[k]) continue;  // src/timestep.f90:471, 496
+        if (PX * PY * PZ == 1) {
+          // open boundaries, the main image alone: the operations of the
+          // batched direct items (qv_batch.cu), so that a batched system is
+          // bitwise the same system run alone
+          if (jj == ii[k]) continue;
+          const float r1x = (A.x - th[k][0][1]) + (A.w - tl[k][0][1]);
+          const float r1y = (A.y - th[k][1][1]) + (B.x - tl[k][1][1]);
+          const float r1z = (A.z - th[k][2][1]) + (B.y - tl[k][2][1]);
+          const float r2x = (B.z - th[k][0][1]) + (Cc.y - tl[k][0][1]);
+          const float r2y = (B.w - th[k][1][1]) + (Cc.z - tl[k][1][1]);
+          const float r2z = (Cc.x - th[k][2][1]) + (Cc.w - tl[k][2][1]);
+          const float r1s = fmaf(r1x, r1x, fmaf(r1y, r1y, r1z * r1z));
+          float ox, oy, oz;
+          qv_seg32(r1x, r1y, r1z, r2x, r2y, r2z, sx, sy, sz, r1s, ox, oy, oz);
+          k0[k].add(ox, oy, oz);
+          continue;
+        }
         float r1x[3], r2x[3], r1y[3], r2y[3], r1z[3], r2z[3];
 #pragma unroll
         for (int s = 0; s < 3; s++) {

@@ -9,7 +9,8 @@ temporaries live in one file-scope device array of fixed size.
 The test calls it through the C ABI on device buffers, twice in a row, and
 compares each result with the u_bs that the allocating entry point
 qv_velocity returns for the same system, within the tolerances of the other
-GPU tests: 1e-10 relative (FP64) and 1e-6 RMS relative (mixed precision).
+GPU tests: 1e-10 relative (FP64) and 1e-6 RMS relative (mixed precision), for
+each boundary kind (the image sets and the ghost unwrapping differ).
 This file is collected last so that a run stopping at its first failure has
 already run every other test.
 """
@@ -27,8 +28,9 @@ def _system():
     return W.random_rings(30, 0.006, 0.012, 5e-4, 0.1, seed=21)
 
 
+@pytest.mark.parametrize("boundary", ["periodic", "open", "openx", "openxy"])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
-def test_noalloc_matches_allocating_entry_point(prec, tol):
+def test_noalloc_matches_allocating_entry_point(prec, tol, boundary):
     import torch
 
     from qvort_b200 import lib as L
@@ -36,7 +38,8 @@ def test_noalloc_matches_allocating_entry_point(prec, tol):
     w = _system()
     n = w.n
     assert 0 < n <= L.QV_NOALLOC_MAX_POINTS
-    p = L.default_params(**dict(w.params, velocity="BS", tree_theta=0.0, precision=prec))
+    p = L.default_params(**dict(w.params, velocity="BS", tree_theta=0.0, precision=prec,
+                                boundary=boundary))
     with L.Context(p) as c:
         c.set_points(w.x, w.infront, w.behind)
         _, _, ref, _ = c.velocity()
