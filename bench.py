@@ -57,6 +57,8 @@ def parse():
                     choices=["large", "tangle", "batch", "gradient", "ring", "direct"],
                     help="large: the headline line; the others print only that workload's "
                          "entry")
+    ap.add_argument("--batch-config", default=None,
+                    help="--suite batch: warps_per_block,blocks_per_sm,order instead of the tuner")
     ap.add_argument("--quick", action="store_true",
                     help="headline timing only (no comparators, e2e or CPU baseline)")
     return ap.parse_args()
@@ -640,7 +642,7 @@ def direct_rate(L, torch, steps: int = 3, warmup: int = 1) -> dict:
     return out
 
 
-def batch_rate(L, torch, steps: int = 20) -> dict:
+def batch_rate(L, torch, steps: int = 20, config=None) -> dict:
     """512 independent open systems (rings and leap-frogging pairs, N log-uniform
     in [100, 8000], dt from {5e-8, 1e-7, 2e-7}, direct below 2000 points,
     Barnes-Hut theta 0.4 above) advanced by qv_batch_step, against the same
@@ -654,7 +656,12 @@ def batch_rate(L, torch, steps: int = 20) -> dict:
                                 precision="mixed"))
     b = L.Batch(p, [(w.x, w.infront, w.behind) for w in ws], [w.params["velocity"] for w in ws],
                 [w.params["dt"] for w in ws])
-    tuned = b.tune(3)
+    if config:  # a given launch shape (warps per block, blocks per SM, order) instead of the tuner
+        b.set_config(*config)
+        tuned = {"warps_per_block": config[0], "blocks_per_sm": config[1], "order": config[2],
+                 "given": True}
+    else:
+        tuned = b.tune(3)
     u_batch = b.velocity()
     b.step(3)
     torch.cuda.synchronize()
@@ -672,18 +679,26 @@ def batch_rate(L, torch, steps: int = 20) -> dict:
         equal = equal and bool(np.array_equal(c.velocity(False)[0], u))
         ctxs.append((c, w.params["velocity"] == "Tree"))
 
-    def seq_step():
+    # the comparator: the same systems one after another, each through its own
+    # context at its fastest -- a direct system replays a CUDA graph of its step
+    # (qv_steps: one host wait for all K steps), a Barnes-Hut system runs qv_step
+    # per step (its tree build reads the node count back)
+    K = 20
+
+    def seq_steps(it0):
         for c, tree in ctxs:
             if tree:
-                c.build_tree()
-            c.velocity(False)
-            c.step_ab()
+                for k in range(K):
+                    c.step(it0 + k)
+            else:
+                c.steps(it0, K)
 
-    seq_step()
+    seq_steps(1)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(2):
-        seq_step()
-    seq_ms = (time.perf_counter() - t0) * 1e3 / 2
+    seq_steps(1 + K)
+    torch.cuda.synchronize()
+    seq_ms = (time.perf_counter() - t0) * 1e3 / K
     for c, _ in ctxs:
         c.close()
     return {"ms_per_step": ms, "system_steps_per_s": len(ws) * 1e3 / ms,
@@ -691,6 +706,9 @@ def batch_rate(L, torch, steps: int = 20) -> dict:
             "speedup_vs_sequential": seq_ms / ms, "velocities_bitwise_equal_to_sequential": equal,
             "graph": st["graph"], "tuned": tuned, "leaf_evals": st["leaf_evals"],
             "far_evals": st["far_evals"],
+            "sequential": "each system through its own context, one after another: direct "
+                          "systems replay a CUDA graph of their step (qv_steps, one wait per "
+                          f"{K} steps), Barnes-Hut systems call qv_step per step; wall clock",
             "workload": f"512 open systems, N={n_all} points ({sum(w.params['velocity'] == 'Tree' for w in ws)} "
                         "Barnes-Hut theta 0.4, the rest direct), per-system dt; pairs = sum N_s^2 "
                         "(direct-equivalent); wall clock over the graph replays"}
@@ -706,7 +724,8 @@ def main():
         from qvort_b200 import lib as L
 
         if args.suite == "batch":
-            r = batch_rate(L, torch, args.steps)
+            cfg = [int(v) for v in args.batch_config.split(",")] if args.batch_config else None
+            r = batch_rate(L, torch, args.steps, cfg)
         elif args.suite == "tangle":
             s = torch.cuda.Stream()
             r = tangle_rate(L, torch, s, torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8,

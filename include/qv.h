@@ -204,7 +204,9 @@ int qv_velocity_device(qv_ctx *ctx, double *u);
 int qv_velocity_vjp(qv_ctx *ctx, const double *u_bar, double *x_bar);
 /* energy_info (src/diagnostic.f90:259-280) for the context's positions and the
  * device velocities u, with dE/dx (explicit, through s' and the segment
- * lengths) and dE/du, device pointers (3n); energy on the host. */
+ * lengths) and dE/du, device pointers (3n); energy on the host, its per-point
+ * terms summed with compensation (qv_energy sums them in the reference's
+ * sequential order). */
 int qv_energy_grad(qv_ctx *ctx, const double *u, double *energy, double *x_bar, double *u_bar);
 /* One position update of pmotion (src/timestep.f90:48-71: the Adams-Bashforth
  * ladder, rung chosen per point by exact-zero tests of the history) followed by
@@ -342,6 +344,19 @@ int qv_probe_fp32(void *stream, double *tflops);
  * the status word, return QV_ERR_CUDA) can be exercised while every copy
  * still lands; 0 restores normal waits.  Process-wide. */
 int qv_test_stage_timeout(int enable);
+
+/* Test hook, no counterpart in the reference: how the tree's root centroid is
+ * taken.  mode -1 (the default): trees of at least 32768 slots start the
+ * build and the walk from a bounded estimate of the root centroid while its
+ * exact sequential sum runs alongside, and fix up the root tests the bound
+ * leaves undecided (results are those of the exact centroid); 0: always wait
+ * for the exact sum; 1: always start from the estimate.  bound_scale >= 1
+ * widens the estimate's bound, so that a test can make root tests undecided
+ * and exercise the fix-up.  Process-wide. */
+int qv_test_root_speculation(int mode, double bound_scale);
+/* The number of root tests the last estimate-started build left undecided
+ * (see qv_test_root_speculation; 0 when the build waited for the exact sum). */
+int qv_root_undecided(qv_ctx *ctx, int *count);
 
 /* Non-local direct Biot-Savart velocity without any device allocation.
  * No counterpart in the reference: it exists for hosts that cannot call

@@ -812,9 +812,17 @@ extern "C" int qv_energy_grad(qv_ctx *c, const double *u, double *energy, double
   QV_CUDA(c, cudaMemcpyAsync(h.data(), eterm, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
   QV_CUDA(c, cudaFree(W));
-  double e = 0.;
-  for (int i = 0; i < n; i++) e += h[i];  // the reference's sequential order
-  *energy = e * c->p.quant_circ;
+  // Neumaier-compensated sum of the per-point terms: the energy of a loss is
+  // differenced across nearby states, and a plain sequential sum's rounding
+  // (up to n u sum|t|) would dominate a difference quotient at small steps;
+  // qv_energy keeps the reference's sequential order
+  double e = 0., comp = 0.;
+  for (int i = 0; i < n; i++) {
+    const double t = e + h[i];
+    comp += fabs(e) >= fabs(h[i]) ? (e - t) + h[i] : (h[i] - t) + e;
+    e = t;
+  }
+  *energy = (e + comp) * c->p.quant_circ;
   return QV_OK;
 }
 

@@ -453,10 +453,13 @@ __device__ __forceinline__ void seg_terms(float r1s, float r2s, float dd, float 
   const float ra = rsqrtf(r1s), rb = rsqrtf(r2s);
   const float q = ra * rb;
   const float cs = dd * q;
-  float den = 1.f + cs;
-  if (cs < 0.f) den = fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
   float f = (ra + rb) * q;
-  f = den > 0.f ? __fdividef(f, den) : 0.f;
+  if (cs >= 0.f) {
+    f = __fdividef(f, 1.f + cs);  // 1 + cos >= 1
+  } else {
+    const float den = fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
+    f = den > 0.f ? __fdividef(f, den) : 0.f;
+  }
   ox = f * cx;
   oy = f * cy;
   oz = f * cz;

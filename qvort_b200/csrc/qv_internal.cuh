@@ -125,6 +125,7 @@ struct TreeBuf {
   bool root_pending = false;    // headers hold the estimate
 };
 #define QV_ROOT_UNC_CAP 8192
+#define QV_ROOT_SPEC_MIN 32768  // slots from which the root starts from its estimate
 #define QV_ROOT_EST_BLOCKS 296
 
 // Phases timed with CUDA events when profiling is on (qv_profile).
@@ -283,10 +284,13 @@ __device__ __forceinline__ void qv_seg32(float r1x, float r1y, float r1z, float 
   float cy = fmaf(r1z, sx, -r1x * sz);
   float cz = fmaf(r1x, sy, -r1y * sx);
   float cs = dd * q;
-  float den = cs >= 0.f ? 1.f + cs
-                        : fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
   float f = (ra + rb) * q;
-  f = den > 0.f ? __fdividef(f, den) : 0.f;
+  if (cs >= 0.f) {
+    f = __fdividef(f, 1.f + cs);  // 1 + cos >= 1
+  } else {
+    const float den = fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
+    f = den > 0.f ? __fdividef(f, den) : 0.f;
+  }
   ox = f * cx;
   oy = f * cy;
   oz = f * cz;

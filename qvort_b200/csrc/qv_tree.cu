@@ -976,7 +976,8 @@ __global__ void __launch_bounds__(512) k_root_cent(const int *__restrict__ d_nac
 __global__ void __launch_bounds__(256) k_root_est(const int *__restrict__ d_nact,
                                                   const int *__restrict__ act,
                                                   const double *__restrict__ x, double *xc,
-                                                  double *part, int *ctl, double *est) {
+                                                  double *part, int *ctl, double *est,
+                                                  double bound_scale) {
   const int n = *d_nact;
   double v[6] = {0., 0., 0., 0., 0., 0.};
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -1021,11 +1022,24 @@ __global__ void __launch_bounds__(256) k_root_est(const int *__restrict__ d_nact
       const double e = 2. * gam * S[3 + c] / n + 4. * u * fabs(est[c]);
       e2 += e * e;
     }
-    est[3] = sqrt(e2) * (1. + 1e-6) + 1e-300;
+    est[3] = sqrt(e2) * (1. + 1e-6) * bound_scale + 1e-300;
     ctl[0] = 0;
     ctl[2] = 0;
     ctl[3] = 0;
   }
+}
+
+// When the root's headers start from the estimate: by size (-1; trees of at
+// least QV_ROOT_SPEC_MIN slots), never (0) or always (1); and a factor on the
+// estimate's bound.  Set only by the test hook qv_test_root_speculation.
+static int g_root_spec_mode = -1;
+static double g_root_bound_scale = 1.;
+
+extern "C" int qv_test_root_speculation(int mode, double bound_scale) {
+  if (mode < -1 || mode > 1 || !(bound_scale >= 1.)) return QV_ERR_ARG;
+  g_root_spec_mode = mode;
+  g_root_bound_scale = bound_scale;
+  return QV_OK;
 }
 
 // Put the exact root centroid in (cent[0..2] and the root's headers) once its
@@ -1397,15 +1411,29 @@ int qv_launch_tree_build(qv_ctx *c) {
                          std::max(t.cap_levels, std::min(QV_MAX_DEPTH + 1, 40)))))
     return rc;
   // The root centroid (the reference's sequential sum, src/tree.f90:53-55)
-  // is a chain of n dependent FP64 adds.  It runs on a side stream over a
-  // private copy of the active positions and is joined only by the first
-  // reader of the tree after the walk's launch; the build and the walk use the
-  // bounded estimate k_root_est makes here (see root_open).
-  k_root_est<<<QV_ROOT_EST_BLOCKS, 256, 0, c->stream>>>(c->d_nact, c->act, c->x, t.root_xc,
-                                                        t.root_part, t.root_ctl, t.root_est);
-  QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 1);
-  bool chain_started = false;
+  // is a chain of n dependent FP64 adds.  On large trees it runs on a side
+  // stream over a private copy of the active positions and is joined only by
+  // the first reader of the tree after the walk's launch; the build and the
+  // walk use the bounded estimate k_root_est makes here (see root_open).  On
+  // small trees the chain is short: it starts here, beside the build (whose
+  // cooperative grid then leaves SMs free), and the packs wait for it.
+  const bool spec = g_root_spec_mode > 0 || (g_root_spec_mode < 0 && n >= QV_ROOT_SPEC_MIN);
+  if (spec) {
+    k_root_est<<<QV_ROOT_EST_BLOCKS, 256, 0, c->stream>>>(c->d_nact, c->act, c->x, t.root_xc,
+                                                          t.root_part, t.root_ctl, t.root_est,
+                                                          g_root_bound_scale);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+  } else {
+    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    QV_CUDA(c, cudaStreamWaitEvent(c->aux[1], c->ev_fork, 0));
+    k_root_cent<<<1, 512, 2 * RC * 3 * sizeof(double), c->aux[1]>>>(c->d_nact, c->act, c->x,
+                                                                     t.root_est + 4);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
+    QV_CUDA(c, cudaEventRecord(c->ev_join[1], c->aux[1]));
+  }
+  bool chain_started = !spec;
   if (!t.h_ctl) {
     QV_CUDA(c, cudaMallocHost((void **)&t.h_ctl, sizeof(int) * CTL_SIZE));
     QV_CUDA(c, cudaEventCreateWithFlags(&t.ev_ctl, cudaEventDisableTiming));
@@ -1490,7 +1518,9 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[2], 0));
-    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, t.root_est,
+    if (!spec) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
+    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk,
+                                                          spec ? t.root_est : t.root_est + 4,
                                                           t.cent);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
@@ -1522,6 +1552,17 @@ int qv_launch_tree_build(qv_ctx *c) {
     return QV_OK;
   }
   return qv_fail(c, QV_ERR_NOMEM, "tree build did not fit after repeated growth");
+}
+
+extern "C" int qv_root_undecided(qv_ctx *c, int *count) {
+  if (!c || !count) return QV_ERR_ARG;
+  *count = 0;
+  if (!c->tree.root_ctl) return QV_OK;
+  if (cudaMemcpyAsync(count, c->tree.root_ctl, sizeof(int), cudaMemcpyDeviceToHost, c->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return qv_fail(c, QV_ERR_CUDA, "qv_root_undecided: copy failed");
+  return QV_OK;
 }
 
 int qv_tree_finalize_root(qv_ctx *c) {

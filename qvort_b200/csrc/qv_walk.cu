@@ -75,7 +75,7 @@ __device__ __forceinline__ void slot_image(int bc, int s, int &ma, int &mb, int 
 
 // ---------------------------------------------------------------- FP64 walk
 template <int BC>
-__global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
+__device__ __forceinline__ void walk64_body(const WalkArgs &a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   __shared__ int2 stk[WW][STK];
   if (a.gate && *a.gate == 0) return;
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) {
 
 // ---------------------------------------------------------------- mixed walk
 template <int BC>
-__global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 blocks/SM: measured fastest (5-7 tried)
+__device__ __forceinline__ void walk32_body(const WalkArgs &a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
   extern __shared__ StkEnt stk_dyn[];
   if (a.gate && *a.gate == 0) return;
@@ -388,6 +388,19 @@ __global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) {  // 6 block
   }
 }
 
+// The walks, and the same walks under a second name for the gated relaunch
+// after an overflowing root fix-up (it returns at once unless flagged), so
+// that a profile tells the two launches apart.
+template <int BC>
+__global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) { walk64_body<BC>(a); }
+template <int BC>
+__global__ void __launch_bounds__(WW * 32) k_walk64_redo(WalkArgs a) { walk64_body<BC>(a); }
+// 6 blocks/SM: measured fastest (5-7 tried)
+template <int BC>
+__global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) { walk32_body<BC>(a); }
+template <int BC>
+__global__ void __launch_bounds__(WW * 32, 6) k_walk32_redo(WalkArgs a) { walk32_body<BC>(a); }
+
 // u_bs = main + images, u = (u_li + main) + images, with the main image summed
 // over the root's children in child order and the images in the reference's
 // loop order (src/timestep.f90:276-288).
@@ -477,18 +490,25 @@ int qv_launch_walk(qv_ctx *c) {
   bool mixed = c->p.precision == QV_PREC_MIXED;
   if (mixed && smem > 48 * 1024) {
     if (smem > c->smem_walk) {  // per context: attributes are per device
-      cudaFuncSetAttribute(k_walk32<QV_BC_OPEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(k_walk32<QV_BC_PERIODIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(k_walk32<QV_BC_OPENX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaFuncSetAttribute(k_walk32<QV_BC_OPENXY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      const void *fs[] = {(const void *)k_walk32<QV_BC_OPEN>, (const void *)k_walk32<QV_BC_PERIODIC>,
+                          (const void *)k_walk32<QV_BC_OPENX>, (const void *)k_walk32<QV_BC_OPENXY>,
+                          (const void *)k_walk32_redo<QV_BC_OPEN>,
+                          (const void *)k_walk32_redo<QV_BC_PERIODIC>,
+                          (const void *)k_walk32_redo<QV_BC_OPENX>,
+                          (const void *)k_walk32_redo<QV_BC_OPENXY>};
+      for (const void *f : fs)
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       c->smem_walk = smem;
     }
   }
   auto launch = [&](const WalkArgs &w, int grid) -> int {
+    const bool redo = w.gate != nullptr;
     switch (c->p.boundary) {
 #define QV_WALK_CASE(BCV)                                                        \
   case BCV:                                                                      \
-    if (mixed) k_walk32<BCV><<<grid, WW * 32, smem, c->stream>>>(w);             \
+    if (mixed && redo) k_walk32_redo<BCV><<<grid, WW * 32, smem, c->stream>>>(w); \
+    else if (mixed) k_walk32<BCV><<<grid, WW * 32, smem, c->stream>>>(w);        \
+    else if (redo) k_walk64_redo<BCV><<<grid, WW * 32, 0, c->stream>>>(w);       \
     else k_walk64<BCV><<<grid, WW * 32, 0, c->stream>>>(w);                      \
     break;
       QV_WALK_CASE(QV_BC_OPEN)

@@ -139,6 +139,8 @@ _SIGS = {
                     C.POINTER(C.c_longlong)],
     "qv_probe_fp32": [_P, _D],
     "qv_test_stage_timeout": [C.c_int],
+    "qv_test_root_speculation": [C.c_int, C.c_double],
+    "qv_root_undecided": [_P, _I],
     "qv_velocity_direct_noalloc": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, _P],
     "qv_velocity_device": [_P, _P],
     "qv_velocity_vjp": [_P, _P, _P],
@@ -441,6 +443,11 @@ class Context:
         self._sync_count()
         return it.value, t.value, rcn.value
 
+    def root_undecided(self) -> int:
+        k = C.c_int()
+        self._check(_lib.qv_root_undecided(self._h, C.byref(k)))
+        return k.value
+
     def write_snapshot(self, path, t: float):
         self._check(_lib.qv_write_snapshot(self._h, str(path).encode(), t))
 
@@ -581,6 +588,14 @@ def test_stage_timeout(enable: bool) -> None:
     """Test hook: every direct-sum source-tile wait reports that it ran out
     (the copies still land and are drained); False restores normal waits."""
     _lib.qv_test_stage_timeout(int(bool(enable)))
+
+
+def test_root_speculation(mode: int = -1, bound_scale: float = 1.0) -> None:
+    """Test hook: -1 by tree size (default), 0 never, 1 always start from the
+    root centroid's estimate; bound_scale widens the estimate's bound."""
+    rc = _lib.qv_test_root_speculation(int(mode), float(bound_scale))
+    if rc < 0:
+        raise QvError(rc, "bad root speculation setting")
 
 
 def probe_fp32(stream: int | None = None) -> float:

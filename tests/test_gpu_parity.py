@@ -667,3 +667,31 @@ def test_field_velocity_direct_matches_oracle(L, bc):
     uo = O.field_velocity(p, w.x, w.infront, og[0], pts)
     c.close()
     assert rel_max(u, uo) < 1e-10, rel_max(u, uo)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_root_estimate_gives_the_exact_walk(L, precision):
+    """The walk started from the root centroid's bounded estimate (while the
+    exact sequential sum runs alongside) returns the velocities and evaluation
+    counts of the walk from the exact centroid, bit for bit: with the true
+    bound (every root test decided), with a bound widened until some tests are
+    undecided (the fix-up drops the images whose root is in fact far), and
+    widened until the fix-up's list overflows (the gated second walk redoes
+    every task)."""
+    w = small_tangle()
+    c = ctx_for(L, w, precision=precision)
+    try:
+        L.test_root_speculation(0)
+        u0, _, _, ev0 = c.velocity()
+        seen = []
+        for scale in (1.0, 1e12, 1e13):
+            L.test_root_speculation(1, scale)
+            c.set_points(w.x, w.infront, w.behind)
+            u, _, _, ev = c.velocity()
+            seen.append(c.root_undecided())
+            assert np.array_equal(u, u0), scale
+            assert ev == ev0, scale
+    finally:
+        L.test_root_speculation(-1, 1.0)
+        c.close()
+    assert seen[0] == 0 and 0 < seen[1] <= 8192 < seen[2], seen
