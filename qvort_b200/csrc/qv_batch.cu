@@ -154,34 +154,31 @@ __device__ __forceinline__ void walk_item(const BatchArgs &a, StkEnt *st, int g,
         }
       }
     } else {
-      bool open = false;
-      if (in) {
-        if (h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo)) {
-          open = d2 < h.rlo;
-        } else {
-          const WNode64 h64 = a.w64[node];
-          open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
-        }
-        if (!open) {
-          ev++;
-          evf++;
-          if (node >= a.nroots) {
-            const WPay32 &P = a.p32[node];
-            float rd = rsqrtf(d2);
-            float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
-            float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
-            float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
-            float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
-            float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
-            float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
-            float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
-            float wx = fmaf(v1, z2, -v2 * z1);
-            float wy = fmaf(v2, z0, -v0 * z2);
-            float wz = fmaf(v0, z1, -v1 * z0);
-            float t5 = 3.f * rd5;
-            k0.add(fmaf(cx, rd3, wx * t5), fmaf(cy, rd3, wy * t5), fmaf(cz, rd3, wz * t5));
-          }
-        }
+      // one predicate (far) guards the far-field term, as in the single walk
+      const bool amb = in && !(h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo));
+      bool open = in && d2 < h.rlo;
+      if (amb) {
+        const WNode64 h64 = a.w64[node];
+        open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+      }
+      const bool far = in && !open;
+      ev += far ? 1u : 0u;
+      evf += far ? 1u : 0u;
+      if (far && node >= a.nroots) {  // a root's moments are zero
+        const WPay32 &P = a.p32[node];
+        float rd = rsqrtf(d2);
+        float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
+        float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
+        float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
+        float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
+        float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
+        float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
+        float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
+        float wx = fmaf(v1, z2, -v2 * z1);
+        float wy = fmaf(v2, z0, -v0 * z2);
+        float wz = fmaf(v0, z1, -v1 * z0);
+        float t5 = 3.f * rd5;
+        k0.add(fmaf(cx, rd3, wx * t5), fmaf(cy, rd3, wy * t5), fmaf(cz, rd3, wz * t5));
       }
       unsigned om = __ballot_sync(0xffffffffu, open);
       if (om) {

@@ -447,22 +447,26 @@ __global__ void __launch_bounds__(DTILE) k_direct64(int na, const int *__restric
 //
 // Pair term: the straight-segment form of qv_seg32 (src/tree.f90:380-390),
 // (1/|R1| + 1/|R2|) q / (1 + cos) (R1 x s), q = 1/(|R1||R2|), cos = R1.R2 q,
-// with 1 + cos taken from sin^2 / (1 - cos) when cos < 0.
+// with 1 + cos taken from sin^2 / (1 - cos) when cos < 0.  Both cases are
+// computed with selects and one division, without a branch: a branch per pair
+// keeps the compiler from interleaving the 27 independent image pairs of a
+// source, which costs more than the few extra multiplies.
 __device__ __forceinline__ void seg_terms(float r1s, float r2s, float dd, float cx, float cy,
                                           float cz, float &ox, float &oy, float &oz) {
   const float ra = rsqrtf(r1s), rb = rsqrtf(r2s);
   const float q = ra * rb;
   const float cs = dd * q;
-  float f = (ra + rb) * q;
-  if (cs >= 0.f) {
-    f = __fdividef(f, 1.f + cs);  // 1 + cos >= 1
-  } else {
-    const float den = fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q) / (1.f - cs);
-    f = den > 0.f ? __fdividef(f, den) : 0.f;
-  }
-  ox = f * cx;
-  oy = f * cy;
-  oz = f * cz;
+  const float f = (ra + rb) * q;
+  // one division for both signs of cos: f / (1 + cos), or, when cos < 0,
+  // f (1 - cos) / (|R1 x s|^2 q^2) (the same quotient, without cancellation)
+  const bool pos = cs >= 0.f;
+  const float s2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz)) * (q * q);
+  const float num = pos ? f : f * (1.f - cs);
+  const float den = pos ? 1.f + cs : s2;
+  const float g = den > 0.f ? __fdividef(num, den) : 0.f;
+  ox = g * cx;
+  oy = g * cy;
+  oz = g * cz;
 }
 
 template <int BC, int NT>
