@@ -1,10 +1,13 @@
 // qv_walk.cu -- Barnes-Hut tree walk of calc_velocity's Tree arm
 // (tree_walk, src/tree.f90:336-421; image loop src/timestep.f90:276-307).
 //
-// Execution model: a warp task is (32 targets adjacent in the tree's
+// Execution model: a warp task is (32 or 64 targets adjacent in the tree's
 // depth-first point order, one periodic image, and for the unshifted image one
 // of the root's children); these walks are independent, so the split gives
 // the GPU enough warps to hide latency with and keeps the longest task short.
+// The mixed walk's lanes carry two targets each in most tasks (see
+// walk_task2): one node pop then serves 64 targets, and their FP32 arithmetic
+// runs as packed pairs.
 // Each task writes per-target partial sums; a second kernel adds them in the
 // reference's order (main image by root child, then images peri,perj,perk =
 // -1..1), so results do not depend on scheduling.  The
@@ -31,6 +34,9 @@
 #define WW 4                           // warps per block
 #define STK (7 * QV_MAX_DEPTH + 16)    // stack entries per warp (FP64 walk)
 #define NSPLIT 8                       // tasks per target group for the main image
+// Active points from which the mixed walk's unshifted-image tasks carry 64
+// targets, not 32.
+#define QV_WALK_PAIR_NEAR 65536
 
 struct WalkArgs {
   int n_act;
@@ -46,6 +52,9 @@ struct WalkArgs {
   double *part;  // (NSPLIT+NIMG) x n_act x 3 partial sums, slot-major
   double L, theta, gfac;
   int extra, ngroups, stk_cap;
+  // mixed walk: groups of 64 targets, and whether the unshifted image's tasks
+  // carry 64 targets (else 32 per task, ngroups of them per slot)
+  int ng64, pair_near;
   unsigned long long *evals, *evals_far;
   int *status;
   // Root header speculation (see root_open): root_est[3] bounds the distance
@@ -214,6 +223,404 @@ __device__ __forceinline__ void walk64_body(const WalkArgs &a) {
 }
 
 // ---------------------------------------------------------------- mixed walk
+// Image shift of task slot sl (FP64), for the rare exact tests.
+__device__ __forceinline__ void slot_shift(int bc, int sl, double L, double *s) {
+  int ma, mb, mc;
+  slot_image(bc, sl, ma, mb, mc);
+  s[0] = shift_of(ma, L); s[1] = shift_of(mb, L); s[2] = shift_of(mc, L);
+}
+
+// One target of a lane's pair: its point index and links.
+struct PairTarget {
+  int i, bi, fi;  // point index (0-based), behind, infront; bi = fi = -1 if not live
+};
+
+// Leaf pair (src/tree.f90:371-391) of half H of a lane's two targets.
+template <int H>
+__device__ __forceinline__ void leaf_half(const WalkArgs &a, int bc, int sl, int node,
+                                          const WNode32 &h, const PairTarget &t,
+                                          const float2 *th, const float2 *tl, float2 v0,
+                                          float2 v1, float2 v2, float2 d2, Kahan3x2 &k,
+                                          unsigned &ev, bool &bad) {
+  const int j = h.jb;
+  if (j == t.i + 1 || j == t.bi || j == t.fi) return;
+  const float d2h = pick(d2, H);
+  bool sing = false;
+  if (d2h < 1e-20f) {
+    double s[3];
+    slot_shift(bc, sl, a.L, s);
+    const double xi[3] = {a.x[3 * t.i], a.x[3 * t.i + 1], a.x[3 * t.i + 2]};
+    sing = exact_dist(xi, a.w64[node], s) < QV_DEPS;
+  }
+  if (sing) {
+    bad = true;
+    return;
+  }
+  const WPay32 &P = a.p32[node];
+  const float r2x = (P.a[0] - pick(th[0], H)) + (P.b[0] - pick(tl[0], H));
+  const float r2y = (P.a[1] - pick(th[1], H)) + (P.b[1] - pick(tl[1], H));
+  const float r2z = (P.a[2] - pick(th[2], H)) + (P.b[2] - pick(tl[2], H));
+  float ox, oy, oz;
+  qv_seg32(-pick(v0, H), -pick(v1, H), -pick(v2, H), r2x, r2y, r2z, P.C[0], P.C[1], P.C[2], d2h,
+           ox, oy, oz);
+  k.add1<H>(ox, oy, oz);
+  ev++;
+}
+
+// The reference's FP64 opening test on an internal node for one target whose
+// FP32 test fell inside the margin.
+__device__ __forceinline__ bool exact_test(const WalkArgs &a, int bc, int sl, int node, int i,
+                                           double rdelta, bool &runc) {
+  double s[3];
+  slot_shift(bc, sl, a.L, s);
+  const double xi[3] = {a.x[3 * i], a.x[3 * i + 1], a.x[3 * i + 2]};
+  const WNode64 h64 = a.w64[node];
+  return node == 0 ? root_open(xi, h64, s, a.theta, a.extra, rdelta, runc)
+                   : exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+}
+
+// One task of one target per lane: 32 targets (group g of 32), task slot sl.
+template <int BC>
+__device__ __forceinline__ void walk_task1(const WalkArgs &a, StkEnt *st, int lane, int sl,
+                                           int g, double rdelta) {
+  int q = g * 32 + lane;
+  bool live = q < a.n_act;
+  int i = live ? a.perm[q] : 0;
+  double xi[3] = {0., 0., 0.};
+  int bi = -1, fi = -1, ii = -1;
+  if (live) {
+    xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
+    bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
+  }
+  Kahan3w k0;
+  k0.zero();
+  unsigned ev = 0, evf = 0;  // per task: far below 2^32
+  bool bad = false, runc = false;
+  int ma, mb, mc;
+  slot_image(BC, sl, ma, mb, mc);
+  const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
+  // target recentred for this image, t = x_i - shift as (hi, lo) floats
+  float th[3], tl[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    double t = xi[c] - s[c];
+    th[c] = __double2float_rn(t);
+    tl[c] = __double2float_rn(t - (double)th[c]);
+  }
+  int top = 0;
+  if (sl >= NSPLIT) {
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    if (lane == 0) {
+      st[0].h = a.w32[0];
+      st[0].node = 0;
+      st[0].mask = live_mask;
+    }
+    top = live_mask ? 1 : 0;
+  } else {
+    // unshifted image: the root's own decision, then only root child sl
+    const WNode64 r = a.w64[0];
+    bool ropen = false;
+    if (r.count == 1) {
+      const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+      if (sl == 0 && lane == 0) {
+        st[0].h = a.w32[0];
+        st[0].node = 0;
+        st[0].mask = live_mask;
+      }
+      top = (sl == 0 && live_mask) ? 1 : 0;
+    } else {
+      if (live) {
+        ropen = root_open(xi, r, s, a.theta, a.extra, rdelta, runc);
+        if (!ropen && sl == 0) { ev++; evf++; }  // root far field: zero moments
+      }
+      const unsigned om = __ballot_sync(0xffffffffu, ropen);
+      if (om && sl < r.nchild) {
+        if (lane == 0) {
+          st[0].h = a.w32[r.child_first + sl];
+          st[0].node = r.child_first + sl;
+          st[0].mask = om;
+        }
+        top = 1;
+      }
+    }
+  }
+  __syncwarp();
+  while (top > 0) {
+    top--;
+    const WNode32 h = st[top].h;
+    const int node = st[top].node;
+    const bool in = (st[top].mask >> lane) & 1u;
+    __syncwarp();
+    // v = t - cent  (= x_i - (cent + shift))
+    float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
+    float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
+    float v2 = (th[2] - h.ch[2]) + (tl[2] - h.cl[2]);
+    float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+    if (h.count == 1) {
+      if (in) {
+        int j = h.jb;
+        if (j != ii && j != bi && j != fi) {
+          bool sing = false;
+          if (d2 < 1e-20f) {
+            double dist = exact_dist(xi, a.w64[node], s);
+            sing = dist < QV_DEPS;
+          }
+          if (sing) {
+            bad = true;
+          } else {
+            const WPay32 &P = a.p32[node];
+            float r2x = (P.a[0] - th[0]) + (P.b[0] - tl[0]);
+            float r2y = (P.a[1] - th[1]) + (P.b[1] - tl[1]);
+            float r2z = (P.a[2] - th[2]) + (P.b[2] - tl[2]);
+            float ox, oy, oz;
+            qv_seg32(-v0, -v1, -v2, r2x, r2y, r2z, P.C[0], P.C[1], P.C[2], d2, ox, oy, oz);
+            k0.add(ox, oy, oz);
+            ev++;
+          }
+        }
+      }
+    } else {
+      // accept (far field) iff d^2 > rc2, decided in FP32 outside a
+      // relative margin of 4e-6 and by the reference's FP64 test inside it.
+      // One predicate (far) guards the far-field term: nested per-lane
+      // branches cost a reconvergence each on every node pop.
+      const bool amb = in && !(h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo));
+      bool open = in && d2 < h.rlo;
+      if (amb) {
+        const WNode64 h64 = a.w64[node];
+        open = node == 0 ? root_open(xi, h64, s, a.theta, a.extra, rdelta, runc)
+                         : exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+      }
+      const bool far = in && !open;
+      ev += far ? 1u : 0u;
+      evf += far ? 1u : 0u;
+      if (far && node != 0) {  // the root's moments are zero
+        const WPay32 &P = a.p32[node];
+        float rd = rsqrtf(d2);
+        float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
+        float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
+        float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
+        float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
+        float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
+        float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
+        float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
+        float wx = fmaf(v1, z2, -v2 * z1);
+        float wy = fmaf(v2, z0, -v0 * z2);
+        float wz = fmaf(v0, z1, -v1 * z0);
+        float t5 = 3.f * rd5;
+        k0.add(fmaf(cx, rd3, wx * t5), fmaf(cy, rd3, wy * t5), fmaf(cz, rd3, wz * t5));
+      }
+      unsigned om = __ballot_sync(0xffffffffu, open);
+      if (om) {
+        int nc = h.nchild;
+        if (top + nc > a.stk_cap) {  // unreachable: the cap follows the tree depth
+          bad = true;
+          nc = 0;
+        }
+        if (lane < nc) {
+          int ch = h.child_first + nc - 1 - lane;
+          StkEnt &E = st[top + lane];
+          E.h = a.w32[ch];
+          E.node = ch;
+          E.mask = om;
+        }
+        top += nc;
+      }
+      __syncwarp();
+    }
+  }
+  if (live) {
+    double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
+    o[0] = k0.get(0); o[1] = k0.get(1); o[2] = k0.get(2);
+  }
+  if (runc) note_undecided(a, q, sl, ev, evf);
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_down_sync(0xffffffffu, ev, o);
+    evf += __shfl_down_sync(0xffffffffu, evf, o);
+  }
+  if (lane == 0 && ev) atomicAdd(a.evals, (unsigned long long)ev);
+  if (lane == 0 && evf) atomicAdd(a.evals_far, (unsigned long long)evf);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, QV_STAT_SINGULAR);
+}
+
+// Each lane carries two targets of a 64-target group (q and q + 32), their
+// FP32 state as float2 pairs: one node pop serves 64 targets, and the
+// far-field term and the recentring run on the packed FP32 pipe for both.
+// Per target, every operation and its order are those of a one-target lane:
+// the warp's pops follow the depth-first order of the union of the targets'
+// walks, in which each target meets its own nodes in its own walk's order.
+template <int BC>
+__device__ __forceinline__ void walk_task2(const WalkArgs &a, StkEnt *st, int lane, int sl,
+                                           int g, double rdelta) {
+  const int qa = g * 64 + lane, qb = qa + 32;
+  const bool la = qa < a.n_act, lb = qb < a.n_act;
+  PairTarget ta = {0, -1, -1}, tb = {0, -1, -1};
+  float2 th[3], tl[3];
+  {
+    double s[3];
+    slot_shift(BC, sl, a.L, s);
+    double xa[3] = {0., 0., 0.}, xb[3] = {0., 0., 0.};
+    if (la) {
+      ta.i = a.perm[qa];
+      ta.bi = a.beh[ta.i]; ta.fi = a.inf[ta.i];
+      xa[0] = a.x[3 * ta.i]; xa[1] = a.x[3 * ta.i + 1]; xa[2] = a.x[3 * ta.i + 2];
+    }
+    if (lb) {
+      tb.i = a.perm[qb];
+      tb.bi = a.beh[tb.i]; tb.fi = a.inf[tb.i];
+      xb[0] = a.x[3 * tb.i]; xb[1] = a.x[3 * tb.i + 1]; xb[2] = a.x[3 * tb.i + 2];
+    }
+    // target recentred for this image, t = x_i - shift as (hi, lo) floats
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double ua = xa[c] - s[c], ub = xb[c] - s[c];
+      th[c].x = __double2float_rn(ua);
+      tl[c].x = __double2float_rn(ua - (double)th[c].x);
+      th[c].y = __double2float_rn(ub);
+      tl[c].y = __double2float_rn(ub - (double)th[c].y);
+    }
+  }
+  Kahan3x2 k0;
+  k0.zero();
+  unsigned eva = 0, evfa = 0, evb = 0, evfb = 0;  // per task: far below 2^32
+  bool bad = false, runa = false, runb = false;
+  int top = 0;
+  if (sl >= NSPLIT) {
+    const unsigned ma = __ballot_sync(0xffffffffu, la), mb = __ballot_sync(0xffffffffu, lb);
+    if (lane == 0) {
+      st[0].h = a.w32[0];
+      st[0].node = 0;
+      st[0].mask = ma;
+      st[0].mask2 = mb;
+    }
+    top = (ma | mb) ? 1 : 0;
+  } else {
+    // unshifted image: the root's own decision, then only root child sl
+    const WNode64 r = a.w64[0];
+    if (r.count == 1) {
+      const unsigned ma = __ballot_sync(0xffffffffu, la), mb = __ballot_sync(0xffffffffu, lb);
+      if (sl == 0 && lane == 0) {
+        st[0].h = a.w32[0];
+        st[0].node = 0;
+        st[0].mask = ma;
+        st[0].mask2 = mb;
+      }
+      top = (sl == 0 && (ma | mb)) ? 1 : 0;
+    } else {
+      bool oa = false, ob = false;
+      if (la) {
+        oa = exact_test(a, BC, sl, 0, ta.i, rdelta, runa);
+        if (!oa && sl == 0) { eva++; evfa++; }  // root far field: zero moments
+      }
+      if (lb) {
+        ob = exact_test(a, BC, sl, 0, tb.i, rdelta, runb);
+        if (!ob && sl == 0) { evb++; evfb++; }
+      }
+      const unsigned ma = __ballot_sync(0xffffffffu, oa), mb = __ballot_sync(0xffffffffu, ob);
+      if ((ma | mb) && sl < r.nchild) {
+        if (lane == 0) {
+          st[0].h = a.w32[r.child_first + sl];
+          st[0].node = r.child_first + sl;
+          st[0].mask = ma;
+          st[0].mask2 = mb;
+        }
+        top = 1;
+      }
+    }
+  }
+  __syncwarp();
+  while (top > 0) {
+    top--;
+    const WNode32 h = st[top].h;
+    const int node = st[top].node;
+    const bool ina = (st[top].mask >> lane) & 1u, inb = (st[top].mask2 >> lane) & 1u;
+    __syncwarp();
+    // v = t - cent  (= x_i - (cent + shift))
+    const float2 v0 = add2(sub2(th[0], bc2(h.ch[0])), sub2(tl[0], bc2(h.cl[0])));
+    const float2 v1 = add2(sub2(th[1], bc2(h.ch[1])), sub2(tl[1], bc2(h.cl[1])));
+    const float2 v2 = add2(sub2(th[2], bc2(h.ch[2])), sub2(tl[2], bc2(h.cl[2])));
+    const float2 d2 = fma2(v0, v0, fma2(v1, v1, mul2(v2, v2)));
+    if (h.count == 1) {
+      if (ina) leaf_half<0>(a, BC, sl, node, h, ta, th, tl, v0, v1, v2, d2, k0, eva, bad);
+      if (inb) leaf_half<1>(a, BC, sl, node, h, tb, th, tl, v0, v1, v2, d2, k0, evb, bad);
+    } else {
+      // accept (far field) iff d^2 > rc2, decided in FP32 outside a
+      // relative margin of 4e-6 and by the reference's FP64 test inside it.
+      // One predicate per target (far) guards the far-field term: nested
+      // per-lane branches cost a reconvergence each on every node pop.
+      const bool sure = h.rhi > 0.f;
+      const bool amba = ina && !(sure && (d2.x > h.rhi || d2.x < h.rlo));
+      const bool ambb = inb && !(sure && (d2.y > h.rhi || d2.y < h.rlo));
+      bool opa = ina && d2.x < h.rlo, opb = inb && d2.y < h.rlo;
+      if (amba) opa = exact_test(a, BC, sl, node, ta.i, rdelta, runa);
+      if (ambb) opb = exact_test(a, BC, sl, node, tb.i, rdelta, runb);
+      const bool fa = ina && !opa, fb = inb && !opb;
+      eva += fa ? 1u : 0u;
+      evfa += fa ? 1u : 0u;
+      evb += fb ? 1u : 0u;
+      evfb += fb ? 1u : 0u;
+      if ((fa || fb) && node != 0) {  // the root's moments are zero
+        const WPay32 &P = a.p32[node];
+        const float2 rd = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+        const float2 rd2 = mul2(rd, rd), rd3 = mul2(rd2, rd), rd5 = mul2(rd3, rd2);
+        const float2 z0 = fma2(v0, bc2(P.C[0]), fma2(v1, bc2(P.C[3]), mul2(v2, bc2(P.C[6]))));
+        const float2 z1 = fma2(v0, bc2(P.C[1]), fma2(v1, bc2(P.C[4]), mul2(v2, bc2(P.C[7]))));
+        const float2 z2 = fma2(v0, bc2(P.C[2]), fma2(v1, bc2(P.C[5]), mul2(v2, bc2(P.C[8]))));
+        const float2 cx = sub2(fma2(bc2(P.a[1]), v2, mul2(bc2(-P.a[2]), v1)), bc2(P.b[0]));
+        const float2 cy = sub2(fma2(bc2(P.a[2]), v0, mul2(bc2(-P.a[0]), v2)), bc2(P.b[1]));
+        const float2 cz = sub2(fma2(bc2(P.a[0]), v1, mul2(bc2(-P.a[1]), v0)), bc2(P.b[2]));
+        const float2 wx = fma2(v1, z2, mul2(neg2(v2), z1));
+        const float2 wy = fma2(v2, z0, mul2(neg2(v0), z2));
+        const float2 wz = fma2(v0, z1, mul2(neg2(v1), z0));
+        const float2 t5 = mul2(bc2(3.f), rd5);
+        k0.add(fma2(cx, rd3, mul2(wx, t5)), fma2(cy, rd3, mul2(wy, t5)),
+               fma2(cz, rd3, mul2(wz, t5)), fa, fb);
+      }
+      const unsigned ma = __ballot_sync(0xffffffffu, opa), mb = __ballot_sync(0xffffffffu, opb);
+      if (ma | mb) {
+        int nc = h.nchild;
+        if (top + nc > a.stk_cap) {  // unreachable: the cap follows the tree depth
+          bad = true;
+          nc = 0;
+        }
+        if (lane < nc) {
+          const int ch = h.child_first + nc - 1 - lane;
+          StkEnt &E = st[top + lane];
+          E.h = a.w32[ch];
+          E.node = ch;
+          E.mask = ma;
+          E.mask2 = mb;
+        }
+        top += nc;
+      }
+      __syncwarp();
+    }
+  }
+  if (la) {
+    double *o = a.part + ((size_t)sl * a.n_act + qa) * 3;
+    o[0] = k0.get(0, 0); o[1] = k0.get(0, 1); o[2] = k0.get(0, 2);
+  }
+  if (lb) {
+    double *o = a.part + ((size_t)sl * a.n_act + qb) * 3;
+    o[0] = k0.get(1, 0); o[1] = k0.get(1, 1); o[2] = k0.get(1, 2);
+  }
+  if (runa) note_undecided(a, qa, sl, eva, evfa);
+  if (runb) note_undecided(a, qb, sl, evb, evfb);
+  unsigned ev = eva + evb, evf = evfa + evfb;
+  for (int o = 16; o > 0; o >>= 1) {
+    ev += __shfl_down_sync(0xffffffffu, ev, o);
+    evf += __shfl_down_sync(0xffffffffu, evf, o);
+  }
+  if (lane == 0 && ev) atomicAdd(a.evals, (unsigned long long)ev);
+  if (lane == 0 && evf) atomicAdd(a.evals_far, (unsigned long long)evf);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, QV_STAT_SINGULAR);
+}
+
+// Tasks in order: the unshifted image's (heaviest first), then the images'.
+// Image tasks carry 64 targets (two per lane); the unshifted image's carry 64
+// when the system is large and 32 (one per lane) otherwise, which halves the
+// longest task when there are few tasks per warp.  Either kind computes, per
+// target, the same sums bit for bit.
 template <int BC>
 __device__ __forceinline__ void walk32_body(const WalkArgs &a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
@@ -222,167 +629,17 @@ __device__ __forceinline__ void walk32_body(const WalkArgs &a) {
   const double rdelta = a.root_est ? a.root_est[3] : 0.;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   StkEnt *st = stk_dyn + wid * a.stk_cap;
-  const int items = a.ngroups * (NSPLIT + NIMG);
+  const int near1 = a.pair_near ? 0 : NSPLIT * a.ngroups;  // one-target tasks
+  const int s0 = a.pair_near ? 0 : NSPLIT;                 // first slot of the paired tasks
+  const int items = near1 + (NSPLIT + NIMG - s0) * a.ng64;
   for (int item = blockIdx.x * WW + wid; item < items; item += gridDim.x * WW) {
-    const int sl = item / a.ngroups, g = item - sl * a.ngroups;
-    int q = g * 32 + lane;
-    bool live = q < a.n_act;
-    int i = live ? a.perm[q] : 0;
-    double xi[3] = {0., 0., 0.};
-    int bi = -1, fi = -1, ii = -1;
-    if (live) {
-      xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
-      bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
-    }
-    Kahan3w k0;
-    k0.zero();
-    unsigned ev = 0, evf = 0;  // per task: far below 2^32
-    bool bad = false, runc = false;
-    int ma, mb, mc;
-    slot_image(BC, sl, ma, mb, mc);
-    const double s[3] = {shift_of(ma, a.L), shift_of(mb, a.L), shift_of(mc, a.L)};
-    // target recentred for this image, t = x_i - shift as (hi, lo) floats
-    float th[3], tl[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      double t = xi[c] - s[c];
-      th[c] = __double2float_rn(t);
-      tl[c] = __double2float_rn(t - (double)th[c]);
-    }
-    int top = 0;
-    if (sl >= NSPLIT) {
-      const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-      if (lane == 0) {
-        st[0].h = a.w32[0];
-        st[0].node = 0;
-        st[0].mask = live_mask;
-      }
-      top = live_mask ? 1 : 0;
+    if (item < near1) {
+      const int sl = item / a.ngroups;
+      walk_task1<BC>(a, st, lane, sl, item - sl * a.ngroups, rdelta);
     } else {
-      // unshifted image: the root's own decision, then only root child sl
-      const WNode64 r = a.w64[0];
-      bool ropen = false;
-      if (r.count == 1) {
-        const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-        if (sl == 0 && lane == 0) {
-          st[0].h = a.w32[0];
-          st[0].node = 0;
-          st[0].mask = live_mask;
-        }
-        top = (sl == 0 && live_mask) ? 1 : 0;
-      } else {
-        if (live) {
-          ropen = root_open(xi, r, s, a.theta, a.extra, rdelta, runc);
-          if (!ropen && sl == 0) { ev++; evf++; }  // root far field: zero moments
-        }
-        const unsigned om = __ballot_sync(0xffffffffu, ropen);
-        if (om && sl < r.nchild) {
-          if (lane == 0) {
-            st[0].h = a.w32[r.child_first + sl];
-            st[0].node = r.child_first + sl;
-            st[0].mask = om;
-          }
-          top = 1;
-        }
-      }
+      const int j = item - near1, k = j / a.ng64;
+      walk_task2<BC>(a, st, lane, s0 + k, j - k * a.ng64, rdelta);
     }
-    __syncwarp();
-    while (top > 0) {
-      top--;
-      const WNode32 h = st[top].h;
-      const int node = st[top].node;
-      const bool in = (st[top].mask >> lane) & 1u;
-      __syncwarp();
-      // v = t - cent  (= x_i - (cent + shift))
-      float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
-      float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
-      float v2 = (th[2] - h.ch[2]) + (tl[2] - h.cl[2]);
-      float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
-      if (h.count == 1) {
-        if (in) {
-          int j = h.jb;
-          if (j != ii && j != bi && j != fi) {
-            bool sing = false;
-            if (d2 < 1e-20f) {
-              double dist = exact_dist(xi, a.w64[node], s);
-              sing = dist < QV_DEPS;
-            }
-            if (sing) {
-              bad = true;
-            } else {
-              const WPay32 &P = a.p32[node];
-              float r2x = (P.a[0] - th[0]) + (P.b[0] - tl[0]);
-              float r2y = (P.a[1] - th[1]) + (P.b[1] - tl[1]);
-              float r2z = (P.a[2] - th[2]) + (P.b[2] - tl[2]);
-              float ox, oy, oz;
-              qv_seg32(-v0, -v1, -v2, r2x, r2y, r2z, P.C[0], P.C[1], P.C[2], d2, ox, oy, oz);
-              k0.add(ox, oy, oz);
-              ev++;
-            }
-          }
-        }
-      } else {
-        // accept (far field) iff d^2 > rc2, decided in FP32 outside a
-        // relative margin of 4e-6 and by the reference's FP64 test inside it.
-        // One predicate (far) guards the far-field term: nested per-lane
-        // branches cost a reconvergence each on every node pop.
-        const bool amb = in && !(h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo));
-        bool open = in && d2 < h.rlo;
-        if (amb) {
-          const WNode64 h64 = a.w64[node];
-          open = node == 0 ? root_open(xi, h64, s, a.theta, a.extra, rdelta, runc)
-                           : exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
-        }
-        const bool far = in && !open;
-        ev += far ? 1u : 0u;
-        evf += far ? 1u : 0u;
-        if (far && node != 0) {  // the root's moments are zero
-          const WPay32 &P = a.p32[node];
-          float rd = rsqrtf(d2);
-          float rd2 = rd * rd, rd3 = rd2 * rd, rd5 = rd3 * rd2;
-          float z0 = fmaf(v0, P.C[0], fmaf(v1, P.C[3], v2 * P.C[6]));
-          float z1 = fmaf(v0, P.C[1], fmaf(v1, P.C[4], v2 * P.C[7]));
-          float z2 = fmaf(v0, P.C[2], fmaf(v1, P.C[5], v2 * P.C[8]));
-          float cx = fmaf(P.a[1], v2, -P.a[2] * v1) - P.b[0];
-          float cy = fmaf(P.a[2], v0, -P.a[0] * v2) - P.b[1];
-          float cz = fmaf(P.a[0], v1, -P.a[1] * v0) - P.b[2];
-          float wx = fmaf(v1, z2, -v2 * z1);
-          float wy = fmaf(v2, z0, -v0 * z2);
-          float wz = fmaf(v0, z1, -v1 * z0);
-          float t5 = 3.f * rd5;
-          k0.add(fmaf(cx, rd3, wx * t5), fmaf(cy, rd3, wy * t5), fmaf(cz, rd3, wz * t5));
-        }
-        unsigned om = __ballot_sync(0xffffffffu, open);
-        if (om) {
-          int nc = h.nchild;
-          if (top + nc > a.stk_cap) {  // unreachable: the cap follows the tree depth
-            bad = true;
-            nc = 0;
-          }
-          if (lane < nc) {
-            int ch = h.child_first + nc - 1 - lane;
-            StkEnt &E = st[top + lane];
-            E.h = a.w32[ch];
-            E.node = ch;
-            E.mask = om;
-          }
-          top += nc;
-        }
-        __syncwarp();
-      }
-    }
-    if (live) {
-      double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
-      o[0] = k0.get(0); o[1] = k0.get(1); o[2] = k0.get(2);
-    }
-    if (runc) note_undecided(a, q, sl, ev, evf);
-    for (int o = 16; o > 0; o >>= 1) {
-      ev += __shfl_down_sync(0xffffffffu, ev, o);
-      evf += __shfl_down_sync(0xffffffffu, evf, o);
-    }
-    if (lane == 0 && ev) atomicAdd(a.evals, (unsigned long long)ev);
-    if (lane == 0 && evf) atomicAdd(a.evals_far, (unsigned long long)evf);
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, QV_STAT_SINGULAR);
   }
 }
 
@@ -393,11 +650,11 @@ template <int BC>
 __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) { walk64_body<BC>(a); }
 template <int BC>
 __global__ void __launch_bounds__(WW * 32) k_walk64_redo(WalkArgs a) { walk64_body<BC>(a); }
-// 6 blocks/SM: measured fastest (5-7 tried)
+// 5 blocks/SM (96 registers): faster than 4 (111 registers) on the paired tasks
 template <int BC>
-__global__ void __launch_bounds__(WW * 32, 6) k_walk32(WalkArgs a) { walk32_body<BC>(a); }
+__global__ void __launch_bounds__(WW * 32, 5) k_walk32(WalkArgs a) { walk32_body<BC>(a); }
 template <int BC>
-__global__ void __launch_bounds__(WW * 32, 6) k_walk32_redo(WalkArgs a) { walk32_body<BC>(a); }
+__global__ void __launch_bounds__(WW * 32, 5) k_walk32_redo(WalkArgs a) { walk32_body<BC>(a); }
 
 // u_bs = main + images, u = (u_li + main) + images, with the main image summed
 // over the root's children in child order and the images in the reference's
@@ -478,14 +735,18 @@ int qv_launch_walk(qv_ctx *c) {
     a.root_est = t.root_est; a.unc = t.root_unc; a.unc_count = t.root_ctl;
     a.unc_cap = QV_ROOT_UNC_CAP;
   }
+  const bool mixed = c->p.precision == QV_PREC_MIXED;
   a.ngroups = (t.n_act + 31) / 32;
+  a.ng64 = (t.n_act + 63) / 64;
+  a.pair_near = t.n_act >= QV_WALK_PAIR_NEAR;
   // a depth-first stack over a tree of depth D never holds more than 7 D + 1
   // entries (each open pushes at most 8 and pops 1)
   a.stk_cap = 7 * (t.depth + 1) + 8;
   size_t smem = sizeof(StkEnt) * a.stk_cap * WW;
   long items = (long)a.ngroups * (NSPLIT + nimg);
+  if (mixed) items = (a.pair_near ? 0L : (long)NSPLIT * a.ngroups) +
+                     (long)a.ng64 * (nimg + (a.pair_near ? NSPLIT : 0));
   int nb = (int)std::min<long>((items + WW - 1) / WW, 64L * c->sm_count);
-  bool mixed = c->p.precision == QV_PREC_MIXED;
   if (mixed && smem > 48 * 1024) {
     if (smem > c->smem_walk) {  // per context: attributes are per device
       const void *fs[] = {(const void *)k_walk32<QV_BC_OPEN>, (const void *)k_walk32<QV_BC_PERIODIC>,

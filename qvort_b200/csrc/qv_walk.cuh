@@ -3,6 +3,7 @@
 // (src/tree.f90:350-365, 394), the compensated FP32 accumulator and the
 // stack entry of the mixed-precision walk.
 #pragma once
+#include "qv_f32x2.cuh"
 #include "qv_internal.cuh"
 
 __device__ __forceinline__ double shift_of(int m, double L) {
@@ -87,12 +88,56 @@ struct Kahan3w {
   __device__ __forceinline__ double get(int k) const { return (double)s[k] - (double)c[k]; }
 };
 
+// Kahan3w for two targets at once: (s, c) hold target a in .x and target b
+// in .y.  add() applies the scalar update's operations to both halves and
+// keeps the new values only where the half's flag is set, so each half goes
+// through exactly the sequence of updates a Kahan3w of its own would.
+struct Kahan3x2 {
+  float2 s[3], c[3];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 3; k++) s[k] = c[k] = make_float2(0.f, 0.f);
+  }
+  __device__ __forceinline__ void add(float2 a0, float2 a1, float2 a2, bool fx, bool fy) {
+    const float2 a[3] = {a0, a1, a2};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float2 y = sub2(a[k], c[k]);
+      const float2 t = add2(s[k], y);
+      const float2 cn = sub2(sub2(t, s[k]), y);
+      s[k].x = fx ? t.x : s[k].x;
+      s[k].y = fy ? t.y : s[k].y;
+      c[k].x = fx ? cn.x : c[k].x;
+      c[k].y = fy ? cn.y : c[k].y;
+    }
+  }
+  // half H alone (a leaf pair of one of the two targets)
+  template <int H>
+  __device__ __forceinline__ void add1(float a0, float a1, float a2) {
+    const float a[3] = {a0, a1, a2};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float &sk = H ? s[k].y : s[k].x;
+      float &ck = H ? c[k].y : c[k].x;
+      const float y = __fsub_rn(a[k], ck);
+      const float t = __fadd_rn(sk, y);
+      ck = __fsub_rn(__fsub_rn(t, sk), y);
+      sk = t;
+    }
+  }
+  __device__ __forceinline__ double get(int h, int k) const {
+    return (double)pick(s[k], h) - (double)pick(c[k], h);
+  }
+};
+
 // Stack entry: the child's FP32 header, fetched when the child is pushed so
-// that popping it costs a shared-memory read instead of a dependent global load.
+// that popping it costs a shared-memory read instead of a dependent global load,
+// and the lane masks of the targets that opened the parent (mask: the warp's
+// first 32 targets; mask2: the second 32 where a lane carries two).
 struct __align__(16) StkEnt {
   WNode32 h;
   int node;
-  unsigned mask;
-  int pad[2];
+  unsigned mask, mask2;
+  int pad;
 };
 
