@@ -94,10 +94,11 @@ const char *qv_last_error(const qv_ctx *ctx);
 
 /* Gather of f(:)%x, f(:)%infront, f(:)%behind into the context (host
  * pointers).  Resets the AB history and closest to zero.  The links are
- * checked on the host before anything is uploaded (this, qv_set_state and
- * qv_step_exchange): every infront/behind (and closest, where given) in 0..n,
- * and an active slot linking forwards and backwards to active slots;
- * otherwise QV_ERR_ARG and nothing runs. */
+ * checked before the context takes anything (this, qv_set_state and
+ * qv_step_exchange): they are uploaded to a staging buffer and a kernel tests
+ * every infront/behind (and closest, where given) in 0..n, and an active slot
+ * linking forwards and backwards to active slots; otherwise QV_ERR_ARG naming
+ * the first offending slot, and the context's state is as it was. */
 int qv_set_points(qv_ctx *ctx, int n, const double *x, const int *infront, const int *behind);
 /* The same from device pointers (the torch harness); the links are the
  * caller's device arrays and are not checked. */

@@ -145,9 +145,14 @@ extern "C" int qv_destroy(qv_ctx *c) {
       if (q) cudaFree(q);
   }
   if (c->line_host) cudaFreeHost(c->line_host);
+  if (c->line_clr) cudaFree(c->line_clr);
+  if (c->h_clr) cudaFreeHost(c->h_clr);
+  if (c->ev_pins) cudaEventDestroy(c->ev_pins);
   if (c->h_stat) cudaFreeHost(c->h_stat);
   if (c->ev_line) cudaEventDestroy(c->ev_line);
   if (c->walk_part) cudaFree(c->walk_part);
+  if (c->lk) cudaFree(c->lk);
+  if (c->h_lk) cudaFreeHost(c->h_lk);
   for (int k = 0; k < 3; k++) {
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     if (c->ev_join[k]) cudaEventDestroy(c->ev_join[k]);
@@ -244,33 +249,70 @@ int qv_grow_points(qv_ctx *c, int new_cap) {
 // f(infront)/f(behind) (ghosts, derivatives, tree leaves, line operations) and
 // f(closest) (reconnection) without further checks, so an input that breaks
 // these rules is refused here with QV_ERR_ARG and nothing runs.
-static int check_links(qv_ctx *c, int n, const int *inf, const int *beh, const int *closest,
+// The host's links are uploaded to a staging buffer and checked there before
+// the context takes them: res[0] = first slot with an infront or behind
+// outside 0..n, res[1] = first active slot that links to an empty slot (tested
+// only where both links are in range, so inf[a - 1] and inf[b - 1] stay in the
+// array), res[2] = first slot with a closest outside 0..n.  atomicMin keeps the
+// lowest slot, so the verdict names the slot a sequential scan would meet
+// first; 0x7f7f7f7f (above any slot) means none.
+__global__ void k_check_links(int n, const int *__restrict__ inf, const int *__restrict__ beh,
+                              const int *__restrict__ closest, int *res) {
+  const unsigned un = (unsigned)n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = inf[i], b = beh[i];
+    if ((unsigned)a > un || (unsigned)b > un) atomicMin(&res[0], i);
+    else if (a != 0 && (b == 0 || inf[a - 1] == 0 || inf[b - 1] == 0)) atomicMin(&res[1], i);
+    if (closest && (unsigned)closest[i] > un) atomicMin(&res[2], i);
+  }
+}
+
+// Stage infront, behind (and closest, if given) of n slots and check them:
+// every link in 0..n, an active slot linking forwards and backwards to active
+// slots, every closest in 0..n.  One wait.  On success the staged arrays are
+// at c->lk (infront), c->lk + n (behind), c->lk + 2 n (closest); the
+// context's own state is not touched either way.
+static int stage_links(qv_ctx *c, int n, const int *inf, const int *beh, const int *closest,
                        const char *who) {
-  for (int i = 0; i < n; i++) {
-    const int a = inf[i], b = beh[i];
-    if (a < 0 || a > n || b < 0 || b > n)
-      return qv_fail(c, QV_ERR_ARG, "%s: slot %d has infront %d, behind %d, outside 0..%d", who,
-                     i + 1, a, b, n);
+  const size_t need = 3 * (size_t)n + 4;
+  if (need > c->lk_ints) {
+    int rc = qv_grow(c, (void **)&c->lk, sizeof(int) * need);
+    if (rc) return rc;
+    c->lk_ints = need;
   }
-  for (int i = 0; i < n; i++) {
-    const int a = inf[i], b = beh[i];
-    if (a != 0 && (b == 0 || inf[a - 1] == 0 || inf[b - 1] == 0))
-      return qv_fail(c, QV_ERR_ARG, "%s: active slot %d links to an empty slot (infront %d, behind %d)",
-                     who, i + 1, a, b);
-  }
-  if (closest)
-    for (int i = 0; i < n; i++)
-      if (closest[i] < 0 || closest[i] > n)
-        return qv_fail(c, QV_ERR_ARG, "%s: slot %d has closest %d, outside 0..%d", who, i + 1,
-                       closest[i], n);
+  if (!c->h_lk) QV_CUDA(c, cudaHostAlloc((void **)&c->h_lk, 4 * sizeof(int), cudaHostAllocDefault));
+  int *d_inf = c->lk, *d_beh = c->lk + n, *d_cl = c->lk + 2 * (size_t)n, *d_res = c->lk + 3 * (size_t)n;
+  const size_t ni = sizeof(int) * (size_t)n;
+  const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+  QV_CUDA(c, cudaMemcpyAsync(d_inf, inf, ni, h2d, c->stream));
+  QV_CUDA(c, cudaMemcpyAsync(d_beh, beh, ni, h2d, c->stream));
+  if (closest) QV_CUDA(c, cudaMemcpyAsync(d_cl, closest, ni, h2d, c->stream));
+  QV_CUDA(c, cudaMemsetAsync(d_res, 0x7f, 3 * sizeof(int), c->stream));
+  const int grid = (int)std::min<long>((n + 255) / 256, 4L * c->sm_count);
+  k_check_links<<<grid, 256, 0, c->stream>>>(n, d_inf, d_beh, closest ? d_cl : nullptr, d_res);
+  QV_LAUNCH_CHECK(c);
+  QV_COUNT(c, 1);
+  QV_CUDA(c, cudaMemcpyAsync(c->h_lk, d_res, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int *r = c->h_lk;
+  if (r[0] < n)
+    return qv_fail(c, QV_ERR_ARG, "%s: slot %d has infront %d, behind %d, outside 0..%d", who,
+                   r[0] + 1, inf[r[0]], beh[r[0]], n);
+  if (r[1] < n)
+    return qv_fail(c, QV_ERR_ARG, "%s: active slot %d links to an empty slot (infront %d, behind %d)",
+                   who, r[1] + 1, inf[r[1]], beh[r[1]]);
+  if (closest && r[2] < n)
+    return qv_fail(c, QV_ERR_ARG, "%s: slot %d has closest %d, outside 0..%d", who, r[2] + 1,
+                   closest[r[2]], n);
   return QV_OK;
 }
 
 static int set_points_impl(qv_ctx *c, int n, const double *x, const int *inf, const int *beh,
                            cudaMemcpyKind kind) {
   if (n < 0 || (n > 0 && (!x || !inf || !beh))) return qv_fail(c, QV_ERR_ARG, "bad points");
-  if (kind == cudaMemcpyHostToDevice && n > 0) {
-    int rc0 = check_links(c, n, inf, beh, nullptr, "qv_set_points");
+  const bool host = kind == cudaMemcpyHostToDevice;
+  if (host && n > 0) {
+    int rc0 = stage_links(c, n, inf, beh, nullptr, "qv_set_points");
     if (rc0) return rc0;
   }
   int rc = reserve_points(c, std::max(n, 1));
@@ -279,8 +321,9 @@ static int set_points_impl(qv_ctx *c, int n, const double *x, const int *inf, co
   if (n > 0) {
     size_t v = sizeof(double) * 3 * (size_t)n;
     QV_CUDA(c, cudaMemcpyAsync(c->x, x, v, kind, c->stream));
-    QV_CUDA(c, cudaMemcpyAsync(c->infront, inf, sizeof(int) * n, kind, c->stream));
-    QV_CUDA(c, cudaMemcpyAsync(c->behind, beh, sizeof(int) * n, kind, c->stream));
+    const cudaMemcpyKind lk = host ? cudaMemcpyDeviceToDevice : kind;
+    QV_CUDA(c, cudaMemcpyAsync(c->infront, host ? c->lk : inf, sizeof(int) * n, lk, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->behind, host ? c->lk + n : beh, sizeof(int) * n, lk, c->stream));
     double *zv[] = {c->u, c->u1, c->u2, c->u3, c->u_li, c->u_bs};
     for (double *q : zv) QV_CUDA(c, cudaMemsetAsync(q, 0, v, c->stream));
     QV_CUDA(c, cudaMemsetAsync(c->closest, 0, sizeof(int) * n, c->stream));
@@ -362,7 +405,7 @@ extern "C" int qv_set_state(qv_ctx *c, int n, const qv_state *s) {
   QV_CHECK_CTX(c);
   if (!s || n < 0 || (n > 0 && (!s->x || !s->infront || !s->behind)))
     return qv_fail(c, QV_ERR_ARG, "qv_set_state: x, infront and behind are required");
-  int rc = n > 0 ? check_links(c, n, s->infront, s->behind, s->closest, "qv_set_state") : QV_OK;
+  int rc = n > 0 ? stage_links(c, n, s->infront, s->behind, s->closest, "qv_set_state") : QV_OK;
   if (rc) return rc;
   rc = reserve_points(c, std::max(n, 1));
   if (rc) return rc;
@@ -370,16 +413,18 @@ extern "C" int qv_set_state(qv_ctx *c, int n, const qv_state *s) {
   if (n > 0) {
     const size_t v = sizeof(double) * 3 * (size_t)n;
     const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
+    const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
     QV_CUDA(c, cudaMemcpyAsync(c->x, s->x, v, h2d, c->stream));
-    QV_CUDA(c, cudaMemcpyAsync(c->infront, s->infront, sizeof(int) * n, h2d, c->stream));
-    QV_CUDA(c, cudaMemcpyAsync(c->behind, s->behind, sizeof(int) * n, h2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->infront, c->lk, sizeof(int) * n, d2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->behind, c->lk + n, sizeof(int) * n, d2d, c->stream));
     const double *hs[] = {s->u1, s->u2, s->u3};
     double *hd[] = {c->u1, c->u2, c->u3};
     for (int k = 0; k < 3; k++) {
       if (hs[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], hs[k], v, h2d, c->stream));
       else QV_CUDA(c, cudaMemsetAsync(hd[k], 0, v, c->stream));
     }
-    if (s->closest) QV_CUDA(c, cudaMemcpyAsync(c->closest, s->closest, sizeof(int) * n, h2d, c->stream));
+    if (s->closest)
+      QV_CUDA(c, cudaMemcpyAsync(c->closest, c->lk + 2 * (size_t)n, sizeof(int) * n, d2d, c->stream));
     else QV_CUDA(c, cudaMemsetAsync(c->closest, 0, sizeof(int) * n, c->stream));
     double *zv[] = {c->u, c->u_li, c->u_bs};
     for (double *q : zv) QV_CUDA(c, cudaMemsetAsync(q, 0, v, c->stream));
@@ -748,9 +793,11 @@ static int wait_pending_inputs(qv_ctx *c) {
 typedef int (*step_hook)(qv_ctx *c, void *arg);
 
 // One run.f90 step, queued (the host waits inside only for pinsert's new slot
-// count and the tree's node count); `after_lines`, if given, runs once the
-// line operations are queued, before the closing ghosts and wrap.
-static int step_body(qv_ctx *c, int itime, step_hook after_lines, void *arg) {
+// count and the tree's node count); `after_insert`, if given, runs once that
+// count is known (pinsert not resumed), `after_lines` once the line operations
+// are queued, before the closing ghosts and wrap.
+static int step_body(qv_ctx *c, int itime, step_hook after_lines, void *arg,
+                     step_hook after_insert = nullptr) {
   int rc;
   qv_phase_begin(c, PH_GHOSTS);
   if ((rc = qv_launch_ghosts(c))) return rc;                     // run.f90:41
@@ -792,6 +839,8 @@ static int step_body(qv_ctx *c, int itime, step_hook after_lines, void *arg) {
     if ((rc = qv_line_insert_finish(c, nullptr, &resumed))) return rc;
     qv_phase_end(c, PH_LINE);
     if (resumed) searched = false;
+    if (after_insert && !resumed)
+      if ((rc = after_insert(c, arg))) return rc;
   }
   if (search) {                                                  // run.f90:63-69
     if (!searched) {
@@ -829,7 +878,30 @@ struct ExchangeOut {
   int cap;
   qv_state *out;
   bool over = false, queued = false;
+  bool early = false;  // u and the history went out behind pinsert
+  int n_early = 0;     // the slot count they covered
 };
+
+// Once pinsert's slot count is known, u and the AB history are final except in
+// the slots that reconnection and premove clear (clear_particle zeroes u, u1
+// and u2 there and keeps u3): copy them out now, on a side stream behind
+// pinsert, while the candidate search and the other line operations run.  The
+// cleared slots, logged on the device, are zeroed on the host at the end.
+static int exchange_insert_hook(qv_ctx *c, void *arg) {
+  ExchangeOut *o = (ExchangeOut *)arg;
+  if (c->n > o->cap || c->n == 0 || !c->ev_pins) return QV_OK;
+  const size_t v = sizeof(double) * 3 * (size_t)c->n;
+  cudaStream_t sa = c->aux[2];
+  QV_CUDA(c, cudaStreamWaitEvent(sa, c->ev_pins, 0));
+  qv_state *s = o->out;
+  double *hd[] = {s->u, s->u1, s->u2, s->u3};
+  const double *dd[] = {c->u, c->u1, c->u2, c->u3};
+  for (int k = 0; k < 4; k++)
+    if (hd[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], dd[k], v, cudaMemcpyDeviceToHost, sa));
+  o->early = true;
+  o->n_early = c->n;
+  return QV_OK;
+}
 
 // After the line operations every array but x is final: copy those out on a
 // side stream while the closing ghosts and wrap run.
@@ -840,15 +912,18 @@ static int exchange_out_hook(qv_ctx *c, void *arg) {
     return QV_OK;
   }
   if (c->n == 0) return QV_OK;
+  if (o->early && c->n != o->n_early) o->early = false;  // copy them again below
   const size_t v = sizeof(double) * 3 * (size_t)c->n, ni = sizeof(int) * (size_t)c->n;
   const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
   cudaStream_t sa = c->aux[2];
+  int rc;
+  if (o->early && (rc = qv_line_clear_log_queue(c))) return rc;
   QV_CUDA(c, cudaEventRecord(c->ev_fork2, c->stream));
   QV_CUDA(c, cudaStreamWaitEvent(sa, c->ev_fork2, 0));
   qv_state *s = o->out;
   double *hd[] = {s->u, s->u1, s->u2, s->u3};
   const double *dd[] = {c->u, c->u1, c->u2, c->u3};
-  for (int k = 0; k < 4; k++)
+  for (int k = 0; k < 4 && !o->early; k++)
     if (hd[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], dd[k], v, d2h, sa));
   if (s->infront) QV_CUDA(c, cudaMemcpyAsync(s->infront, c->infront, ni, d2h, sa));
   if (s->behind) QV_CUDA(c, cudaMemcpyAsync(s->behind, c->behind, ni, d2h, sa));
@@ -866,7 +941,7 @@ extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in,
   if (!in || !out || !n_out || n < 0 || (n > 0 && (!in->x || !in->infront || !in->behind)))
     return qv_fail(c, QV_ERR_ARG, "qv_step_exchange: x, infront and behind are required");
   int rc;
-  if (n > 0 && (rc = check_links(c, n, in->infront, in->behind, in->closest, "qv_step_exchange")))
+  if (n > 0 && (rc = stage_links(c, n, in->infront, in->behind, in->closest, "qv_step_exchange")))
     return rc;
   if ((rc = reserve_points(c, std::max(n, 1)))) return rc;
   if ((rc = qv_aux_streams(c))) return rc;
@@ -876,9 +951,10 @@ extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in,
     const cudaMemcpyKind h2d = cudaMemcpyHostToDevice;
     // what the step reads first, here; the AB history and closest on a side
     // stream, awaited by the update
+    const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
     QV_CUDA(c, cudaMemcpyAsync(c->x, in->x, v, h2d, c->stream));
-    QV_CUDA(c, cudaMemcpyAsync(c->infront, in->infront, sizeof(int) * n, h2d, c->stream));
-    QV_CUDA(c, cudaMemcpyAsync(c->behind, in->behind, sizeof(int) * n, h2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->infront, c->lk, sizeof(int) * n, d2d, c->stream));
+    QV_CUDA(c, cudaMemcpyAsync(c->behind, c->lk + n, sizeof(int) * n, d2d, c->stream));
     double *zv[] = {c->u, c->u_li, c->u_bs};
     for (double *q : zv) QV_CUDA(c, cudaMemsetAsync(q, 0, v, c->stream));
     QV_CUDA(c, cudaMemsetAsync(c->closestd, 0, sizeof(double) * n, c->stream));
@@ -891,7 +967,9 @@ extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in,
       if (hs[k]) QV_CUDA(c, cudaMemcpyAsync(hd[k], hs[k], v, h2d, sa));
       else QV_CUDA(c, cudaMemsetAsync(hd[k], 0, v, sa));
     }
-    if (in->closest) QV_CUDA(c, cudaMemcpyAsync(c->closest, in->closest, sizeof(int) * n, h2d, sa));
+    if (in->closest)
+      QV_CUDA(c, cudaMemcpyAsync(c->closest, c->lk + 2 * (size_t)n, sizeof(int) * n,
+                                 cudaMemcpyDeviceToDevice, sa));
     else QV_CUDA(c, cudaMemsetAsync(c->closest, 0, sizeof(int) * n, sa));
     QV_CUDA(c, cudaEventRecord(c->ev_in, sa));
     c->in_pending = true;
@@ -902,7 +980,8 @@ extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in,
   ExchangeOut o;
   o.cap = cap;
   o.out = out;
-  rc = step_body(c, itime, exchange_out_hook, &o);
+  if (n > 0 && c->p.line_ops && (rc = qv_line_clear_log_reset(c))) return rc;
+  rc = step_body(c, itime, exchange_out_hook, &o, exchange_insert_hook);
   if (rc) {
     // nothing may still read the caller's arrays once this returns
     c->in_pending = false;
@@ -917,6 +996,24 @@ extern "C" int qv_step_exchange(qv_ctx *c, int itime, int n, const qv_state *in,
   if (o.queued) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[2], 0));
   rc = velocity_collect(c, nullptr);
   if (rc) return rc;
+  if (o.early && !o.over) {
+    const int ncl = c->h_clr[0];
+    double *hz[] = {out->u, out->u1, out->u2};  // what clear_particle zeroes (u3 is kept)
+    const double *dz[] = {c->u, c->u1, c->u2};
+    if (ncl > QV_LINE_CLR_HOST) {  // more than the log's host copy: take the arrays again
+      for (int k = 0; k < 3; k++)
+        if (hz[k])
+          QV_CUDA(c, cudaMemcpyAsync(hz[k], dz[k], sizeof(double) * 3 * (size_t)c->n,
+                                     cudaMemcpyDeviceToHost, c->stream));
+      QV_CUDA(c, cudaStreamSynchronize(c->stream));
+    } else {
+      for (int e = 0; e < ncl; e++) {
+        const size_t i = (size_t)c->h_clr[1 + e];
+        for (int k = 0; k < 3; k++)
+          if (hz[k]) hz[k][3 * i] = hz[k][3 * i + 1] = hz[k][3 * i + 2] = 0.;
+      }
+    }
+  }
   if (o.over)
     return qv_fail(c, QV_ERR_ARG, "qv_step_exchange: %d slots in use, host arrays hold %d", c->n,
                    cap);

@@ -164,12 +164,18 @@ struct qv_ctx {
   int *dstatus = nullptr;               // device status word
   double *dscalar = nullptr;            // device scalar scratch
   double *walk_part = nullptr;          // per-image partial sums of the walk
+  int *lk = nullptr;                    // staged host links: infront, behind, closest, verdict
+  size_t lk_ints = 0;
+  int *h_lk = nullptr;                  // pinned: the link check's verdict
   size_t walk_part_bytes = 0;
   bool ghosts_valid = false;
   bool ghosts_stored = false;  // ghost arrays hold values (possibly from before a move)
   // line operations (pinsert / premove): flag and list scratch, sequential state
   void *line_flags = nullptr, *line_st = nullptr, *line_rec = nullptr;
   void *line_host = nullptr;       // pinned copy of the ordered passes' state
+  int *line_clr = nullptr;         // slots the line operations cleared (QV_LINE_CLR_CAP)
+  int *h_clr = nullptr;            // pinned: their count and the first QV_LINE_CLR_HOST
+  cudaEvent_t ev_pins = nullptr;   // recorded behind each pinsert scan
   cudaEvent_t ev_line = nullptr;   // recorded when that copy is queued
   unsigned long long *h_stat = nullptr;  // pinned: evaluation counters and status word
   cudaEvent_t ev_in = nullptr;  // qv_step_exchange: the side-stream inputs are in
@@ -237,6 +243,12 @@ int qv_grow_points(qv_ctx *c, int new_cap);
 int qv_line_insert(qv_ctx *c, int *inserted);
 int qv_line_remove(qv_ctx *c, int *removed);
 int qv_line_reconnect(qv_ctx *c, int *count);
+// The log of slots cleared by premove and reconnection (clear_particle):
+// reset it, and queue the copy of its count and first entries to c->h_clr.
+#define QV_LINE_CLR_CAP 65536
+#define QV_LINE_CLR_HOST 4096
+int qv_line_clear_log_reset(qv_ctx *c);
+int qv_line_clear_log_queue(qv_ctx *c);
 // ordered compaction kernels (qv_direct.cu): counts of nonzero flags per
 // 256-slot block, their exclusive scan (total to *total), the scatter
 __global__ void k_count_active(int n, const int *__restrict__ inf, int *blk_cnt);

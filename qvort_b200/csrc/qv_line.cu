@@ -40,7 +40,8 @@ struct LineState {
   int heap_n;
   int status;        // 1: more slots needed, 2: heap overflow
   int done;          // points inserted / removed so far
-  int pad[6];
+  int n_clr;         // entries of the cleared-slot log (may exceed its capacity)
+  int pad[5];
   int heap[LHEAP];
 };
 
@@ -76,6 +77,7 @@ struct LineArgs {
   int *flag_a, *flag_b;
   LineState *st;
   int *dstatus;  // the context's status word (QV_STAT_HEAP: a scan's re-test heap overflowed)
+  int *clr;      // cleared-slot log, QV_LINE_CLR_CAP entries
 };
 
 // clear_particle, src/general.f90:11-22 (u3 is kept)
@@ -89,6 +91,9 @@ __device__ __forceinline__ void clear_slot(const LineArgs &a, int i) {
   a.beh[i] = 0;
   a.closest[i] = 0;
   a.closestd[i] = 0.;
+  // the log lets a host copy taken before this scan be corrected afterwards
+  const int k = atomicAdd(&a.st->n_clr, 1);
+  if (k < QV_LINE_CLR_CAP) a.clr[k] = i;
 }
 
 __device__ __forceinline__ double seg_len(const double *a, const double *b) {
@@ -412,8 +417,12 @@ static int line_reserve(qv_ctx *c) {
   int rc;
   if ((rc = qv_grow(c, (void **)&c->line_flags, sizeof(int) * 4 * n))) return rc;
   if ((rc = qv_grow(c, (void **)&c->line_rec, sizeof(RecEval) * n))) return rc;
-  if (!c->line_st)
+  if (!c->line_st) {
     if ((rc = qv_grow(c, (void **)&c->line_st, sizeof(LineState)))) return rc;
+    QV_CUDA(c, cudaMemsetAsync(c->line_st, 0, sizeof(LineState), c->stream));
+  }
+  if (!c->line_clr)
+    if ((rc = qv_grow(c, (void **)&c->line_clr, sizeof(int) * QV_LINE_CLR_CAP))) return rc;
   c->line_cap = n;
   return QV_OK;
 }
@@ -439,6 +448,7 @@ static LineArgs line_args(qv_ctx *c) {
   a.empt = f + 3 * n;
   a.st = (LineState *)c->line_st;
   a.dstatus = c->dstatus;
+  a.clr = c->line_clr;
   return a;
 }
 
@@ -511,6 +521,8 @@ int qv_line_insert_queue(qv_ctx *c) {
   k_pinsert_seq<<<1, 1, 0, c->stream>>>(a);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
+  if (!c->ev_pins) QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_pins, cudaEventDisableTiming));
+  QV_CUDA(c, cudaEventRecord(c->ev_pins, c->stream));
   return queue_state_copy(c);
 }
 
@@ -551,6 +563,26 @@ int qv_line_insert(qv_ctx *c, int *inserted) {
 }
 
 const int *qv_line_count_dev(qv_ctx *c) { return &((LineState *)c->line_st)->n_cur; }
+
+int qv_line_clear_log_reset(qv_ctx *c) {
+  int rc;
+  if ((rc = line_reserve(c))) return rc;
+  QV_CUDA(c, cudaMemsetAsync(&((LineState *)c->line_st)->n_clr, 0, sizeof(int), c->stream));
+  return QV_OK;
+}
+
+int qv_line_clear_log_queue(qv_ctx *c) {
+  if (!c->line_st || !c->line_clr) return qv_fail(c, QV_ERR_STATE, "no cleared-slot log");
+  if (!c->h_clr)
+    QV_CUDA(c, cudaHostAlloc((void **)&c->h_clr, sizeof(int) * (QV_LINE_CLR_HOST + 1),
+                             cudaHostAllocDefault));
+  const cudaMemcpyKind d2h = cudaMemcpyDeviceToHost;
+  QV_CUDA(c, cudaMemcpyAsync(c->h_clr, &((LineState *)c->line_st)->n_clr, sizeof(int), d2h,
+                             c->stream));
+  QV_CUDA(c, cudaMemcpyAsync(c->h_clr + 1, c->line_clr, sizeof(int) * QV_LINE_CLR_HOST, d2h,
+                             c->stream));
+  return QV_OK;
+}
 const int *qv_line_status_dev(qv_ctx *c) { return &((LineState *)c->line_st)->status; }
 
 int qv_line_reconnect(qv_ctx *c, int *count) {

@@ -5,8 +5,9 @@ kernel as an out-of-bounds index or an endless wait:
 
 * corrupted links (an index outside 0..n, an active slot linked to an empty
   slot, a closest index outside 0..n) are refused by qv_set_points,
-  qv_set_state and qv_step_exchange before anything is uploaded -- no kernel is
-  launched -- and the context stays usable;
+  qv_set_state and qv_step_exchange: the links are checked on a staging copy
+  before the context takes anything -- the check is the only launch -- and the
+  context stays usable;
 * a NaN in the positions of an empty slot (which no kernel reads) is reported
   at the end of the step as QV_ERR_NAN, as the reference's NAN_finder
   (src/general.f90:253-280, src/run.f90:168) stops the run;
@@ -50,17 +51,22 @@ def _corruptions(w):
     return out
 
 
-def test_corrupted_links_are_refused_before_any_launch():
+def test_corrupted_links_are_refused_before_the_context_changes():
     L, W = _mods()
     w = _tangle(W)
     c = L.Context(L.default_params(**dict(w.params, line_ops=2)))
     n = w.n
+    # a state of its own, which the refused calls must leave as it is
+    x0 = w.x + 1e-4
+    c.set_points(x0, w.infront, w.behind)
     for name, inf, beh, cl in _corruptions(w):
         before = c.counters()["launches"]
+        refused = 2
         if cl is None:
             with pytest.raises(L.QvError) as e:
                 c.set_points(w.x, inf, beh)
             assert e.value.code == L.QV_ERR_ARG, name
+            refused += 1
         with pytest.raises(L.QvError) as e:
             c.set_state(n, x=w.x, infront=inf, behind=beh, closest=cl)
         assert e.value.code == L.QV_ERR_ARG, name
@@ -72,7 +78,11 @@ def test_corrupted_links_are_refused_before_any_launch():
         with pytest.raises(L.QvError) as e:
             c.step_exchange(1, n, 2 * n, inp, out)
         assert e.value.code == L.QV_ERR_ARG, name
-        assert c.counters()["launches"] == before, name   # nothing was launched
+        # one launch per refused call: the check itself
+        assert c.counters()["launches"] == before + refused, name
+    assert c.n == n
+    x1, _ = c.get_points()
+    assert np.array_equal(x1, x0)
     # the context is still usable
     c.set_points(w.x, w.infront, w.behind)
     c.step(1)

@@ -593,13 +593,15 @@ def test_field_velocity_tree_matches_oracle(L, bc, theta):
     assert rel_max(u[ok], uo[ok]) < 1e-12, rel_max(u[ok], uo[ok])
 
 
-@pytest.mark.parametrize("delta", [4.5e-4, 4.1e-4])
+@pytest.mark.parametrize("delta", [4.5e-4, 4.1e-4, 9e-4])
 def test_step_exchange_equals_set_step_get(delta):
     """qv_step_exchange (one call, copies overlapping the step) leaves the host
     copy of f(:) exactly as qv_set_state, qv_step, qv_get_state do, through
-    steps with reconnections (delta 4.5e-4) or insertions (4.1e-4, below the
-    point spacing 4.2e-4); a host copy too small for the slot count is an
-    error that leaves it untouched."""
+    steps with reconnections (delta 4.5e-4), insertions (4.1e-4, below the
+    point spacing 4.2e-4) or removals (9e-4, above half the distance to the
+    second neighbour: the cleared slots are zeroed in the copies taken before
+    premove ran); a host copy too small for the slot count is an error that
+    leaves it untouched."""
     from qvort_b200 import lib as L
     import sys
     from pathlib import Path
@@ -637,6 +639,8 @@ def test_step_exchange_equals_set_step_get(delta):
             assert np.array_equal(ha[k][:na], hb[k][:nb]), (it, k)
     if delta < 4.2e-4:
         assert na > n0                                      # points were inserted
+    elif delta > 8e-4:
+        assert (ha["infront"][:na] != 0).sum() < n0          # points were removed
     else:
         assert not np.array_equal(ha["infront"][:n0], inf)  # links were reconnected
     before = {k: v.copy() for k, v in ha.items()}
