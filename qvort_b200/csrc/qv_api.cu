@@ -151,6 +151,7 @@ extern "C" int qv_destroy(qv_ctx *c) {
   if (c->h_stat) cudaFreeHost(c->h_stat);
   if (c->ev_line) cudaEventDestroy(c->ev_line);
   if (c->walk_part) cudaFree(c->walk_part);
+  if (c->walk_next) cudaFree(c->walk_next);
   if (c->lk) cudaFree(c->lk);
   if (c->h_lk) cudaFreeHost(c->h_lk);
   for (int k = 0; k < 3; k++) {

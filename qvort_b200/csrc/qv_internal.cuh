@@ -164,6 +164,7 @@ struct qv_ctx {
   int *dstatus = nullptr;               // device status word
   double *dscalar = nullptr;            // device scalar scratch
   double *walk_part = nullptr;          // per-image partial sums of the walk
+  int *walk_next = nullptr;             // the mixed walk's task counters
   int *lk = nullptr;                    // staged host links: infront, behind, closest, verdict
   size_t lk_ints = 0;
   int *h_lk = nullptr;                  // pinned: the link check's verdict

@@ -37,6 +37,8 @@
 // Active points from which the mixed walk's unshifted-image tasks carry 64
 // targets, not 32.
 #define QV_WALK_PAIR_NEAR 65536
+// Active points from which the mixed walk hands out its tasks dynamically.
+#define QV_WALK_DYNAMIC 65536
 
 struct WalkArgs {
   int n_act;
@@ -55,6 +57,7 @@ struct WalkArgs {
   // mixed walk: groups of 64 targets, and whether the unshifted image's tasks
   // carry 64 targets (else 32 per task, ngroups of them per slot)
   int ng64, pair_near;
+  int *next;  // mixed walk, large systems: task counters, [0] the walk, [1] its gated relaunch
   unsigned long long *evals, *evals_far;
   int *status;
   // Root header speculation (see root_open): root_est[3] bounds the distance
@@ -616,11 +619,19 @@ __device__ __forceinline__ void walk_task2(const WalkArgs &a, StkEnt *st, int la
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.status, QV_STAT_SINGULAR);
 }
 
-// Tasks in order: the unshifted image's (heaviest first), then the images'.
+// Task order: the unshifted image's tasks (the heaviest: they carry the near
+// field), slot by slot, then the periodic images'.  Large systems hand the
+// tasks out one at a time from a counter, so that a warp which finishes early
+// takes the next task instead of idling until its block's slowest warp is
+// done.  Small ones (a few tasks per warp) keep a fixed task per warp, whose
+// block's four warps walk neighbouring target groups and share their nodes in
+// L1: handed out dynamically, or longest first by the last walk's task times,
+// they ran slower (the walk's length is then its longest near-field task).
 // Image tasks carry 64 targets (two per lane); the unshifted image's carry 64
 // when the system is large and 32 (one per lane) otherwise, which halves the
-// longest task when there are few tasks per warp.  Either kind computes, per
-// target, the same sums bit for bit.
+// longest task when there are few tasks per warp.  Each (group, slot) task
+// writes its own partial sums, so neither the order nor the kind changes a
+// result: per target, both kinds compute the same sums bit for bit.
 template <int BC>
 __device__ __forceinline__ void walk32_body(const WalkArgs &a) {
   constexpr int NIMG = BC == QV_BC_PERIODIC ? 26 : BC == QV_BC_OPENX ? 8 : BC == QV_BC_OPENXY ? 2 : 0;
@@ -629,17 +640,26 @@ __device__ __forceinline__ void walk32_body(const WalkArgs &a) {
   const double rdelta = a.root_est ? a.root_est[3] : 0.;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   StkEnt *st = stk_dyn + wid * a.stk_cap;
-  const int near1 = a.pair_near ? 0 : NSPLIT * a.ngroups;  // one-target tasks
-  const int s0 = a.pair_near ? 0 : NSPLIT;                 // first slot of the paired tasks
-  const int items = near1 + (NSPLIT + NIMG - s0) * a.ng64;
-  for (int item = blockIdx.x * WW + wid; item < items; item += gridDim.x * WW) {
-    if (item < near1) {
-      const int sl = item / a.ngroups;
-      walk_task1<BC>(a, st, lane, sl, item - sl * a.ngroups, rdelta);
-    } else {
-      const int j = item - near1, k = j / a.ng64;
-      walk_task2<BC>(a, st, lane, s0 + k, j - k * a.ng64, rdelta);
+  const int gn = a.pair_near ? a.ng64 : a.ngroups;  // groups of the unshifted image's tasks
+  const int nnear = NSPLIT * gn;
+  const int items = nnear + NIMG * a.ng64;
+  int *ctr = a.next ? a.next + (a.gate ? 1 : 0) : nullptr;
+  int item = blockIdx.x * WW + wid;
+  for (;;) {
+    if (ctr) {
+      if (lane == 0) item = atomicAdd(ctr, 1);
+      item = __shfl_sync(0xffffffffu, item, 0);
     }
+    if (item >= items) break;
+    if (item < nnear) {
+      const int sl = item / gn, g = item - sl * gn;
+      if (a.pair_near) walk_task2<BC>(a, st, lane, sl, g, rdelta);
+      else walk_task1<BC>(a, st, lane, sl, g, rdelta);
+    } else {
+      const int j = item - nnear, k = j / a.ng64;
+      walk_task2<BC>(a, st, lane, NSPLIT + k, j - k * a.ng64, rdelta);
+    }
+    item += gridDim.x * WW;
   }
 }
 
@@ -651,10 +671,15 @@ __global__ void __launch_bounds__(WW * 32) k_walk64(WalkArgs a) { walk64_body<BC
 template <int BC>
 __global__ void __launch_bounds__(WW * 32) k_walk64_redo(WalkArgs a) { walk64_body<BC>(a); }
 // 5 blocks/SM (96 registers): faster than 4 (111 registers) on the paired tasks
+#define WALK32_BLOCKS_PER_SM 5
 template <int BC>
-__global__ void __launch_bounds__(WW * 32, 5) k_walk32(WalkArgs a) { walk32_body<BC>(a); }
+__global__ void __launch_bounds__(WW * 32, WALK32_BLOCKS_PER_SM) k_walk32(WalkArgs a) {
+  walk32_body<BC>(a);
+}
 template <int BC>
-__global__ void __launch_bounds__(WW * 32, 5) k_walk32_redo(WalkArgs a) { walk32_body<BC>(a); }
+__global__ void __launch_bounds__(WW * 32, WALK32_BLOCKS_PER_SM) k_walk32_redo(WalkArgs a) {
+  walk32_body<BC>(a);
+}
 
 // u_bs = main + images, u = (u_li + main) + images, with the main image summed
 // over the root's children in child order and the images in the reference's
@@ -743,10 +768,20 @@ int qv_launch_walk(qv_ctx *c) {
   // entries (each open pushes at most 8 and pops 1)
   a.stk_cap = 7 * (t.depth + 1) + 8;
   size_t smem = sizeof(StkEnt) * a.stk_cap * WW;
-  long items = (long)a.ngroups * (NSPLIT + nimg);
-  if (mixed) items = (a.pair_near ? 0L : (long)NSPLIT * a.ngroups) +
-                     (long)a.ng64 * (nimg + (a.pair_near ? NSPLIT : 0));
+  const long items = mixed ? (long)NSPLIT * (a.pair_near ? a.ng64 : a.ngroups) + (long)a.ng64 * nimg
+                           : (long)a.ngroups * (NSPLIT + nimg);
   int nb = (int)std::min<long>((items + WW - 1) / WW, 64L * c->sm_count);
+  a.next = nullptr;
+  if (mixed && t.n_act >= QV_WALK_DYNAMIC) {
+    // every warp stays until the task counter runs out: one resident grid
+    nb = (int)std::min<long>((items + WW - 1) / WW, (long)WALK32_BLOCKS_PER_SM * c->sm_count);
+    if (!c->walk_next) {
+      int rc = qv_grow(c, (void **)&c->walk_next, 2 * sizeof(int));
+      if (rc) return rc;
+    }
+    QV_CUDA(c, cudaMemsetAsync(c->walk_next, 0, 2 * sizeof(int), c->stream));
+    a.next = c->walk_next;
+  }
   if (mixed && smem > 48 * 1024) {
     if (smem > c->smem_walk) {  // per context: attributes are per device
       const void *fs[] = {(const void *)k_walk32<QV_BC_OPEN>, (const void *)k_walk32<QV_BC_PERIODIC>,

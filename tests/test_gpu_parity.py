@@ -699,3 +699,36 @@ def test_root_estimate_gives_the_exact_walk(L, precision):
         L.test_root_speculation(-1, 1.0)
         c.close()
     assert seen[0] == 0 and 0 < seen[1] <= 8192 < seen[2], seen
+
+
+def test_root_estimate_gives_the_exact_walk_on_the_tangle(L):
+    """Config 2's tangle (24.7k points, below the size that starts the walk
+    from the estimate by itself): the mixed walk started from the root
+    centroid's bounded estimate gives the velocities and evaluation counts of
+    the walk from the exact centroid, bit for bit, whether the fix-up drops the
+    undecided images or its list overflows and the gated walk redoes every
+    task; the exact walk makes the FP64 walk's decisions (the same evaluation
+    count) within 1e-6 RMS of its velocities."""
+    w = W.tangle(0)
+    c = ctx_for(L, w, precision="mixed")
+    c64 = ctx_for(L, w, precision="fp64")
+    try:
+        L.test_root_speculation(0)
+        u0, _, _, ev0 = c.velocity()
+        u64, _, _, ev64 = c64.velocity()
+        assert ev0 == ev64
+        assert np.sqrt(((u0 - u64) ** 2).sum() / (u64 ** 2).sum()) < 1e-6
+        seen = []
+        for scale in (1.0, 3e10, 1e11, 3e11, 1e12, 1e13, 1e14):
+            L.test_root_speculation(1, scale)
+            c.set_points(w.x, w.infront, w.behind)
+            u, _, _, ev = c.velocity()
+            seen.append(c.root_undecided())
+            assert np.array_equal(u, u0), scale
+            assert ev == ev0, scale
+    finally:
+        L.test_root_speculation(-1, 1.0)
+        c.close()
+        c64.close()
+    assert seen[0] == 0, seen
+    assert any(0 < s <= 8192 for s in seen) and any(s > 8192 for s in seen), seen
