@@ -14,9 +14,12 @@
 #include "qv_internal.cuh"
 
 #define CW 4
-#ifndef TPW
-#define TPW 8  // targets per warp: the search is latency-bound; more, shorter warps hide more of it (32 -> 8: -22 us per config-2 step)
-#endif
+// Targets per warp: the search is latency-bound, so small systems run more,
+// shorter warps (8 targets each: 22 us less per config-2 step than 32), while
+// large ones fill the warp (32: 0.68 ms less per config-3 step than 8).
+#define TPW_SMALL 8
+#define TPW_LARGE 32
+#define TPW_LARGE_MIN 65536
 
 __device__ __forceinline__ double dist_exact(const double *a, double b0, double b1, double b2) {
   double d0 = __dsub_rn(a[0], b0), d1 = __dsub_rn(a[1], b1), d2 = __dsub_rn(a[2], b2);
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int 
                                                          const int *__restrict__ parent,
                                                          const int *__restrict__ leaf_of,
                                                          int n_leaf, int nn, float box,
-                                                         int stk_cap,
+                                                         int stk_cap, int tpw,
                                                          int *closest, double *closestd,
                                                          int *status) {
   extern __shared__ CStkEnt cstk[];
@@ -172,10 +175,10 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int 
   const int n = d_n ? *d_n : n_host;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   CStkEnt *st = cstk + wid * stk_cap;
-  const int nwarps = (n + TPW - 1) / TPW;
+  const int nwarps = (n + tpw - 1) / tpw;
   for (int w = blockIdx.x * CW + wid; w < nwarps; w += gridDim.x * CW) {
-    int i = w * TPW + lane;
-    bool live = lane < TPW && i < n && inf[i] != 0;
+    int i = w * tpw + lane;
+    bool live = lane < tpw && i < n && inf[i] != 0;
     double xi[3] = {0., 0., 0.};
     int ii = i + 1, fi = -1, bi = -1, cl = 0;
     double cd = 100.;
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(CW * 32) k_closest_tree(int n_host, const int 
       }
       __syncwarp();
     }
-    if (lane < TPW && i < n) {
+    if (lane < tpw && i < n) {
       closestd[i] = cd;  // 100 for empty slots too (src/tree.f90:225)
       if (live) closest[i] = cl;
     }
@@ -345,7 +348,8 @@ int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_gri
     if (!c->tree.valid) return qv_fail(c, QV_ERR_STATE, "pclose_tree without a built tree");
     int rc = qv_tree_finalize_root(c);
     if (rc) return rc;
-    int nwarps = (n_grid + TPW - 1) / TPW;
+    const int tpw = n_grid >= TPW_LARGE_MIN ? TPW_LARGE : TPW_SMALL;
+    int nwarps = (n_grid + tpw - 1) / tpw;
     int cap = 7 * (c->tree.depth + 1) + 8;
     size_t smem = sizeof(CStkEnt) * cap * CW;
     if (smem > 48 * 1024 && smem > c->smem_search) {  // per context: attributes are per device
@@ -356,7 +360,7 @@ int qv_launch_closest_ex(qv_ctx *c, const int *d_n, const int *d_skip, int n_gri
     const TreeBuf &t = c->tree;
     k_closest_tree<<<(nwarps + CW - 1) / CW, CW * 32, smem, c->stream>>>(
         c->n, d_n, d_skip, c->x, c->infront, c->behind, t.w64, t.c32, t.parent, t.leaf_of,
-        t.n_leaf, std::min(t.n_nodes, t.cap_nodes), (float)c->p.box_size, cap, c->closest,
+        t.n_leaf, std::min(t.n_nodes, t.cap_nodes), (float)c->p.box_size, cap, tpw, c->closest,
         c->closestd, c->dstatus);
   } else {
     k_pclose<<<(n_grid + PT - 1) / PT, PT, 0, c->stream>>>(c->n, d_n, d_skip, c->x, c->infront,
