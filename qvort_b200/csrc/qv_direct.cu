@@ -469,6 +469,19 @@ __device__ __forceinline__ void seg_terms(float r1s, float r2s, float dd, float 
   oz = g * cz;
 }
 
+// seg_terms where cos is known to be positive: f / (1 + cos).
+__device__ __forceinline__ void seg_terms_pos(float r1s, float r2s, float dd, float cx, float cy,
+                                              float cz, float &ox, float &oy, float &oz) {
+  const float ra = rsqrtf(r1s), rb = rsqrtf(r2s);
+  const float q = ra * rb;
+  const float cs = dd * q;
+  const float f = (ra + rb) * q;
+  const float g = __fdividef(f, 1.f + cs);
+  ox = g * cx;
+  oy = g * cy;
+  oz = g * cz;
+}
+
 template <int BC, int NT>
 __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restrict__ act,
                                                     const double *__restrict__ x,
@@ -526,8 +539,9 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
       const float sx = D.y, sy = D.z, sz = D.w;
 #pragma unroll
       for (int k = 0; k < NT; k++) {
-        if (jj == bi[k]) continue;  // src/timestep.f90:471, 496
+        const bool skip_src = jj == bi[k];  // src/timestep.f90:471, 496
         if (PX * PY * PZ == 1) {
+          if (skip_src) continue;
           // open boundaries, the main image alone: the operations of the
           // batched direct items (qv_batch.cu), so that a batched system is
           // bitwise the same system run alone
@@ -567,32 +581,47 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
           a1z[s] = r1z[s] * r1z[s]; a2z[s] = r2z[s] * r2z[s]; pdz[s] = r1z[s] * r2z[s];
           zsy[s] = r1z[s] * sy; zsx[s] = r1z[s] * sx;
         }
+        // When |R1| > |s| in every image, every image's cos is positive
+        // (R1.R2 >= |R1| (|R1| - |s|)): the warp then takes the select-free
+        // form of the term for this source, the pos case of seg_terms.  The
+        // least |R1|^2 over the images is the sum over axes of each axis' least
+        // square; the factor 1.0001 covers the rounding of both sides.
+        float m1 = PX == 3 ? fminf(fminf(a1x[0], a1x[1]), a1x[2]) : a1x[1];
+        m1 += PY == 3 ? fminf(fminf(a1y[0], a1y[1]), a1y[2]) : a1y[1];
+        m1 += PZ == 3 ? fminf(fminf(a1z[0], a1z[1]), a1z[2]) : a1z[1];
+        const float ss = fmaf(sx, sx, fmaf(sy, sy, sz * sz));
+        const bool fast = __all_sync(0xffffffffu, skip_src || m1 > 1.0001f * ss);
+        if (skip_src) continue;
         float ix = 0.f, iy = 0.f, iz = 0.f;
+        auto images = [&](auto term) {
 #pragma unroll
-        for (int a = 0; a < PX; a++) {
-          const int sa = PX == 3 ? a : 1;  // index of the x shift (1 = none)
+          for (int a = 0; a < PX; a++) {
+            const int sa = PX == 3 ? a : 1;  // index of the x shift (1 = none)
 #pragma unroll
-          for (int b = 0; b < PY; b++) {
-            const int sb = PY == 3 ? b : 1;
+            for (int b = 0; b < PY; b++) {
+              const int sb = PY == 3 ? b : 1;
 #pragma unroll
-            for (int cc = 0; cc < PZ; cc++) {
-              const int sc = PZ == 3 ? cc : 1;
-              const bool main_img = sa == 1 && sb == 1 && sc == 1;
-              if (main_img && jj == ii[k]) continue;
-              float ox, oy, oz;
-              seg_terms(a1x[sa] + a1y[sb] + a1z[sc], a2x[sa] + a2y[sb] + a2z[sc],
-                        pdx[sa] + pdy[sb] + pdz[sc], ysz[sb] - zsy[sc], zsx[sc] - xsz[sa],
-                        xsy[sa] - ysx[sb], ox, oy, oz);
-              if (main_img) {
-                k0[k].add(ox, oy, oz);
-              } else {
-                ix += ox;
-                iy += oy;
-                iz += oz;
+              for (int cc = 0; cc < PZ; cc++) {
+                const int sc = PZ == 3 ? cc : 1;
+                const bool main_img = sa == 1 && sb == 1 && sc == 1;
+                if (main_img && jj == ii[k]) continue;
+                float ox, oy, oz;
+                term(a1x[sa] + a1y[sb] + a1z[sc], a2x[sa] + a2y[sb] + a2z[sc],
+                     pdx[sa] + pdy[sb] + pdz[sc], ysz[sb] - zsy[sc], zsx[sc] - xsz[sa],
+                     xsy[sa] - ysx[sb], ox, oy, oz);
+                if (main_img) {
+                  k0[k].add(ox, oy, oz);
+                } else {
+                  ix += ox;
+                  iy += oy;
+                  iz += oz;
+                }
               }
             }
           }
-        }
+        };
+        if (fast) images(seg_terms_pos);
+        else images(seg_terms);
         if (PX * PY * PZ > 1) k1[k].add(ix, iy, iz);
       }
     }
