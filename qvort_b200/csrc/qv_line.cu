@@ -111,7 +111,10 @@ __device__ __forceinline__ void begin_state(LineState *s, int n) {
 // pinsert's test on the stored ghosts (src/line.f90:41,49) and the empty slots.
 __global__ void k_ins_flags(int n, LineArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) begin_state(a.st, n);
+  if (i == 0) {
+    begin_state(a.st, n);
+    a.st->n_clr = 0;  // a step's line operations start with pinsert: a fresh cleared-slot log
+  }
   if (i >= n) return;
   int act = a.inf[i] != 0;
   a.flag_b[i] = !act;
@@ -319,6 +322,8 @@ __device__ void norm_tan(const LineArgs &a, int i, double *t) {
 struct RecEval {
   int j, pari, parjb, parallel;
   double l_before, s3, l_after;
+  int maybe;  // the test, on the links at the start of the pass, reconnects
+  int pad;
 };
 
 __global__ void k_rec_eval(int n, LineArgs a, RecEval *rec) {
@@ -345,48 +350,70 @@ __global__ void k_rec_eval(int n, LineArgs a, RecEval *rec) {
     r.s3 = seg_len(xi, a.gb + 3 * i) + seg_len(xi, xj) + seg_len(xj, a.gi + 3 * j);
     r.l_after = r.s3 + seg_len(a.x + 3 * r.pari, a.x + 3 * r.parjb);
   }
+  // the ordered pass's test on the links as they are now (src/reconnection.f90:163-190)
+  const int parb = a.beh[i] - 1;
+  r.maybe = a.inf[i] != 0 && r.j >= 0 && r.j != r.pari && r.j != parb && a.inf[r.j] != 0 &&
+            !r.parallel && r.l_after <= r.l_before;
+  r.pad = 0;
   rec[q] = r;
 }
 
-// The ordered pass of precon_original.  The block first gathers, for a batch
-// of candidates, the candidate, its precomputed record and the current links
-// of i and j into shared memory; thread 0 then runs the candidates in order
-// from there, and after its first change of a link within the batch reads the
-// links from global memory again, so every test sees the current links.
-#define PB 512  // candidates gathered per batch
-__global__ void __launch_bounds__(256) k_precon_seq(LineArgs a, const RecEval *rec) {
-  __shared__ RecEval s_r[PB];
-  __shared__ int s_i[PB], s_ii[PB], s_ib[PB], s_jf[PB], s_jb[PB];
+// The ordered pass of precon_original.  A candidate's test reads the links of
+// its own slot i and of its partner j (and positions, which the pass changes
+// only in the slots loop_killer clears, whose links it clears too).  So while
+// neither i's nor j's links have changed since the pass began, the test gives
+// what it gave on the starting links, which k_rec_eval evaluated for every
+// candidate (maybe).  The block therefore scans the candidates in order, a
+// window of PC_T at a time, for the first that either reconnects on the
+// starting links or has a slot whose links the pass has changed, and thread 0
+// runs the reference's test on the current links for that one only: every
+// candidate skipped would have done nothing.  The changed slots (the four
+// relinked ones and those loop_killer clears, from the cleared-slot log) are
+// listed in shared memory; past PC_CHG of them every candidate is tested.
+#define PC_T 256
+#define PC_CHG 1024
+__device__ __forceinline__ bool pc_changed(const int *chg, int nchg, int slot) {
+  for (int k = 0; k < nchg; k++)
+    if (chg[k] == slot) return true;
+  return false;
+}
+
+__global__ void __launch_bounds__(PC_T) k_precon_scan(LineArgs a, const RecEval *rec) {
+  __shared__ int chg[PC_CHG];
+  __shared__ int nchg, first;
   LineState *s = a.st;
   const int nc = s->nc, pc0 = s->pc;
+  const int tid = threadIdx.x;
+  if (tid == 0) nchg = 0;
   int done = 0;
-  for (int base = pc0; base < nc; base += PB) {
-    const int m = min(PB, nc - base);
+  for (int pos = pc0; pos < nc;) {
     __syncthreads();
-    for (int q = threadIdx.x; q < m; q += blockDim.x) {
-      const int i = a.cand[base + q];
-      const RecEval r = rec[base + q];
-      s_r[q] = r;
-      s_i[q] = i;
-      s_ii[q] = a.inf[i];
-      s_ib[q] = a.beh[i];
-      s_jf[q] = r.j >= 0 ? a.inf[r.j] : 0;
-      s_jb[q] = r.j >= 0 ? a.beh[r.j] : 0;
+    if (tid == 0) first = PC_T;
+    __syncthreads();
+    const int q = pos + tid;
+    if (q < nc) {
+      const int n_c = nchg;
+      bool hit = rec[q].maybe != 0 || n_c > PC_CHG;
+      if (!hit && n_c > 0) {
+        const int j = rec[q].j;
+        hit = pc_changed(chg, n_c, a.cand[q]) || (j >= 0 && pc_changed(chg, n_c, j));
+      }
+      if (hit) atomicMin(&first, tid);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      bool dirty = false;  // a link changed since the gather
-      for (int q = 0; q < m; q++) {
-        const int i = s_i[q];
-        const int infi = dirty ? a.inf[i] : s_ii[q];
-        if (infi == 0) continue;  // cleared by an earlier loop_killer
-        const int pari = infi - 1, parb = (dirty ? a.beh[i] : s_ib[q]) - 1;
-        const RecEval &r = s_r[q];
-        const int j = r.j;
-        if (j == pari || j == parb || j < 0) continue;
-        if ((dirty ? a.inf[j] : s_jf[q]) == 0) continue;
-        const int parjb = (dirty ? a.beh[j] : s_jb[q]) - 1;
-        if (r.parallel) continue;  // parallel filaments do not reconnect
+    const int f = first;
+    if (f == PC_T) {
+      pos += PC_T;
+      continue;
+    }
+    if (tid == 0) {
+      const int qq = pos + f, i = a.cand[qq];
+      const RecEval r = rec[qq];
+      const int infi = a.inf[i];
+      const int pari = infi - 1, parb = a.beh[i] - 1, j = r.j;
+      // src/reconnection.f90:163-190 on the current links
+      if (infi != 0 && j >= 0 && j != pari && j != parb && a.inf[j] != 0 && !r.parallel) {
+        const int parjb = a.beh[j] - 1;
         const double l_after = (pari == r.pari && parjb == r.parjb)
                                    ? r.l_after
                                    : r.s3 + seg_len(a.x + 3 * pari, a.x + 3 * parjb);
@@ -395,15 +422,25 @@ __global__ void __launch_bounds__(256) k_precon_seq(LineArgs a, const RecEval *r
           a.beh[pari] = parjb + 1;
           a.inf[i] = j + 1;
           a.beh[j] = i + 1;
+          const int c0 = s->n_clr;
           loop_killer(a, pari);
           loop_killer(a, i);
+          const int c1 = s->n_clr;
+          int m = nchg;
+          const int mine[4] = {parjb, pari, i, j};
+          for (int k = 0; k < 4; k++, m++)
+            if (m < PC_CHG) chg[m] = mine[k];
+          for (int k = c0; k < c1; k++, m++)
+            if (m < PC_CHG) chg[m] = k < QV_LINE_CLR_CAP ? a.clr[k] : -1;
+          if (c1 > QV_LINE_CLR_CAP) m = PC_CHG + 1;  // the log lost entries: test them all
+          nchg = m;
           done++;
-          dirty = true;
         }
       }
     }
+    pos += f + 1;
   }
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     s->pc = max(nc, pc0);
     s->done += done;
   }
@@ -597,7 +634,7 @@ int qv_line_reconnect(qv_ctx *c, int *count) {
   if ((rc = compact_flags(c, n, a.flag_a, (int *)a.cand, &a.st->nc))) return rc;
   RecEval *rec = (RecEval *)c->line_rec;
   k_rec_eval<<<nblk(n, 128), 128, 0, c->stream>>>(n, a, rec);
-  k_precon_seq<<<1, 256, 0, c->stream>>>(a, rec);
+  k_precon_scan<<<1, PC_T, 0, c->stream>>>(a, rec);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 2);
   if (count) {

@@ -209,6 +209,49 @@ def test_precon_matches_oracle():
     c.close()
 
 
+def test_precon_many_pairs_and_tangle_match_oracle():
+    """The ordered pass visits only the candidates whose test can reconnect on
+    the starting links or whose slots an earlier reconnection relinked: on
+    six touching ring pairs (gaps from 2e-5 to 2.4e-4 cm, some of whose
+    reconnections leave loops that loop_killer clears, and candidates that do
+    not reconnect) next to the config-2 tangle, its links and count are the
+    oracle's precon_original bit for bit."""
+    L, W = _mods()
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).parent))
+    from test_oracle import _touching_rings
+
+    xs, infs, behs, off = [], [], [], 0
+    for k, (n, gap) in enumerate([(40, 2e-5), (12, 4e-5), (40, 1.2e-4), (8, 6e-5), (40, 2.4e-4),
+                                  (24, 1e-4)]):
+        x, inf, beh = _touching_rings(n=n, R=0.002 + 0.0004 * k, gap=gap)
+        x = x + np.array([-0.04 + 0.015 * k, 0.03, -0.02])
+        xs.append(x); infs.append(inf + off); behs.append(beh + off)
+        off += len(x)
+    w = W.tangle(0)
+    xs.append(w.x); infs.append(w.infront + off); behs.append(w.behind + off)
+    x = np.concatenate(xs); inf = np.concatenate(infs).astype(np.int32)
+    beh = np.concatenate(behs).astype(np.int32)
+    prm = dict(w.params, delta=5e-4)
+    c = L.Context(L.default_params(**prm))
+    c.set_points(x, inf, beh)
+    c.ghosts()
+    c.build_tree()
+    cl, cd = c.closest()  # pclose_tree
+    st = _ctx_state(c)
+    n0, ref = _oracle_state(st, len(x))
+    ref["closest"][:] = cl
+    ref["closestd"][:] = cd
+    cand = int(((cd < 2.5e-4) & (cd > 0) & (inf != 0)).sum())
+    k_ref = O.precon(O.params(**prm), n0, ref)
+    k = c.precon()
+    assert k == k_ref and k >= 3, (k, k_ref)
+    assert cand > 20, cand
+    _compare(c, n0, ref)
+    c.close()
+
+
 def test_step_with_reconnection_equals_the_call_sequence():
     """line_ops = 2: pinsert, candidate search, precon, premove in qv_step."""
     L, W = _mods()
