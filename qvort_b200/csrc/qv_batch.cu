@@ -30,7 +30,11 @@
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "qv_walk.cuh"
+
+namespace cg = cooperative_groups;
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
@@ -268,16 +272,14 @@ __device__ __forceinline__ void direct_item(const BatchArgs &a, float4 *tile, in
   }
 }
 
-// ---------------------------------------------------------- work kernel
-// Persistent: each warp takes the next item from a global counter until the
-// list is exhausted; the list is ordered by estimated cost, largest first.
-__global__ void k_batch_work(BatchArgs a) {
+// ---------------------------------------------------------- work items
+// Each warp takes the next item from a global counter until the list is
+// exhausted; the list is ordered by estimated cost, largest first.
+__device__ __forceinline__ void batch_items(const BatchArgs &a) {
   extern __shared__ __align__(16) unsigned char bsm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const size_t per_warp = (size_t)max(a.stk_cap * (int)sizeof(StkEnt), 32 * 4 * (int)sizeof(float4));
   unsigned char *mine = bsm + per_warp * wid;
-  if (*a.status) return;
-  if (a.nroots > 0 && a.ctl[QV_CTL_OVERFLOW]) return;
   const int *perm = a.nroots > 0 ? a.perm : nullptr;
   unsigned ev = 0, evf = 0;  // per warp: far below 2^32
   bool bad = false;
@@ -307,20 +309,24 @@ __global__ void k_batch_work(BatchArgs a) {
 // order; no images under open boundaries), u = u_LI + u_BS, then, when
 // do_ab, the AB ladder of pmotion with the system's dt (the arithmetic of
 // k_ab: exact-zero rung tests, products and sums rounded one at a time).
-__global__ void k_batch_update(int ntot, const int *__restrict__ sysof, const int4 *__restrict__ sys,
-                               const double *__restrict__ dts, const double *__restrict__ partw,
-                               const double *__restrict__ partd, double gfac_w, double gfac_d,
-                               const double *__restrict__ u_li, const int *__restrict__ inf,
-                               const int *__restrict__ ctl, int has_tree, int do_ab,
-                               int *status, double *x, double *u, double *u_bs, double *u1,
-                               double *u2, double *u3) {
-  if (has_tree && ctl[QV_CTL_OVERFLOW]) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status, BST_TREE);
-    return;
-  }
-  if (*status) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ntot || inf[i] == 0) return;
+struct UpdateArgs {
+  int ntot, do_ab;
+  const int *sysof;
+  const double *dts, *u_li;
+  double gfac_w, gfac_d;
+  double *x, *u, *u_bs, *u1, *u2, *u3;
+  int *done;  // steps applied (counted on the device)
+};
+
+__device__ __forceinline__ void batch_update_point(const BatchArgs &a, const UpdateArgs &b, int i) {
+  const int ntot = b.ntot, do_ab = b.do_ab;
+  const int *__restrict__ sysof = b.sysof;
+  const int4 *__restrict__ sys = a.sys;
+  const double *__restrict__ dts = b.dts, *__restrict__ u_li = b.u_li;
+  const double *__restrict__ partw = a.partw, *__restrict__ partd = a.partd;
+  const double gfac_w = b.gfac_w, gfac_d = b.gfac_d;
+  double *x = b.x, *u = b.u, *u_bs = b.u_bs, *u1 = b.u1, *u2 = b.u2, *u3 = b.u3;
+  if (a.inf[i] == 0) return;
   const int s = sysof[i];
   const int4 S = sys[s];
   double s0[3] = {0., 0., 0.}, s1[3] = {0., 0., 0.};
@@ -380,10 +386,9 @@ __global__ void k_batch_update(int ntot, const int *__restrict__ sysof, const in
 
 // FP32 source pack of the direct systems' slots (k_pack_sources' FP32 half):
 // x hi/lo, ghosti hi/lo, slot, s = ghosti - x.
-__global__ void k_batch_pack(int nd, const int *__restrict__ dact, const double *__restrict__ x,
-                             const double *__restrict__ gi, float *s32) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nd) return;
+__device__ __forceinline__ void batch_pack_point(int q, const int *__restrict__ dact,
+                                                 const double *__restrict__ x,
+                                                 const double *__restrict__ gi, float *s32) {
   int j = dact[q];
   double X[3], G[3];
 #pragma unroll
@@ -405,8 +410,42 @@ __global__ void k_batch_pack(int nd, const int *__restrict__ dact, const double 
   f[15] = __double2float_rn(e2);
 }
 
-__global__ void k_batch_count(const int *status, int *done) {
-  if (*status == 0) atomicAdd(done, 1);
+struct PackArgsB {
+  int nd;
+  const int *dact;
+  const double *gi;
+  float *s32;
+};
+
+// ------------------------------------------------------------ the step
+// One cooperative launch after the forest build: the FP32 source pack of the
+// direct systems; a grid barrier; the work items; a grid barrier; per point the
+// non-local velocity from its partial sums and, when do_ab, the AB update, and
+// the count of applied steps.  The barriers replace three kernel boundaries
+// (the pack, the items and the update used to be separate launches with the
+// same order).  Nothing is updated when any status bit is set (a forest or
+// stack overflow makes the host resize and run the step again).  Ghosts and
+// LIA stay separate launches before the forest build: the forest's moments
+// need the ghosts, and LIA keeps the single-system kernel's arithmetic (its
+// file is compiled without FMA contraction).
+__global__ void k_batch_step(BatchArgs a, UpdateArgs ub, PackArgsB pb) {
+  cg::grid_group grid = cg::this_grid();
+  const int nthreads = gridDim.x * blockDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool overflow = a.nroots > 0 && a.ctl[QV_CTL_OVERFLOW];
+  if (gt == 0) {
+    *a.evals = 0;
+    *a.evals_far = 0;
+    if (overflow) atomicOr(a.status, BST_TREE);
+  }
+  for (int q = gt; q < pb.nd; q += nthreads) batch_pack_point(q, pb.dact, a.x, pb.gi, pb.s32);
+  grid.sync();
+  if (*a.status == 0) batch_items(a);
+  grid.sync();
+  if (gt == 0) *a.counter = 0;  // every fetch is done: ready for the next step
+  if (*a.status) return;
+  for (int i = gt; i < ub.ntot; i += nthreads) batch_update_point(a, ub, i);
+  if (gt == 0 && ub.do_ab) atomicAdd(ub.done, 1);
 }
 
 // ================================================================ host side
@@ -495,24 +534,32 @@ static BatchArgs work_args(qv_batch *b) {
   return a;
 }
 
-static int launch_work(qv_batch *b) {
+// The cooperative step kernel (pack, items, update) with the batch's launch
+// shape; the tuner keeps that shape within what is resident at once.
+static int launch_step(qv_batch *b, int do_ab) {
   qv_ctx *c = b->c;
   BatchArgs a = work_args(b);
+  const qv_params &p = c->p;
+  UpdateArgs ub;
+  ub.ntot = b->ntot; ub.do_ab = do_ab; ub.sysof = b->d_sysof; ub.dts = b->d_dt; ub.u_li = c->u_li;
+  ub.gfac_w = p.quant_circ / 4. / QV_PI; ub.gfac_d = p.quant_circ / (4. * QV_PI);
+  ub.x = c->x; ub.u = c->u; ub.u_bs = c->u_bs; ub.u1 = c->u1; ub.u2 = c->u2; ub.u3 = c->u3;
+  ub.done = b->d_done;
+  PackArgsB pb;
+  pb.nd = b->nd; pb.dact = b->d_dact; pb.gi = c->gi; pb.s32 = b->d_src32;
   size_t smem = work_smem_per_warp(b) * b->wpb;
-  k_batch_work<<<b->bps * c->sm_count, b->wpb * 32, smem, c->stream>>>(a);
-  QV_LAUNCH_CHECK(c);
+  void *args[] = {&a, &ub, &pb};
+  QV_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_batch_step, dim3(b->bps * c->sm_count),
+                                         dim3(b->wpb * 32), args, smem, c->stream));
   QV_COUNT(c, 1);
   return QV_OK;
 }
 
 // One step (or one velocity evaluation when do_ab is 0) on the context stream,
-// with no host synchronisation.
+// with no host synchronisation: ghosts, LIA, the forest build, the step kernel.
 static int enqueue_step(qv_batch *b, int do_ab) {
   qv_ctx *c = b->c;
   int rc;
-  QV_CUDA(c, cudaMemsetAsync(b->d_counter, 0, sizeof(int), c->stream));
-  QV_CUDA(c, cudaMemsetAsync(c->evals, 0, sizeof(unsigned long long), c->stream));
-  QV_CUDA(c, cudaMemsetAsync(c->evals_far, 0, sizeof(unsigned long long), c->stream));
   if ((rc = qv_launch_ghosts(c))) return rc;
   if ((rc = qv_launch_lia(c))) return rc;
   if (b->nroots > 0) {
@@ -521,27 +568,7 @@ static int enqueue_step(qv_batch *b, int do_ab) {
     f.froot = b->d_froot; f.d_nfact = b->d_nfact;
     if ((rc = qv_forest_build(c, f))) return rc;
   }
-  if (b->nd > 0) {
-    k_batch_pack<<<nblk(b->nd, 256), 256, 0, c->stream>>>(b->nd, b->d_dact, c->x, c->gi,
-                                                          b->d_src32);
-    QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 1);
-  }
-  if ((rc = launch_work(b))) return rc;
-  const qv_params &p = c->p;
-  k_batch_update<<<nblk(b->ntot, 256), 256, 0, c->stream>>>(
-      b->ntot, b->d_sysof, b->d_sys, b->d_dt, b->d_part, b->d_part, p.quant_circ / 4. / QV_PI,
-      p.quant_circ / (4. * QV_PI), c->u_li, c->infront, c->tree.ctl, b->nroots > 0, do_ab,
-      b->d_status, c->x, c->u, c->u_bs, c->u1, c->u2, c->u3);
-  QV_LAUNCH_CHECK(c);
-  QV_COUNT(c, 1);
-  if (do_ab) {
-    // count applied steps on the device (the update skips on any status bit)
-    k_batch_count<<<1, 1, 0, c->stream>>>(b->d_status, b->d_done);
-    QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 1);
-  }
-  return QV_OK;
+  return launch_step(b, do_ab);
 }
 
 // Chunking of the single-system direct kernel for na active sources
@@ -654,6 +681,7 @@ extern "C" int qv_batch_create(const qv_params *p, int nsys, const int *offsets,
   if (e == cudaSuccess && b->nd > 0) e = cudaMalloc((void **)&b->d_src32, sizeof(float) * 16 * (size_t)b->nd);
   if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(b->d_done, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_counter, 0, sizeof(int));  // the step kernel resets it after use
   if (e != cudaSuccess) {
     cudaGetLastError();
     free_batch_tables(b);
@@ -710,7 +738,7 @@ static int size_stack(qv_batch *b) {
       drop_graph(b);
     }
     size_t smem = work_smem_per_warp(b) * 8;
-    QV_CUDA(c, cudaFuncSetAttribute(k_batch_work, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    QV_CUDA(c, cudaFuncSetAttribute(k_batch_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)std::min<size_t>(smem, 227 * 1024)));
     return QV_OK;
   }
@@ -886,7 +914,7 @@ extern "C" int qv_batch_tune(qv_batch *b, int reps, int *best_cfg, float *best_m
         size_t smem = work_smem_per_warp(b) * w;
         if (smem > 227 * 1024) continue;
         int per = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_work, w * 32, smem) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step, w * 32, smem) !=
             cudaSuccess) {
           cudaGetLastError();
           continue;
@@ -896,9 +924,8 @@ extern "C" int qv_batch_tune(qv_batch *b, int reps, int *best_cfg, float *best_m
         b->bps = s;
         float tmin = 1e30f;
         for (int r = 0; r < reps + 1; r++) {
-          QV_CUDA(c, cudaMemsetAsync(b->d_counter, 0, sizeof(int), c->stream));
           QV_CUDA(c, cudaEventRecord(e0, c->stream));
-          if ((rc = launch_work(b))) return rc;
+          if ((rc = launch_step(b, 0))) return rc;  // velocity only: the state does not move
           QV_CUDA(c, cudaEventRecord(e1, c->stream));
           QV_CUDA(c, cudaEventSynchronize(e1));
           float ms = 0.f;
@@ -931,6 +958,17 @@ extern "C" int qv_batch_set_config(qv_batch *b, int warps_per_block, int blocks_
   if (!b || warps_per_block < 1 || warps_per_block > 32 || blocks_per_sm < 1 || order < 0 || order > 1)
     return QV_ERR_ARG;
   qv_ctx *c = b->c;
+  // the step kernel is a cooperative launch: all its blocks must fit at once
+  int per = 0;
+  size_t smem = work_smem_per_warp(b) * warps_per_block;
+  if (smem > 227 * 1024 ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_step, warps_per_block * 32, smem) !=
+          cudaSuccess ||
+      per < blocks_per_sm) {
+    cudaGetLastError();
+    return qv_fail(c, QV_ERR_ARG, "qv_batch_set_config: %d blocks of %d warps per SM do not fit (%d do)",
+                   blocks_per_sm, warps_per_block, per);
+  }
   b->wpb = warps_per_block;
   b->bps = blocks_per_sm;
   if (order != b->order) {
