@@ -704,23 +704,32 @@ __global__ void __launch_bounds__(BT) k_build_local(BuildArgs a) {
 // circ = (circ + ghosti) - x (src/tree.f90:160).  Every lane runs the same
 // add-then-subtract, the subtrahend being +0 outside lanes 3-5 (s - 0 = s
 // exactly), so the warp never splits into two serialised paths; each group
-// of four points is loaded ahead of its eight dependent roundings (measured
-// on B200: 19 cycles per point, the floor of two 10-cycle FP64 roundings).
+// of four points is loaded while the previous group's eight dependent
+// roundings run, so the chain waits on the FP64 adds alone.
 __device__ __forceinline__ double chain15(double acc, const double *rows, int stride, int m,
                                           int lane) {
   const bool cl = lane >= 3 && lane < 6;
   const double *pa = rows + lane, *pz = rows + (cl ? lane - 3 : lane);
   int q = 0;
-  for (; q + 4 <= m; q += 4) {
-    double a0 = pa[stride * q], a1 = pa[stride * (q + 1)];
-    double a2 = pa[stride * (q + 2)], a3 = pa[stride * (q + 3)];
-    double z0 = pz[stride * q], z1 = pz[stride * (q + 1)];
-    double z2 = pz[stride * (q + 2)], z3 = pz[stride * (q + 3)];
-    if (!cl) { z0 = 0.; z1 = 0.; z2 = 0.; z3 = 0.; }
-    acc = __dsub_rn(__dadd_rn(acc, a0), z0);
-    acc = __dsub_rn(__dadd_rn(acc, a1), z1);
-    acc = __dsub_rn(__dadd_rn(acc, a2), z2);
-    acc = __dsub_rn(__dadd_rn(acc, a3), z3);
+  if (m >= 4) {
+    // the next group's loads go out before this group's dependent roundings
+    double a[4], z[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) { a[u] = pa[stride * u]; z[u] = cl ? pz[stride * u] : 0.; }
+    for (q = 4; q + 4 <= m; q += 4) {
+      double na[4], nz[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        na[u] = pa[stride * (q + u)];
+        nz[u] = cl ? pz[stride * (q + u)] : 0.;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) acc = __dsub_rn(__dadd_rn(acc, a[u]), z[u]);
+#pragma unroll
+      for (int u = 0; u < 4; u++) { a[u] = na[u]; z[u] = nz[u]; }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) acc = __dsub_rn(__dadd_rn(acc, a[u]), z[u]);
   }
   for (; q < m; q++) acc = __dsub_rn(__dadd_rn(acc, pa[stride * q]), cl ? pz[stride * q] : 0.);
   return acc;
