@@ -22,9 +22,9 @@
 // Work split: blockIdx.x = tile of 128 targets, blockIdx.y = chunk of sources;
 // per-chunk partial sums go to a buffer and are added in fixed chunk order,
 // so results are deterministic.
-#include <cstdlib>
 
 #include "qv_internal.cuh"
+#include "qv_tma.cuh"
 
 static inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
@@ -254,7 +254,6 @@ __device__ __forceinline__ double shifted(double v, int a, double L) {
 // (QV_STAGE_WAIT_NS of wall time, and an iteration cap); a wait that runs out
 // sets QV_STAT_STAGE in the status word and the block stops summing, so a
 // copy that never lands ends the launch with an error, not a hang.
-#define QV_STAGE_WAIT_NS 1000000000ull  // 1 s
 
 // Test hook (qv_test_stage_timeout): nonzero makes every tile acquire report
 // a wait that ran out, without waiting, so that the error path -- drain the
@@ -265,62 +264,6 @@ static int g_stage_fail = 0;
 extern "C" int qv_test_stage_timeout(int enable) {
   g_stage_fail = enable ? 1 : 0;
   return QV_OK;
-}
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(unsigned bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-}
-
-// make the initialised barriers visible to the copy engine before first use
-__device__ __forceinline__ void mbar_init_fence() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// one thread: arm the barrier for `bytes` and start the copy
-__device__ __forceinline__ void stage_copy(unsigned dst, const void *src, unsigned bytes,
-                                           unsigned bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(dst),
-      "l"(src), "r"(bytes), "r"(bar)
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(done)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-__device__ __forceinline__ unsigned long long wall_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// wait for the barrier's phase of parity `parity` to complete, giving up
-// after QV_STAGE_WAIT_NS or 2^30 polls
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = wall_ns();
-  for (unsigned it = 0; it < (1u << 30); it++) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if (wall_ns() - t0 > QV_STAGE_WAIT_NS) break;
-  }
-  return false;
 }
 
 // Double-buffered tile pipeline over sources [j0, j1) of a pack with 64-byte
@@ -636,26 +579,13 @@ __global__ void __launch_bounds__(DTILE) k_direct32(int na, const int *__restric
   }
 }
 
-// Targets per thread of the mixed kernel.
-static int direct_nt() {
-  static int nt = 0;
-  if (!nt) {
-    const char *e = getenv("QV_DIRECT_NT");
-    nt = (e && atoi(e) == 2) ? 2 : 1;
-  }
-  return nt;
-}
-
 template <int BC>
-static void launch_direct32(int nt, dim3 grid, cudaStream_t s, int na, const int *act,
-                            const double *x, const int *beh, const float *src, int chunk_len,
-                            double L, double *part, int *status, int stage_fail) {
-  if (nt == 2)
-    k_direct32<BC, 2><<<grid, DTILE, 0, s>>>(na, act, x, beh, src, chunk_len, L, part, status,
-                                             stage_fail);
-  else
-    k_direct32<BC, 1><<<grid, DTILE, 0, s>>>(na, act, x, beh, src, chunk_len, L, part, status,
-                                             stage_fail);
+static void launch_direct32(dim3 grid, cudaStream_t s, int na, const int *act, const double *x,
+                            const int *beh, const float *src, int chunk_len, double L,
+                            double *part, int *status, int stage_fail) {
+  // one target per thread: two (NT = 2) took 17 % longer on the tangle
+  k_direct32<BC, 1><<<grid, DTILE, 0, s>>>(na, act, x, beh, src, chunk_len, L, part, status,
+                                           stage_fail);
 }
 
 // u_bs = s0 + s1, u = (u_li + s0) + s1, in fixed chunk order.
@@ -695,8 +625,7 @@ int qv_launch_direct(qv_ctx *c) {
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 1);
   bool mixed = c->p.precision == QV_PREC_MIXED;
-  const int nt = mixed ? direct_nt() : 1;  // targets per thread
-  int bx = nblk(na, DTILE * nt);
+  int bx = nblk(na, DTILE);
   // enough chunks to fill ~4 blocks per SM, each chunk at least 4 tiles
   int want = (4 * c->sm_count + bx - 1) / bx;
   int maxch = max(1, na / (4 * DTILE));
@@ -716,7 +645,7 @@ int qv_launch_direct(qv_ctx *c) {
 #define QV_DIRECT_CASE(BCV)                                                                   \
   case BCV:                                                                                   \
     if (mixed)                                                                                \
-      launch_direct32<BCV>(nt, grid, c->stream, na, c->act, c->x, c->behind, c->src32,       \
+      launch_direct32<BCV>(grid, c->stream, na, c->act, c->x, c->behind, c->src32,           \
                                                      chunk_len, L, part, c->dstatus,          \
                                                      g_stage_fail);                           \
     else                                                                                      \
@@ -778,8 +707,7 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
   int *stat = blk + nb + 1;
   if (cudaMemsetAsync(stat, 0, sizeof(int), s) != cudaSuccess) return QV_ERR_CUDA;
   k_pack_sources<<<tb, 256, 0, s>>>(na, act, x, gi, src64, src32);
-  const int nt = mixed ? direct_nt() : 1;
-  int bx = nblk(na, DTILE * nt);
+  int bx = nblk(na, DTILE);
   int want = (4 * sm_count + bx - 1) / bx;
   int maxch = max(1, na / (4 * DTILE));
   int nchunk = max(1, min(min(want, maxch), max_chunks));
@@ -791,7 +719,7 @@ int qv_direct_scratch(cudaStream_t s, const qv_params *p, int sm_count, int n, c
 #define QV_DIRECT_SCRATCH_CASE(BCV)                                                      \
   case BCV:                                                                              \
     if (mixed)                                                                           \
-      launch_direct32<BCV>(nt, grid, s, na, act, x, beh, src32, chunk_len, L, part,      \
+      launch_direct32<BCV>(grid, s, na, act, x, beh, src32, chunk_len, L, part,          \
                                              stat, g_stage_fail);                        \
     else                                                                                 \
       k_direct64<BCV><<<grid, DTILE, 0, s>>>(na, act, x, beh, src64, chunk_len, L, part,  \
