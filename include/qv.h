@@ -355,6 +355,14 @@ int qv_test_stage_timeout(int enable);
  * widens the estimate's bound, so that a test can make root tests undecided
  * and exercise the fix-up.  Process-wide. */
 int qv_test_root_speculation(int mode, double bound_scale);
+
+/* Test hook, no counterpart in the reference: when a mixed-precision Tree
+ * build takes the root children's long circ and Cij sums off the path to the
+ * walk.  mode -1 (the default): builds of at least 65536 slots pack the
+ * children of more than 512 points late, and the walk adds their far-field
+ * terms after its launch (results within the mixed walk's rounding of the
+ * other path, same evaluation counts); 0: never; 1: always.  Process-wide. */
+int qv_test_late_level1(int mode);
 /* The number of root tests the last estimate-started build left undecided
  * (see qv_test_root_speculation; 0 when the build waited for the exact sum). */
 int qv_root_undecided(qv_ctx *ctx, int *count);

@@ -99,9 +99,9 @@ static void free_tree(TreeBuf &t) {
   if (t.h_ctl) cudaFreeHost(t.h_ctl);
   if (t.ev_ctl) cudaEventDestroy(t.ev_ctl);
   void *ps[] = {t.pos, t.width, t.cent, t.circ, t.C, t.count, t.start, t.parent, t.child_first,
-                t.nchild, t.first, t.level, t.digit, t.cmask, t.w64, t.p64, t.w32, t.c32, t.p32, t.leaf_of,
+                t.nchild, t.first, t.level, t.digit, t.cmask, t.w64, t.p64, t.w32, t.c32, t.p32_raw, t.leaf_of,
                 t.ord, t.nodeA, t.nodeB, t.dig, t.rnk, t.cnt9, t.rs9, t.chunk9, t.ctl, t.permb,
-                t.root_est, t.root_ctl, t.root_unc, t.root_part, t.root_xc};
+                t.root_est, t.root_ctl, t.root_unc, t.root_part, t.root_xc, t.l1list};
   for (void *q : ps)
     if (q) cudaFree(q);
   t = TreeBuf();
@@ -127,6 +127,8 @@ static void free_points(qv_ctx *c) {
 extern "C" int qv_destroy(qv_ctx *c) {
   QV_CHECK_CTX(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int k = 0; k < 5; k++)  // chains of a tree that no reader joined
+    if (c->aux[k]) cudaStreamSynchronize(c->aux[k]);
   free_tree(c->tree);
   free_points(c);
   if (c->evals) cudaFree(c->evals);
@@ -152,12 +154,15 @@ extern "C" int qv_destroy(qv_ctx *c) {
   if (c->ev_line) cudaEventDestroy(c->ev_line);
   if (c->walk_part) cudaFree(c->walk_part);
   if (c->walk_next) cudaFree(c->walk_next);
+  if (c->walk_defer) cudaFree(c->walk_defer);
   if (c->lk) cudaFree(c->lk);
   if (c->h_lk) cudaFreeHost(c->h_lk);
-  for (int k = 0; k < 3; k++) {
+  for (int k = 0; k < 5; k++) {
     if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
     if (c->ev_join[k]) cudaEventDestroy(c->ev_join[k]);
   }
+  if (c->ev_l1) cudaEventDestroy(c->ev_l1);
+  if (c->ev_l1list) cudaEventDestroy(c->ev_l1list);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_fork2) cudaEventDestroy(c->ev_fork2);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
@@ -564,6 +569,9 @@ extern "C" int qv_build_tree(qv_ctx *c) {
   int rc = qv_launch_tree_build(c);
   if (rc) return rc;
   QV_CUDA(c, cudaStreamSynchronize(c->stream));
+  // the late level-1 chains read x and the ghosts, which the caller may
+  // overwrite once this returns
+  if (c->tree.l1_pending) QV_CUDA(c, cudaEventSynchronize(c->ev_l1));
   return QV_OK;
 }
 

@@ -96,7 +96,8 @@ struct TreeBuf {
   WPay64 *p64 = nullptr;
   WNode32 *w32 = nullptr;
   SNode32 *c32 = nullptr;
-  WPay32 *p32 = nullptr;
+  WPay32 *p32 = nullptr;  // = p32_raw + 1: node 1's payload starts a 128-byte line
+  WPay32 *p32_raw = nullptr;
   // build scratch
   int *ord = nullptr;       // cap_levels * cap_pts: per-level orders
   int *nodeA = nullptr, *nodeB = nullptr;  // node of each position
@@ -123,7 +124,30 @@ struct TreeBuf {
   double *root_part = nullptr;  // per-block partial sums of the estimate
   double *root_xc = nullptr;    // the active positions in active order (the chain's input)
   bool root_pending = false;    // headers hold the estimate
+  // Late level-1 moments.  The circ and Cij chains of the root's children of
+  // more than QV_L1_BIG points are the longest sequential sums of a large tree
+  // (two dependent roundings per point).  In a mixed-precision Tree build of at
+  // least QV_L1_LATE_MIN slots they run on a side stream while the walk runs:
+  // those nodes' headers (centroid from its own, shorter chain) are packed with
+  // the rest, their payloads once the chains end (event ev_l1 of the context).
+  // l1list = [count, nodes...].
+  int *l1list = nullptr;
+  bool l1_late = false;     // this tree's big level-1 payloads come late
+  bool l1_pending = false;  // ... and no reader has joined them yet
 };
+#define QV_L1_LATE_MIN 65536  // slots from which a mixed Tree build packs level 1 late
+#define QV_L1_BIG 512         // level-1 nodes of more points take the late path
+
+// Whether root child k (1 <= k < l1_end, the level-1 nodes) takes the late
+// path: it and the node that shares its 128-byte line of FP32 payloads (the
+// walk reads those through L1, and node 1 starts a line) hold more than
+// QV_L1_BIG points each.  A line that an early reader brought into L1 then
+// never also holds a late payload.
+__host__ __device__ inline bool qv_l1_late(int k, int l1_end, int count_k, int count_pair) {
+  const int j = ((k - 1) ^ 1) + 1;  // its line partner
+  return k >= 1 && k < l1_end && j < l1_end && count_k > QV_L1_BIG && count_pair > QV_L1_BIG;
+}
+__host__ __device__ inline int qv_l1_pair(int k) { return ((k - 1) ^ 1) + 1; }
 #define QV_ROOT_UNC_CAP 8192
 #define QV_ROOT_SPEC_MIN 32768  // slots from which the root starts from its estimate
 #define QV_ROOT_EST_BLOCKS 296
@@ -193,8 +217,11 @@ struct qv_ctx {
   double phase_ms[PH_N] = {};
   long long launches = 0;
   unsigned long long *evals_far = nullptr;
-  cudaStream_t aux[3] = {nullptr, nullptr, nullptr};  // side streams for independent chains
-  cudaEvent_t ev_fork = nullptr, ev_fork2 = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t aux[5] = {};  // side streams for independent chains
+  cudaEvent_t ev_fork = nullptr, ev_fork2 = nullptr, ev_join[5] = {};
+  cudaEvent_t ev_l1 = nullptr, ev_l1list = nullptr;  // late level-1 moments (TreeBuf)
+  unsigned char *walk_defer = nullptr;  // per (task slot, target): deferred level-1 far cells
+  size_t walk_defer_bytes = 0;
   long long last_leaf = 0, last_far = 0;
   char err[512] = {0};
 };
@@ -222,8 +249,9 @@ int qv_launch_ghosts(qv_ctx *c);
 int qv_launch_lia(qv_ctx *c);
 int qv_launch_direct(qv_ctx *c);
 int qv_launch_tree_build(qv_ctx *c);
-// Join the exact root centroid and re-pack the root with it (no-op when it is
-// in already).  Every reader of the tree other than the velocity walk calls it.
+// Join the exact root centroid and re-pack the root with it, and join the late
+// level-1 moments and payloads (no-op when both are in already).  Every reader
+// of the tree calls it; the mixed walk after its launch.
 int qv_tree_finalize_root(qv_ctx *c);
 int qv_launch_walk(qv_ctx *c);
 int qv_launch_ab(qv_ctx *c);

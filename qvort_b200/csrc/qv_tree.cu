@@ -86,7 +86,8 @@ struct PackArgs {
   int n_leaf;
   int full;  // also the FP64 walk payload and the search header (a forest needs neither)
 };
-__device__ void pack_one(const PackArgs &P, int k);
+__device__ void pack_one(const PackArgs &P, int k, int what);
+static_assert(QV_L1_BIG == LCH, "the late level-1 nodes are the big-chain nodes of level 1");
 
 // packed per-digit counters: digits 0..4 in lo (12-bit fields), 5..8 in hi
 struct Pack2 {
@@ -849,13 +850,23 @@ __global__ void __launch_bounds__(MW * 32) k_moments(const int *__restrict__ ctl
 // among the nodes of the grid-wide levels (glob) or of the whole tree.  Nodes
 // of more than BIGN points all come from the grid-wide levels, which are
 // complete once k_build ends (the block-local levels may still be adding).
+// late: 0 = every node, 1 = all but the late root children (qv_l1_late),
+// 2 = those only.
 __global__ void k_list_big(const int *__restrict__ ctl, int cap_nodes, int k0,
                            const int *__restrict__ count, int *list, int *nlist, int lo, int hi,
-                           int glob) {
+                           int glob, int late) {
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[glob ? CTL_NGLOB : CTL_NNODES], cap_nodes);
-  for (int k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
-    if (count[k] > lo && count[k] <= hi) list[atomicAdd(nlist, 1)] = k;
+  const int l1_end = ctl[CTL_LVL + 2];  // the first node of level 2
+  for (int k = k0 + blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x) {
+    if (!(count[k] > lo && count[k] <= hi)) continue;
+    if (late) {
+      const int j = qv_l1_pair(k);
+      const bool lk = qv_l1_late(k, l1_end, count[k], j < n_nodes ? count[j] : 0);
+      if (lk != (late == 2)) continue;
+    }
+    list[atomicAdd(nlist, 1)] = k;
+  }
 }
 
 // One block per node with more than BIGN points: warps 1.. gather x, ghosti and
@@ -869,7 +880,10 @@ __global__ void __launch_bounds__(MBT) k_moments_big(const int *__restrict__ lis
                                                      const int *__restrict__ ord, int cap_pts,
                                                      const double *__restrict__ x,
                                                      const double *__restrict__ gi, double *cent,
-                                                     double *circ, double *C, int *first) {
+                                                     double *circ, double *C, int *first,
+                                                     int l1_late, PackArgs pk, int do_pack) {
+  // l1_late: the late level-1 chains, whose centroid (and first point)
+  // k_moments_cent stores; only circ and Cij are stored here.
   extern __shared__ double mb[];  // [2][MC][15]
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nl = *nlist;
@@ -912,11 +926,90 @@ __global__ void __launch_bounds__(MBT) k_moments_big(const int *__restrict__ lis
       int ci = (lane - 6) / 3, ck = (lane - 6) % 3;
       double cen = __shfl_sync(0xffffffffu, cm, lane >= 6 && lane < 15 ? ci : 0);
       double cir = __shfl_sync(0xffffffffu, acc, lane >= 6 && lane < 15 ? 3 + ck : 0);
-      if (lane < 3) cent[3 * k + lane] = cm;
-      else if (lane < 6) circ[3 * k + lane - 3] = acc;
-      else if (lane < 15) C[9 * k + 3 * ci + ck] = __dsub_rn(acc, __dmul_rn(cen, cir));
-      if (lane == 0) first[k] = o[0];
+      if (lane < 3) {
+        if (!l1_late) cent[3 * k + lane] = cm;
+      } else if (lane < 6) {
+        circ[3 * k + lane - 3] = acc;
+      } else if (lane < 15) {
+        C[9 * k + 3 * ci + ck] = __dsub_rn(acc, __dmul_rn(cen, cir));
+      }
+      if (lane == 0 && !l1_late) first[k] = o[0];
+      __syncwarp();
+      // the node's walk packs (a late root child: its payload)
+      if (do_pack && lane == 0) pack_one(pk, k, l1_late ? 2 : 3);
     }
+  }
+}
+
+// The centroid chains alone (one rounding per point: half the circ chain's
+// latency) of the nodes of list = [count, nodes...], and their walk headers:
+// warps 1.. stage x in chunks of MCC points, lanes 0..2 of warp 0 sum it, in
+// the same order and roundings as chain15's lanes 0..2, so the value is the one
+// k_moments_big computes.  One add per point leaves the chain only ~8 cycles a
+// point, so the chunks are larger than k_moments_big's and each group of eight
+// points is loaded while the previous group's adds run.
+#define MCC 1024
+__global__ void __launch_bounds__(MBT) k_moments_cent(const int *__restrict__ ctl,
+                                                      const int *__restrict__ list,
+                                                      const int *__restrict__ level,
+                                                      const int *__restrict__ start,
+                                                      const int *__restrict__ count,
+                                                      const int *__restrict__ ord, int cap_pts,
+                                                      const double *__restrict__ x, double *cent,
+                                                      int *first, PackArgs pk) {
+  extern __shared__ double mb[];  // [2][MCC][3]
+  if (ctl[CTL_OVERFLOW]) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nl = list[0];
+  for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+    const int k = list[1 + li];
+    const int n = count[k];
+    const int *o = ord + (size_t)level[k] * cap_pts + start[k];
+    const int nch = (n + MCC - 1) / MCC;
+    auto produce = [&](int ch, double *dst) {
+      const int base = ch * MCC, m = min(MCC, n - base);
+      for (int q = threadIdx.x - 32; q < m; q += blockDim.x - 32) {
+        const int idx = o[base + q];
+#pragma unroll
+        for (int c = 0; c < 3; c++) dst[3 * q + c] = x[3 * idx + c];
+      }
+    };
+    __syncthreads();
+    if (wid > 0) produce(0, mb);
+    __syncthreads();
+    double acc = 0.;
+    for (int ch = 0; ch < nch; ch++) {
+      double *cur = mb + (ch & 1) * MCC * 3;
+      if (wid > 0) {
+        if (ch + 1 < nch) produce(ch + 1, mb + ((ch + 1) & 1) * MCC * 3);
+      } else if (lane < 3) {
+        const int m = min(MCC, n - ch * MCC);
+        const double *b = cur + lane;
+        int q = 0;
+        if (m >= 8) {
+          double a[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) a[u] = b[3 * u];
+          for (q = 8; q + 8 <= m; q += 8) {
+            double na[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) na[u] = b[3 * (q + u)];
+#pragma unroll
+            for (int u = 0; u < 8; u++) acc = __dadd_rn(acc, a[u]);
+#pragma unroll
+            for (int u = 0; u < 8; u++) a[u] = na[u];
+          }
+#pragma unroll
+          for (int u = 0; u < 8; u++) acc = __dadd_rn(acc, a[u]);
+        }
+        for (; q < m; q++) acc = __dadd_rn(acc, b[3 * q]);
+      }
+      __syncthreads();
+    }
+    if (wid == 0 && lane < 3) cent[3 * k + lane] = __ddiv_rn(acc, (double)n);
+    if (threadIdx.x == 0) first[k] = o[0];
+    __syncwarp();
+    if (threadIdx.x == 0) pack_one(pk, k, 1);  // the headers; the payload comes late
   }
 }
 
@@ -1051,12 +1144,23 @@ extern "C" int qv_test_root_speculation(int mode, double bound_scale) {
   return QV_OK;
 }
 
+// When a mixed Tree build packs the big root children late: by size (-1;
+// builds of at least QV_L1_LATE_MIN slots), never (0) or always (1).  Set only
+// by the test hook qv_test_late_level1.
+static int g_l1_late_mode = -1;
+
+extern "C" int qv_test_late_level1(int mode) {
+  if (mode < -1 || mode > 1) return QV_ERR_ARG;
+  g_l1_late_mode = mode;
+  return QV_OK;
+}
+
 // Put the exact root centroid in (cent[0..2] and the root's headers) once its
 // chain has been joined.
 __global__ void k_root_pack(PackArgs pk, const double *__restrict__ exact, double *cent) {
   if (threadIdx.x == 0) {
     for (int c = 0; c < 3; c++) cent[c] = exact[c];
-    pack_one(pk, 0);
+    pack_one(pk, 0, 3);
   }
 }
 
@@ -1090,7 +1194,7 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
-                          WPay32 *p32, int *leaf_of, int n_leaf, int full);
+                          WPay32 *p32, int *leaf_of, int n_leaf, int full, int what);
 
 __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ width, const double *__restrict__ cent,
@@ -1101,72 +1205,79 @@ __device__ void pack_node(int k, int nroots, const double *__restrict__ pos,
                           const double *__restrict__ x, const double *__restrict__ gi,
                           const int *__restrict__ inf, const int *__restrict__ beh,
                           double theta, int extra, WNode64 *w64, WPay64 *p64, WNode32 *w32, SNode32 *c32,
-                          WPay32 *p32, int *leaf_of, int n_leaf, int full) {
-  WNode64 h;
-  h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
-  h.width = width[k];
-  // geo_dist = |cent - (pos + width/2.)|, src/tree.f90:355-357
-  double hw = width[k] / 2.;
-  double g0 = __dsub_rn(h.cx, __dadd_rn(pos[3 * k], hw));
-  double g1 = __dsub_rn(h.cy, __dadd_rn(pos[3 * k + 1], hw));
-  double g2 = __dsub_rn(h.cz, __dadd_rn(pos[3 * k + 2], hw));
-  h.geo = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(g0, g0), __dmul_rn(g1, g1)), __dmul_rn(g2, g2)));
-  // a root's count is its system's slot count, empty slots included
+                          WPay32 *p32, int *leaf_of, int n_leaf, int full, int what) {
+  // what: 1 = the headers (w64, w32, c32), 2 = the payloads (p64, p32), 3 = both.
+  // A payload alone (a late level-1 node: more than one point) reads only the
+  // node's count and moments.
   const bool root = k < nroots;
-  int cnt = count[k];
-  h.count = cnt;
-  h.child_first = child_first[k];
-  h.nchild = nchild[k];
-  int f = first[k];
-  h.finf = (f >= 0) ? inf[f] : 0;
-  h.jb = (f >= 0 && h.finf > 0) ? beh[h.finf - 1] : 0;
-  h.first = f;
-  w64[k] = h;
-  if (leaf_of && cnt == 1 && f >= 0 && f < n_leaf) leaf_of[f] = k;
+  const int cnt = count[k];
+  if (what & 1) {
+    WNode64 h;
+    h.cx = cent[3 * k]; h.cy = cent[3 * k + 1]; h.cz = cent[3 * k + 2];
+    h.width = width[k];
+    // geo_dist = |cent - (pos + width/2.)|, src/tree.f90:355-357
+    double hw = width[k] / 2.;
+    double g0 = __dsub_rn(h.cx, __dadd_rn(pos[3 * k], hw));
+    double g1 = __dsub_rn(h.cy, __dadd_rn(pos[3 * k + 1], hw));
+    double g2 = __dsub_rn(h.cz, __dadd_rn(pos[3 * k + 2], hw));
+    h.geo = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(g0, g0), __dmul_rn(g1, g1)), __dmul_rn(g2, g2)));
+    // a root's count is its system's slot count, empty slots included
+    h.count = cnt;
+    h.child_first = child_first[k];
+    h.nchild = nchild[k];
+    int f = first[k];
+    h.finf = (f >= 0) ? inf[f] : 0;
+    h.jb = (f >= 0 && h.finf > 0) ? beh[h.finf - 1] : 0;
+    h.first = f;
+    w64[k] = h;
+    if (leaf_of && cnt == 1 && f >= 0 && f < n_leaf) leaf_of[f] = k;
+    WNode32 h32;
+    split2(h.cx, h32.ch[0], h32.cl[0]);
+    split2(h.cy, h32.ch[1], h32.cl[1]);
+    split2(h.cz, h32.ch[2], h32.cl[2]);
+    // Opening test of src/tree.f90:354-365,394: theta = w/(d - geo) < tree_theta
+    // (extra correction) or w/d < tree_theta.  For d > geo it is d > geo + w/theta.
+    // The centroid lies in its cell, so geo <= (sqrt 3 / 2) w, and d <= geo then
+    // gives w/d >= 2/sqrt 3: the cell opens whenever theta < 2/sqrt 3.  Under that
+    // condition the test is d^2 > rc2 exactly; the walk compares in FP32 with a
+    // margin and falls back to the FP64 expression near the threshold.  The root
+    // (centroid anywhere, zero moments) always takes the FP64 path.
+    bool fast = theta > 0. && (!extra || theta < 1.15);
+    h32.count = cnt;
+    h32.child_first = h.child_first;
+    h32.nchild = h.nchild;
+    h32.jb = h.jb;
+    if (root || !fast) {
+      h32.rhi = h32.rlo = -1.f;
+    } else {
+      double rc = (extra ? h.geo : 0.) + h.width / theta;
+      double rc2 = rc * rc;
+      h32.rhi = __double2float_rn(rc2 * (1. + 4e-6));
+      h32.rlo = __double2float_rn(rc2 * (1. - 4e-6));
+    }
+    w32[k] = h32;
+    if (full) {  // the candidate search's header
+      SNode32 s32;
+      for (int c = 0; c < 3; c++) {
+        s32.ch[c] = h32.ch[c];
+        s32.cl[c] = h32.cl[c];
+        s32.lo[c] = __double2float_rd(pos[3 * k + c]);
+      }
+      double w4 = 4. * h.width * h.width;  // (2 width)^2
+      s32.rhi = __double2float_rn(w4 * (1. + 4e-6));
+      s32.rlo = __double2float_rn(w4 * (1. - 4e-6));
+      s32.w = __double2float_ru(h.width);
+      s32.count = cnt;
+      s32.child_first = h.child_first;
+      s32.nchild = h.nchild;
+      s32.cmask = cmask[k];
+      c32[k] = s32;
+    }
+  }
+  if (!(what & 2)) return;
   WPay64 q;
   WPay32 r;
-  WNode32 h32;
-  split2(h.cx, h32.ch[0], h32.cl[0]);
-  split2(h.cy, h32.ch[1], h32.cl[1]);
-  split2(h.cz, h32.ch[2], h32.cl[2]);
-  // Opening test of src/tree.f90:354-365,394: theta = w/(d - geo) < tree_theta
-  // (extra correction) or w/d < tree_theta.  For d > geo it is d > geo + w/theta.
-  // The centroid lies in its cell, so geo <= (sqrt 3 / 2) w, and d <= geo then
-  // gives w/d >= 2/sqrt 3: the cell opens whenever theta < 2/sqrt 3.  Under that
-  // condition the test is d^2 > rc2 exactly; the walk compares in FP32 with a
-  // margin and falls back to the FP64 expression near the threshold.  The root
-  // (centroid anywhere, zero moments) always takes the FP64 path.
-  bool fast = theta > 0. && (!extra || theta < 1.15);
-  h32.count = cnt;
-  h32.child_first = h.child_first;
-  h32.nchild = h.nchild;
-  h32.jb = h.jb;
-  if (root || !fast) {
-    h32.rhi = h32.rlo = -1.f;
-  } else {
-    double rc = (extra ? h.geo : 0.) + h.width / theta;
-    double rc2 = rc * rc;
-    h32.rhi = __double2float_rn(rc2 * (1. + 4e-6));
-    h32.rlo = __double2float_rn(rc2 * (1. - 4e-6));
-  }
-  w32[k] = h32;
-  if (full) {  // the candidate search's header
-    SNode32 s32;
-    for (int c = 0; c < 3; c++) {
-      s32.ch[c] = h32.ch[c];
-      s32.cl[c] = h32.cl[c];
-      s32.lo[c] = __double2float_rd(pos[3 * k + c]);
-    }
-    double w4 = 4. * h.width * h.width;  // (2 width)^2
-    s32.rhi = __double2float_rn(w4 * (1. + 4e-6));
-    s32.rlo = __double2float_rn(w4 * (1. - 4e-6));
-    s32.w = __double2float_ru(h.width);
-    s32.count = cnt;
-    s32.child_first = h.child_first;
-    s32.nchild = h.nchild;
-    s32.cmask = cmask[k];
-    c32[k] = s32;
-  }
+  const int f = cnt == 1 ? first[k] : -1;
   if (cnt == 1 && f >= 0) {
     for (int c = 0; c < 3; c++) {
       q.a[c] = x[3 * f + c];
@@ -1281,24 +1392,36 @@ __global__ void k_forest_init(int nroots, const int4 *__restrict__ roots, double
   for (size_t q = tid; q < ncnt9; q += stride) cnt9[q] = 0;
 }
 
-__device__ void pack_one(const PackArgs &P, int k) {
+__device__ void pack_one(const PackArgs &P, int k, int what) {
   pack_node(k, P.nroots, P.pos, P.width, P.cent, P.circ, P.C, P.count, P.child_first, P.nchild,
             P.cmask, P.first, P.x, P.gi, P.inf, P.beh, P.theta, P.extra, P.w64, P.p64, P.w32,
-            P.c32, P.p32, P.leaf_of, P.n_leaf, P.full);
+            P.c32, P.p32, P.leaf_of, P.n_leaf, P.full, what);
 }
 
-// Walk packs of every node once all moments are in.  root_cent: the single
-// tree's root centroid, read here in place of cent[0..2] (the chain that makes
-// it runs on its own stream), or null when the roots' centroids are in place.
+
+
+// Walk packs of the nodes of at most max_count points once their moments are
+// in (a forest: every node, max_count = INT_MAX; a single tree: the nodes
+// k_moments sums, the other kernels pack theirs).  root_cent: the single tree's
+// root centroid, read here in place of cent[0..2] (the chain that makes it runs
+// on its own stream), or null when the roots' centroids are in place.
 __global__ void k_pack_nodes(const int *__restrict__ ctl, int cap_nodes, PackArgs pk,
-                             const double *root_cent, double *cent) {
+                             const double *root_cent, double *cent, int max_count) {
   if (ctl[CTL_OVERFLOW]) return;
   const int n_nodes = min(ctl[CTL_NNODES], cap_nodes);
   if (root_cent && blockIdx.x == 0 && threadIdx.x < 3) cent[threadIdx.x] = root_cent[threadIdx.x];
   __syncthreads();
   // node 0 falls to block 0, which made the copy before the barrier
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_nodes; k += gridDim.x * blockDim.x)
-    pack_one(pk, k);
+    if (pk.count[k] <= max_count) pack_one(pk, k, 3);
+}
+
+// The late payloads are in (k_moments_big packs them): set the ready flag of
+// list = [count, nodes..., flag at 15] (release), which the mixed walk's first
+// launch reads before it takes a task that needs them.
+__global__ void k_l1_ready(int *list) {
+  __threadfence();
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(list + 15), "r"(1) : "memory");
 }
 
 // --------------------------------------------------------------- host side
@@ -1326,6 +1449,8 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
   }
   if (!t.ctl)
     if ((rc = qv_grow(c, (void **)&t.ctl, sizeof(int) * CTL_SIZE))) return rc;
+  if (!t.l1list)
+    if ((rc = qv_grow(c, (void **)&t.l1list, sizeof(int) * 16))) return rc;
   if (cap_nodes > t.cap_nodes) {
     size_t m = cap_nodes;
     if ((rc = qv_grow(c, (void **)&t.pos, sizeof(double) * 3 * m))) return rc;
@@ -1346,7 +1471,8 @@ static int tree_reserve(qv_ctx *c, int n_act, int cap_nodes, int cap_levels) {
     if ((rc = qv_grow(c, (void **)&t.p64, sizeof(WPay64) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.w32, sizeof(WNode32) * m))) return rc;
     if ((rc = qv_grow(c, (void **)&t.c32, sizeof(SNode32) * m))) return rc;
-    if ((rc = qv_grow(c, (void **)&t.p32, sizeof(WPay32) * m))) return rc;
+    if ((rc = qv_grow(c, (void **)&t.p32_raw, sizeof(WPay32) * (m + 1)))) return rc;
+    t.p32 = t.p32_raw + 1;
     t.cap_nodes = cap_nodes;
   }
   return QV_OK;
@@ -1356,10 +1482,17 @@ int qv_aux_streams(qv_ctx *c) {
   if (c->aux[0]) return QV_OK;
   QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork2, cudaEventDisableTiming));
   QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
-  for (int k = 0; k < 3; k++) {
-    QV_CUDA(c, cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+  // the long moment chains (aux[0], aux[3], aux[4]) get the highest priority:
+  // their blocks go first when the build's other kernels free SMs
+  int lo_pri = 0, hi_pri = 0;
+  QV_CUDA(c, cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
+  for (int k = 0; k < 5; k++) {
+    const int pri = (k == 0 || k >= 3) ? hi_pri : lo_pri;
+    QV_CUDA(c, cudaStreamCreateWithPriority(&c->aux[k], cudaStreamNonBlocking, pri));
     QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));
   }
+  QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_l1, cudaEventDisableTiming));
+  QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_l1list, cudaEventDisableTiming));
   QV_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   QV_CUDA(c, cudaFuncSetAttribute(k_moments_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   2 * MC * 15 * (int)sizeof(double)));
@@ -1409,6 +1542,17 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
     t.root_pending = false;
   }
+  // ... or the node tables (late level-1 chains and payloads)
+  if (t.l1_pending) {
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_l1, 0));
+    t.l1_pending = false;
+  }
+  t.l1_late = false;
+  // The mixed walk of a large tree takes the root children's far-field terms
+  // after its own launch (their circ and Cij chains, two dependent roundings per
+  // point over up to an eighth of the points, would otherwise hold the walk back).
+  const bool late = c->p.precision == QV_PREC_MIXED && c->p.velocity == QV_VEL_TREE &&
+                    (g_l1_late_mode > 0 || (g_l1_late_mode < 0 && n >= QV_L1_LATE_MIN));
   if (!t.root_est) {
     QV_CUDA(c, cudaMalloc((void **)&t.root_est, 8 * sizeof(double)));
     QV_CUDA(c, cudaMalloc((void **)&t.root_ctl, 4 * sizeof(int)));
@@ -1489,13 +1633,39 @@ int qv_launch_tree_build(qv_ctx *c) {
     }
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
     k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rnk,
-                                                        t.ctl + CTL_NBIG, BIGN, INT_MAX, 1);
+                                                        t.ctl + CTL_NBIG, BIGN, INT_MAX, 1,
+                                                        late ? 1 : 0);
     const PackArgs pk = pack_args(c, 1, t.leaf_of, n);
     k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
         t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
-        t.cent, t.circ, t.C, t.first);
+        t.cent, t.circ, t.C, t.first, 0, pk, 1);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 2);
+    if (late) {
+      // the big root children: their centroid chains (aux[4]; the packs wait
+      // for them), their circ and Cij chains and then their payloads (aux[3];
+      // event ev_l1, joined after the walk's launch)
+      cudaStream_t s3 = c->aux[3], s4 = c->aux[4];
+      QV_CUDA(c, cudaStreamWaitEvent(s3, c->ev_fork, 0));
+      QV_CUDA(c, cudaMemsetAsync(t.l1list, 0, 16 * sizeof(int), s3));  // count, ready flag
+      k_list_big<<<1, 256, 0, s3>>>(t.ctl, t.cap_nodes, 1, t.count, t.l1list + 1, t.l1list, BIGN,
+                                    INT_MAX, 1, 2);
+      QV_LAUNCH_CHECK(c);
+      QV_CUDA(c, cudaEventRecord(c->ev_l1list, s3));
+      QV_CUDA(c, cudaStreamWaitEvent(s4, c->ev_l1list, 0));
+      k_moments_cent<<<8, MBT, 2 * MCC * 3 * sizeof(double), s4>>>(
+          t.ctl, t.l1list, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, t.cent, t.first, pk);
+      QV_LAUNCH_CHECK(c);
+      QV_CUDA(c, cudaEventRecord(c->ev_join[4], s4));
+      k_moments_big<<<8, MBT, 2 * MC * 15 * sizeof(double), s3>>>(
+          t.l1list + 1, t.l1list, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
+          t.cent, t.circ, t.C, t.first, 1, pk, 1);
+      QV_LAUNCH_CHECK(c);
+      k_l1_ready<<<1, 1, 0, s3>>>(t.l1list);
+      QV_LAUNCH_CHECK(c);
+      QV_CUDA(c, cudaEventRecord(c->ev_l1, s3));
+      QV_COUNT(c, 4);
+    }
     k_build_local<<<std::max(1, std::min(nblk(n, LCH), 2 * c->sm_count)), BT, LOCAL_SMEM,
                     c->stream>>>(a);
     QV_LAUNCH_CHECK(c);
@@ -1513,24 +1683,29 @@ int qv_launch_tree_build(qv_ctx *c) {
     QV_CUDA(c, cudaEventRecord(t.ev_ctl, c->aux[2]));
     QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NMID, 0, sizeof(int), c->aux[2]));
     k_list_big<<<4 * c->sm_count, 256, 0, c->aux[2]>>>(t.ctl, t.cap_nodes, 1, t.count, t.rs9,
-                                                        t.ctl + CTL_NMID, MIDN, BIGN, 0);
+                                                        t.ctl + CTL_NMID, MIDN, BIGN, 0, 0);
     k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[2]>>>(
         t.rs9, t.ctl + CTL_NMID, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi,
-        t.cent, t.circ, t.C, t.first);
+        t.cent, t.circ, t.C, t.first, 0, pk, 1);
     QV_CUDA(c, cudaEventRecord(c->ev_join[2], c->aux[2]));
     QV_COUNT(c, 2);
     k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, 1, t.level, t.start,
                                                            t.count, t.ord, t.cap_pts, c->x, c->gi,
                                                            t.cent, t.circ, t.C, t.first);
     QV_LAUNCH_CHECK(c);
-    QV_COUNT(c, 1);
+    // the packs of those nodes (of at most MIDN points) here, while the longer
+    // chains run on; the chain kernels pack the nodes they finish
+    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent,
+                                                          MIDN);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 2);
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
     QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[2], 0));
     if (!spec) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
-    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk,
-                                                          spec ? t.root_est : t.root_est + 4,
-                                                          t.cent);
+    if (late) QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[4], 0));
+    // every other node was packed by the kernel that summed its moments
+    k_root_pack<<<1, 32, 0, c->stream>>>(pk, spec ? t.root_est : t.root_est + 4, t.cent);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
     qv_phase_end_async(c, PH_BUILD_MOMENTS);
@@ -1539,6 +1714,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     if (hc[CTL_OVERFLOW]) {
       // the queued moment/pack kernels saw the flag and did nothing
       QV_CUDA(c, cudaStreamSynchronize(c->stream));
+      if (late) QV_CUDA(c, cudaStreamSynchronize(c->aux[3]));
       if (hc[CTL_OVERFLOW] == 1) {
         cap_nodes *= 2;
         continue;
@@ -1558,6 +1734,7 @@ int qv_launch_tree_build(qv_ctx *c) {
     t.perm = t.permb;
     t.n_leaf = n;
     t.valid = true;
+    t.l1_late = t.l1_pending = late;
     return QV_OK;
   }
   return qv_fail(c, QV_ERR_NOMEM, "tree build did not fit after repeated growth");
@@ -1576,6 +1753,10 @@ extern "C" int qv_root_undecided(qv_ctx *c, int *count) {
 
 int qv_tree_finalize_root(qv_ctx *c) {
   TreeBuf &t = c->tree;
+  if (t.l1_pending) {
+    t.l1_pending = false;
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_l1, 0));
+  }
   if (!t.root_pending) return QV_OK;
   t.root_pending = false;
   QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
@@ -1644,27 +1825,28 @@ int qv_forest_build(qv_ctx *c, const ForestArgs &f) {
   QV_CUDA(c, cudaStreamWaitEvent(c->aux[0], c->ev_fork2, 0));
   QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NBIG, 0, sizeof(int), c->aux[0]));
   k_list_big<<<4 * c->sm_count, 256, 0, c->aux[0]>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rnk,
-                                                      t.ctl + CTL_NBIG, BIGN, INT_MAX, 1);
+                                                      t.ctl + CTL_NBIG, BIGN, INT_MAX, 1, 0);
+  PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
+  pk.full = 0;  // the batch runs the mixed walk only and no candidate search
   k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->aux[0]>>>(
       t.rnk, t.ctl + CTL_NBIG, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
-      t.circ, t.C, t.first);
+      t.circ, t.C, t.first, 0, pk, 0);
   QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
   k_build_local<<<std::max(1, std::min(nblk(f.n_fact, LCH), 2 * c->sm_count)), BT, LOCAL_SMEM,
                   c->stream>>>(a);
   QV_CUDA(c, cudaMemsetAsync(t.ctl + CTL_NMID, 0, sizeof(int), c->stream));
   k_list_big<<<4 * c->sm_count, 256, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.count, t.rs9,
-                                                      t.ctl + CTL_NMID, MIDN, BIGN, 0);
+                                                      t.ctl + CTL_NMID, MIDN, BIGN, 0, 0);
   k_moments_big<<<2 * c->sm_count, MBT, 2 * MC * 15 * sizeof(double), c->stream>>>(
       t.rs9, t.ctl + CTL_NMID, t.level, t.start, t.count, t.ord, t.cap_pts, c->x, c->gi, t.cent,
-      t.circ, t.C, t.first);
+      t.circ, t.C, t.first, 0, pk, 0);
   k_moments<<<16 * c->sm_count, MW * 32, 0, c->stream>>>(t.ctl, t.cap_nodes, f.nroots, t.level,
                                                          t.start, t.count, t.ord, t.cap_pts, c->x,
                                                          c->gi, t.cent, t.circ, t.C, t.first);
   QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[0], 0));
   QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join[1], 0));
-  PackArgs pk = pack_args(c, f.nroots, nullptr, 0);
-  pk.full = 0;  // the batch runs the mixed walk only and no candidate search
-  k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent);
+  k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent,
+                                                        INT_MAX);
   QV_LAUNCH_CHECK(c);
   QV_COUNT(c, 10);
   return QV_OK;

@@ -28,6 +28,7 @@
 // when an image's root passes the opening test the image adds nothing, as in
 // the reference.
 #include <algorithm>
+#include <climits>
 
 #include "qv_walk.cuh"
 
@@ -69,7 +70,37 @@ struct WalkArgs {
   int *unc_count;
   int unc_cap;
   const int *gate;
+  // Late level-1 moments (mixed walk): in the unshifted image's tasks, the
+  // far-field term of a root child (node < l1_end) of more than QV_L1_BIG
+  // points is not taken here; bit node - 1 of the task's byte in defer
+  // (NSPLIT x n_act, slot major like part) records it for k_walk_l1_fix.  The
+  // periodic images' tasks, where those cells are far for most targets, run
+  // once the payloads are in and take every term.  l1_end = 0: no deferral.
+  int l1_end;
+  unsigned char *defer;
+  // Mixed walk, dynamic mode: the task counter next[ctr]; or (split != 0) the
+  // two launches of a late level-1 build (walk32_body), with l1_ready the flag
+  // that the late payloads' pack sets.
+  int ctr, split;
+  const int *l1_ready;
 };
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The one cell of an unshifted-image task whose far-field term the walk may
+// leave to k_walk_l1_fix: the task's root child k, its first cell, when late.
+// That first pop is taken before the task's loop (the loop itself is the
+// inline walk's): the targets that find the cell far set its bit in their
+// task's byte of defer (zeroed before the launch), the others open it.
+__device__ __forceinline__ bool late_cell(const WalkArgs &a, int k) {
+  if (!(k > 0 && k < a.l1_end)) return false;
+  const int j = qv_l1_pair(k);
+  return qv_l1_late(k, a.l1_end, a.w32[k].count, j < a.l1_end ? a.w32[j].count : 0);
+}
 
 // Record a lane whose root test the bound left undecided, with the
 // evaluations its walk of this task counted.
@@ -295,6 +326,9 @@ __device__ __forceinline__ void walk_task1(const WalkArgs &a, StkEnt *st, int la
     xi[0] = a.x[3 * i]; xi[1] = a.x[3 * i + 1]; xi[2] = a.x[3 * i + 2];
     bi = a.beh[i]; fi = a.inf[i]; ii = i + 1;
   }
+  // the gated redo rewrites every task: its bytes of defer start from zero
+  if (a.gate && a.defer && sl < NSPLIT && live) a.defer[(size_t)sl * a.n_act + q] = 0;
+  bool late_first = false;  // the first cell is a late root child (late_cell)
   Kahan3w k0;
   k0.zero();
   unsigned ev = 0, evf = 0;  // per task: far below 2^32
@@ -343,11 +377,48 @@ __device__ __forceinline__ void walk_task1(const WalkArgs &a, StkEnt *st, int la
           st[0].node = r.child_first + sl;
           st[0].mask = om;
         }
+        late_first = late_cell(a, r.child_first + sl);
         top = 1;
       }
     }
   }
   __syncwarp();
+  if (late_first) {
+    // the late root child: the loop's decisions for it, its far-field term
+    // deferred, its children pushed for the targets that open it
+    top = 0;
+    const WNode32 h = st[0].h;
+    const int node = st[0].node;
+    const bool in = (st[0].mask >> lane) & 1u;
+    __syncwarp();
+    float v0 = (th[0] - h.ch[0]) + (tl[0] - h.cl[0]);
+    float v1 = (th[1] - h.ch[1]) + (tl[1] - h.cl[1]);
+    float v2 = (th[2] - h.ch[2]) + (tl[2] - h.cl[2]);
+    float d2 = fmaf(v0, v0, fmaf(v1, v1, v2 * v2));
+    const bool amb = in && !(h.rhi > 0.f && (d2 > h.rhi || d2 < h.rlo));
+    bool open = in && d2 < h.rlo;
+    if (amb) {
+      const WNode64 h64 = a.w64[node];
+      open = exact_open(exact_dist(xi, h64, s), h64, a.theta, a.extra);
+    }
+    const bool far = in && !open;
+    ev += far ? 1u : 0u;
+    evf += far ? 1u : 0u;
+    if (far) a.defer[(size_t)sl * a.n_act + q] = (unsigned char)(1u << (node - 1));
+    const unsigned om = __ballot_sync(0xffffffffu, open);
+    if (om) {
+      const int nc = h.nchild;  // at most 8: the stack holds at least 15
+      if (lane < nc) {
+        int ch = h.child_first + nc - 1 - lane;
+        StkEnt &E = st[lane];
+        E.h = a.w32[ch];
+        E.node = ch;
+        E.mask = om;
+      }
+      top = nc;
+    }
+    __syncwarp();
+  }
   while (top > 0) {
     top--;
     const WNode32 h = st[top].h;
@@ -483,6 +554,12 @@ __device__ __forceinline__ void walk_task2(const WalkArgs &a, StkEnt *st, int la
       tl[c].y = __double2float_rn(ub - (double)th[c].y);
     }
   }
+  // the gated redo rewrites every task: its bytes of defer start from zero
+  if (a.gate && a.defer && sl < NSPLIT) {
+    if (la) a.defer[(size_t)sl * a.n_act + qa] = 0;
+    if (lb) a.defer[(size_t)sl * a.n_act + qb] = 0;
+  }
+  bool late_first = false;  // the first cell is a late root child (late_cell)
   Kahan3x2 k0;
   k0.zero();
   unsigned eva = 0, evfa = 0, evb = 0, evfb = 0;  // per task: far below 2^32
@@ -527,11 +604,53 @@ __device__ __forceinline__ void walk_task2(const WalkArgs &a, StkEnt *st, int la
           st[0].mask = ma;
           st[0].mask2 = mb;
         }
+        late_first = late_cell(a, r.child_first + sl);
         top = 1;
       }
     }
   }
   __syncwarp();
+  if (late_first) {
+    // the late root child: the loop's decisions for it, its far-field term
+    // deferred, its children pushed for the targets that open it
+    top = 0;
+    const WNode32 h = st[0].h;
+    const int node = st[0].node;
+    const bool ina = (st[0].mask >> lane) & 1u, inb = (st[0].mask2 >> lane) & 1u;
+    __syncwarp();
+    const float2 v0 = add2(sub2(th[0], bc2(h.ch[0])), sub2(tl[0], bc2(h.cl[0])));
+    const float2 v1 = add2(sub2(th[1], bc2(h.ch[1])), sub2(tl[1], bc2(h.cl[1])));
+    const float2 v2 = add2(sub2(th[2], bc2(h.ch[2])), sub2(tl[2], bc2(h.cl[2])));
+    const float2 d2 = fma2(v0, v0, fma2(v1, v1, mul2(v2, v2)));
+    const bool sure = h.rhi > 0.f;
+    const bool amba = ina && !(sure && (d2.x > h.rhi || d2.x < h.rlo));
+    const bool ambb = inb && !(sure && (d2.y > h.rhi || d2.y < h.rlo));
+    bool opa = ina && d2.x < h.rlo, opb = inb && d2.y < h.rlo;
+    if (amba) opa = exact_test(a, BC, sl, node, ta.i, rdelta, runa);
+    if (ambb) opb = exact_test(a, BC, sl, node, tb.i, rdelta, runb);
+    const bool fa = ina && !opa, fb = inb && !opb;
+    eva += fa ? 1u : 0u;
+    evfa += fa ? 1u : 0u;
+    evb += fb ? 1u : 0u;
+    evfb += fb ? 1u : 0u;
+    const unsigned char bit = (unsigned char)(1u << (node - 1));
+    if (fa) a.defer[(size_t)sl * a.n_act + qa] = bit;
+    if (fb) a.defer[(size_t)sl * a.n_act + qb] = bit;
+    const unsigned ma = __ballot_sync(0xffffffffu, opa), mb = __ballot_sync(0xffffffffu, opb);
+    if (ma | mb) {
+      const int nc = h.nchild;  // at most 8: the stack holds at least 15
+      if (lane < nc) {
+        const int ch = h.child_first + nc - 1 - lane;
+        StkEnt &E = st[lane];
+        E.h = a.w32[ch];
+        E.node = ch;
+        E.mask = ma;
+        E.mask2 = mb;
+      }
+      top = nc;
+    }
+    __syncwarp();
+  }
   while (top > 0) {
     top--;
     const WNode32 h = st[top].h;
@@ -643,11 +762,46 @@ __device__ __forceinline__ void walk32_body(const WalkArgs &a) {
   const int gn = a.pair_near ? a.ng64 : a.ngroups;  // groups of the unshifted image's tasks
   const int nnear = NSPLIT * gn;
   const int items = nnear + NIMG * a.ng64;
-  int *ctr = a.next ? a.next + (a.gate ? 1 : 0) : nullptr;
+  // Late level-1 split: the unshifted image's tasks come from next[0], the
+  // images' (which read the late payloads) from next[2].  Launch 1 (split 1)
+  // takes the unshifted ones, then the images' if the payloads are in by then
+  // (the flag is read, never waited for: otherwise it stops); launch 2
+  // (split 2), queued behind the payloads, takes the images' and then helps
+  // with the unshifted ones.
+  // split launches, per warp: bit 0 = on its second pool, bit 1 = the ready
+  // flag was seen set (read once: the acquire load is a round trip to L2)
+  __shared__ int wphase[WW];
+  if (lane == 0) wphase[wid] = 0;
   int item = blockIdx.x * WW + wid;
   for (;;) {
-    if (ctr) {
-      if (lane == 0) item = atomicAdd(ctr, 1);
+    if (a.next) {
+      if (lane == 0) {
+        if (!a.split) {
+          item = atomicAdd(a.next + a.ctr, 1);
+        } else {
+          for (;;) {
+            const int phase = wphase[wid] & 1;
+            const bool img = (phase == 0) == (a.split == 2);
+            if (img && a.split == 1 && !(wphase[wid] & 2)) {
+              if (ld_acquire(a.l1_ready) == 0) {
+                item = items;
+                break;
+              }
+              wphase[wid] |= 2;
+            }
+            const int t = atomicAdd(a.next + (img ? 2 : 0), 1);
+            if (t < (img ? items - nnear : nnear)) {
+              item = img ? nnear + t : t;
+              break;
+            }
+            if (phase == 1) {
+              item = items;
+              break;
+            }
+            wphase[wid] |= 1;
+          }
+        }
+      }
       item = __shfl_sync(0xffffffffu, item, 0);
     }
     if (item >= items) break;
@@ -730,9 +884,49 @@ __global__ void k_root_fix(WalkArgs a, int bc, const int4 *__restrict__ unc, int
     if (exact_open(exact_dist(xi, r, s), r, a.theta, a.extra)) continue;
     double *o = a.part + ((size_t)sl * a.n_act + q) * 3;
     o[0] = o[1] = o[2] = 0.;
+    if (a.defer && sl < NSPLIT) a.defer[(size_t)sl * a.n_act + q] = 0;
     const unsigned long long one = (sl == 0 || sl >= NSPLIT) ? 1ull : 0ull;
     atomicAdd(a.evals, one - (unsigned long long)(unsigned)u.z);
     atomicAdd(a.evals_far, one - (unsigned long long)(unsigned)u.w);
+  }
+}
+
+// The root children's far-field terms that the mixed walk deferred (late_cell),
+// once their moments and payloads are in: for each (task slot, target) whose
+// byte is set, the reference's far-cell term (src/tree.f90:394-413) of each
+// flagged child, in child order, in FP64 from the FP64 header and payload, as
+// the FP64 walk takes it, added to that task's partial sum after the walk's
+// compensated FP32 sum.
+__global__ void k_walk_l1_fix(WalkArgs a, int bc, int ntask) {
+  const size_t tot = (size_t)ntask * a.n_act;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot;
+       e += (size_t)gridDim.x * blockDim.x) {
+    unsigned m = a.defer[e];
+    if (!m) continue;
+    const int sl = (int)(e / (size_t)a.n_act), q = (int)(e - (size_t)sl * a.n_act);
+    const int i = a.perm[q];
+    const double xi[3] = {a.x[3 * i], a.x[3 * i + 1], a.x[3 * i + 2]};
+    double s[3];
+    slot_shift(bc, sl, a.L, s);
+    double acc[3] = {0., 0., 0.};
+    for (; m; m &= m - 1) {
+      const int node = __ffs(m);  // bit node - 1
+      const WNode64 h = a.w64[node];
+      const WPay64 &P = a.p64[node];
+      const double dist = exact_dist(xi, h, s);
+      double v[3] = {__dsub_rn(xi[0], __dadd_rn(h.cx, s[0])), __dsub_rn(xi[1], __dadd_rn(h.cy, s[1])),
+                     __dsub_rn(xi[2], __dadd_rn(h.cz, s[2]))};
+      double d2 = dist * dist, d3 = d2 * dist, d5 = d2 * d2 * dist;
+      double cv[3], z[3], vz[3];
+      cross3(P.a, v, cv);
+#pragma unroll
+      for (int l = 0; l < 3; l++) z[l] = v[0] * P.C[l] + v[1] * P.C[3 + l] + v[2] * P.C[6 + l];
+      cross3(v, z, vz);
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[c] += (cv[c] - P.b[c]) / d3 + 3. * vz[c] / d5;
+    }
+    double *o = a.part + e * 3;
+    o[0] += acc[0]; o[1] += acc[1]; o[2] += acc[2];
   }
 }
 
@@ -756,30 +950,62 @@ int qv_launch_walk(qv_ctx *c) {
   a.status = c->dstatus;
   a.root_est = nullptr; a.unc = nullptr; a.unc_count = nullptr; a.unc_cap = 0; a.gate = nullptr;
   const bool spec = t.root_pending;
+  const bool mixed = c->p.precision == QV_PREC_MIXED;
+  // Late level-1 payloads (qv_launch_tree_build): the mixed walk runs the
+  // unshifted image's tasks at once, deferring those cells' rare far-field
+  // terms, and the periodic images' tasks on a side stream once the payloads
+  // are in; its blocks take the SMs as the first launch's blocks run out of
+  // tasks.  The FP64 walk reads every payload, so it joins them first.
+  const bool l1 = mixed && t.l1_pending && t.lvl_start.size() > 2;
+  a.l1_end = 0;
+  a.defer = nullptr;
+  if (l1) {
+    const size_t nbytes = (size_t)NSPLIT * t.n_act;
+    if (nbytes > c->walk_defer_bytes) {
+      int rc = qv_grow(c, (void **)&c->walk_defer, nbytes);
+      if (rc) return rc;
+      c->walk_defer_bytes = nbytes;
+    }
+    a.l1_end = t.lvl_start[2];
+    a.defer = c->walk_defer;
+  } else if (t.l1_pending) {
+    QV_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_l1, 0));
+    t.l1_pending = false;
+  }
   if (spec) {
     a.root_est = t.root_est; a.unc = t.root_unc; a.unc_count = t.root_ctl;
     a.unc_cap = QV_ROOT_UNC_CAP;
   }
-  const bool mixed = c->p.precision == QV_PREC_MIXED;
   a.ngroups = (t.n_act + 31) / 32;
   a.ng64 = (t.n_act + 63) / 64;
   a.pair_near = t.n_act >= QV_WALK_PAIR_NEAR;
+  a.ctr = 0;
+  a.split = 0;
+  a.l1_ready = nullptr;
   // a depth-first stack over a tree of depth D never holds more than 7 D + 1
   // entries (each open pushes at most 8 and pops 1)
   a.stk_cap = 7 * (t.depth + 1) + 8;
   size_t smem = sizeof(StkEnt) * a.stk_cap * WW;
-  const long items = mixed ? (long)NSPLIT * (a.pair_near ? a.ng64 : a.ngroups) + (long)a.ng64 * nimg
-                           : (long)a.ngroups * (NSPLIT + nimg);
-  int nb = (int)std::min<long>((items + WW - 1) / WW, 64L * c->sm_count);
+  const long nnear = (long)NSPLIT * (a.pair_near ? a.ng64 : a.ngroups);
+  const long items = mixed ? nnear + (long)a.ng64 * nimg : (long)a.ngroups * (NSPLIT + nimg);
+  const bool dynamic = mixed && (t.n_act >= QV_WALK_DYNAMIC || l1);
+  // blocks of a launch of m tasks
+  auto grid_for = [&](long m) -> int {
+    const long cap = dynamic ? (long)WALK32_BLOCKS_PER_SM * c->sm_count  // one resident grid
+                             : 64L * c->sm_count;
+    return (int)std::max(1L, std::min<long>((m + WW - 1) / WW, cap));
+  };
+  int nb = grid_for(items);
   a.next = nullptr;
-  if (mixed && t.n_act >= QV_WALK_DYNAMIC) {
-    // every warp stays until the task counter runs out: one resident grid
-    nb = (int)std::min<long>((items + WW - 1) / WW, (long)WALK32_BLOCKS_PER_SM * c->sm_count);
+  if (dynamic) {
+    // every warp stays until its task counters run out: next[0] the walk (the
+    // unshifted image's tasks when level 1 is late), next[1] the gated redo,
+    // next[2] the images' tasks when level 1 is late
     if (!c->walk_next) {
-      int rc = qv_grow(c, (void **)&c->walk_next, 2 * sizeof(int));
+      int rc = qv_grow(c, (void **)&c->walk_next, 4 * sizeof(int));
       if (rc) return rc;
     }
-    QV_CUDA(c, cudaMemsetAsync(c->walk_next, 0, 2 * sizeof(int), c->stream));
+    QV_CUDA(c, cudaMemsetAsync(c->walk_next, 0, 4 * sizeof(int), c->stream));
     a.next = c->walk_next;
   }
   if (mixed && smem > 48 * 1024) {
@@ -795,15 +1021,15 @@ int qv_launch_walk(qv_ctx *c) {
       c->smem_walk = smem;
     }
   }
-  auto launch = [&](const WalkArgs &w, int grid) -> int {
+  auto launch = [&](const WalkArgs &w, int grid, cudaStream_t st) -> int {
     const bool redo = w.gate != nullptr;
     switch (c->p.boundary) {
-#define QV_WALK_CASE(BCV)                                                        \
-  case BCV:                                                                      \
-    if (mixed && redo) k_walk32_redo<BCV><<<grid, WW * 32, smem, c->stream>>>(w); \
-    else if (mixed) k_walk32<BCV><<<grid, WW * 32, smem, c->stream>>>(w);        \
-    else if (redo) k_walk64_redo<BCV><<<grid, WW * 32, 0, c->stream>>>(w);       \
-    else k_walk64<BCV><<<grid, WW * 32, 0, c->stream>>>(w);                      \
+#define QV_WALK_CASE(BCV)                                                  \
+  case BCV:                                                                \
+    if (mixed && redo) k_walk32_redo<BCV><<<grid, WW * 32, smem, st>>>(w); \
+    else if (mixed) k_walk32<BCV><<<grid, WW * 32, smem, st>>>(w);        \
+    else if (redo) k_walk64_redo<BCV><<<grid, WW * 32, 0, st>>>(w);       \
+    else k_walk64<BCV><<<grid, WW * 32, 0, st>>>(w);                      \
     break;
       QV_WALK_CASE(QV_BC_OPEN)
       QV_WALK_CASE(QV_BC_PERIODIC)
@@ -817,20 +1043,48 @@ int qv_launch_walk(qv_ctx *c) {
     QV_COUNT(c, 1);
     return QV_OK;
   };
-  int rc = launch(a, nb);
-  if (rc) return rc;
-  if (spec) {
-    // the exact root centroid (joined now, long after it finished), the fix-up
-    // of undecided root tests, and the second walk that runs only if the
-    // fix-up's list overflowed
+  int rc;
+  if (l1) {
+    // launch 1 now; launch 2 behind the late payloads on aux[3] (the stream
+    // that packs them).  In practice launch 1 finds the payloads in once the
+    // unshifted tasks run out and takes every task; launch 2's blocks then
+    // find both counters spent.
+    QV_CUDA(c, cudaMemsetAsync(c->walk_defer, 0, (size_t)NSPLIT * t.n_act, c->stream));
+    WalkArgs a1 = a;
+    a1.split = 1;
+    a1.l1_ready = t.l1list + 15;
+    QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    if ((rc = launch(a1, nb, c->stream))) return rc;
+    WalkArgs a2 = a;
+    a2.split = 2;
+    cudaStream_t s3 = c->aux[3];
+    QV_CUDA(c, cudaStreamWaitEvent(s3, c->ev_fork, 0));
+    if ((rc = launch(a2, nb, s3))) return rc;
+    QV_CUDA(c, cudaEventRecord(c->ev_l1, s3));
+    // the finalize below joins ev_l1: the payloads and launch 2
+  } else if ((rc = launch(a, nb, c->stream))) {
+    return rc;
+  }
+  // joined now, long after they finished: the images' walk and the late
+  // level-1 payloads, and the exact root centroid
+  if (spec || l1)
     if ((rc = qv_tree_finalize_root(c))) return rc;
+  if (spec) {
+    // the fix-up of undecided root tests, and the second walk that runs only
+    // if the fix-up's list overflowed (it defers the same cells)
     k_root_fix<<<1, 256, 0, c->stream>>>(a, c->p.boundary, t.root_unc, t.root_ctl);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 1);
     WalkArgs b = a;
     b.root_est = nullptr; b.unc = nullptr; b.unc_count = nullptr; b.unc_cap = 0;
     b.gate = t.root_ctl + 2;
-    if ((rc = launch(b, std::min(nb, 2 * c->sm_count)))) return rc;
+    b.ctr = 1;
+    if ((rc = launch(b, std::min(nb, 2 * c->sm_count), c->stream))) return rc;
+  }
+  if (l1) {
+    k_walk_l1_fix<<<4 * c->sm_count, 256, 0, c->stream>>>(a, c->p.boundary, NSPLIT);
+    QV_LAUNCH_CHECK(c);
+    QV_COUNT(c, 1);
   }
   k_walk_reduce<<<(t.n_act + 255) / 256, 256, 0, c->stream>>>(t.n_act, nimg, t.perm, c->walk_part,
                                                                 a.gfac, c->u_li, c->u, c->u_bs);

@@ -140,6 +140,7 @@ _SIGS = {
     "qv_probe_fp32": [_P, _D],
     "qv_test_stage_timeout": [C.c_int],
     "qv_test_root_speculation": [C.c_int, C.c_double],
+    "qv_test_late_level1": [C.c_int],
     "qv_root_undecided": [_P, _I],
     "qv_velocity_direct_noalloc": [C.POINTER(QvParams), C.c_int, _P, _P, _P, _P, _P],
     "qv_velocity_device": [_P, _P],
@@ -588,6 +589,15 @@ def test_stage_timeout(enable: bool) -> None:
     """Test hook: every direct-sum source-tile wait reports that it ran out
     (the copies still land and are drained); False restores normal waits."""
     _lib.qv_test_stage_timeout(int(bool(enable)))
+
+
+def test_late_level1(mode: int = -1) -> None:
+    """Test hook: -1 by build size (default), 0 never, 1 always pack the big
+    root children of a mixed Tree build late (the walk adds their far-field
+    terms after its launch)."""
+    rc = _lib.qv_test_late_level1(int(mode))
+    if rc < 0:
+        raise QvError(rc, "bad late level-1 setting")
 
 
 def test_root_speculation(mode: int = -1, bound_scale: float = 1.0) -> None:

@@ -732,3 +732,100 @@ def test_root_estimate_gives_the_exact_walk_on_the_tangle(L):
         c64.close()
     assert seen[0] == 0, seen
     assert any(0 < s <= 8192 for s in seen) and any(s > 8192 for s in seen), seen
+
+
+# ----------------------------------------------- late level-1 moments (mixed)
+@pytest.mark.parametrize("bc", ["periodic", "open"])
+def test_late_level1_matches_the_inline_walk(L, bc):
+    """A mixed Tree build that packs the big root children late (their circ
+    and Cij sums still running when the walk starts: the unshifted image's
+    tasks defer those cells' far-field terms, the images' tasks wait for the
+    payloads) gives the walk of the inline build's decisions and evaluation
+    counts; the deferred terms are added in FP64 after the compensated FP32
+    sum instead of inside it, so the velocities differ by that rounding only
+    (1e-7 RMS), and both are within 1e-6 RMS of the FP64 walk.  A second walk
+    on the same tree, its payloads all in, takes every term inline and repeats
+    the inline build's velocities bit for bit."""
+    w = W.tangle(0)
+    c = ctx_for(L, w, precision="mixed", boundary=bc)
+    c64 = ctx_for(L, w, precision="fp64", boundary=bc)
+    try:
+        L.test_late_level1(0)
+        u0, _, _, ev0 = c.velocity()
+        L.test_late_level1(1)
+        c.set_points(w.x, w.infront, w.behind)
+        u1, _, _, ev1 = c.velocity()
+        u2, _, _, ev2 = c.velocity()
+        u64, _, _, ev64 = c64.velocity()
+    finally:
+        L.test_late_level1(-1)
+        c.close()
+        c64.close()
+    assert ev1 == ev0 == ev2 == ev64
+    assert np.array_equal(u2, u0)
+    assert rel_rms(u1, u0) < 1e-7
+    assert rel_rms(u1, u64) < 1e-6 and rel_rms(u0, u64) < 1e-6
+
+
+def test_late_level1_with_the_root_estimate(L):
+    """Late level-1 payloads together with the root centroid's bounded
+    estimate: whether every root test is decided, the fix-up drops undecided
+    images (and their deferred cells), or its list overflows and the gated
+    walk redoes every task, the velocities and evaluation counts are those of
+    the late build from the exact centroid, bit for bit."""
+    w = W.tangle(0)
+    c = ctx_for(L, w, precision="mixed")
+    try:
+        L.test_late_level1(1)
+        L.test_root_speculation(0)
+        c.set_points(w.x, w.infront, w.behind)
+        u0, _, _, ev0 = c.velocity()
+        seen = []
+        for scale in (1.0, 3e10, 1e11, 3e11, 1e12, 1e13, 1e14):
+            L.test_root_speculation(1, scale)
+            c.set_points(w.x, w.infront, w.behind)
+            u, _, _, ev = c.velocity()
+            seen.append(c.root_undecided())
+            assert np.array_equal(u, u0), scale
+            assert ev == ev0, scale
+    finally:
+        L.test_root_speculation(-1, 1.0)
+        L.test_late_level1(-1)
+        c.close()
+    assert seen[0] == 0, seen
+    assert any(0 < s <= 8192 for s in seen) and any(s > 8192 for s in seen), seen
+
+
+def test_late_level1_by_size(L):
+    """80,843 points (above the size from which a mixed Tree build packs the
+    big root children late by default): the default build against the inline
+    one, same evaluation counts, 1e-7 RMS apart, both within 1e-6 RMS of the
+    FP64 walk; and a few steps of the default loop keep the links and the
+    candidate pairs of the inline build's steps."""
+    w = W.large_tangle(0, n_rings=300)
+    assert w.n >= 65536
+    res = {}
+    for mode in (-1, 0):
+        L.test_late_level1(mode)
+        try:
+            c = ctx_for(L, w, precision="mixed", line_ops=2)
+            u, _, _, ev = c.velocity()
+            for it in range(1, 4):
+                c.step(it)
+            n = c.n
+            inf, beh = c.get_links()
+            cl, _ = c.get_closest()
+            res[mode] = (u, ev, n, inf[:n].copy(), beh[:n].copy(), cl[:n].copy())
+            c.close()
+        finally:
+            L.test_late_level1(-1)
+    c64 = ctx_for(L, w, precision="fp64")
+    u64, _, _, ev64 = c64.velocity()
+    c64.close()
+    (ua, eva, *sa), (ub, evb, *sb) = res[-1], res[0]
+    assert eva == evb == ev64
+    assert rel_rms(ua, ub) < 1e-7
+    assert rel_rms(ua, u64) < 1e-6 and rel_rms(ub, u64) < 1e-6
+    assert sa[0] == sb[0]
+    for x, y in zip(sa[1:], sb[1:]):
+        np.testing.assert_array_equal(x, y)
