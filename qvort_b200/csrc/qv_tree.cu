@@ -1694,9 +1694,12 @@ int qv_launch_tree_build(qv_ctx *c) {
                                                            t.cent, t.circ, t.C, t.first);
     QV_LAUNCH_CHECK(c);
     // the packs of those nodes (of at most MIDN points) here, while the longer
-    // chains run on; the chain kernels pack the nodes they finish
-    k_pack_nodes<<<4 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent,
-                                                          MIDN);
+    // chains run on; the chain kernels pack the nodes they finish.  Four times
+    // the blocks of a full pack: each thread's few nodes are dependent loads
+    // (first point, its links), and more of them in flight shortened this pass
+    // by 0.13 ms at 0.8M points.
+    k_pack_nodes<<<16 * c->sm_count, 128, 0, c->stream>>>(t.ctl, t.cap_nodes, pk, nullptr, t.cent,
+                                                           MIDN);
     QV_LAUNCH_CHECK(c);
     QV_COUNT(c, 2);
     QV_CUDA(c, cudaEventRecord(c->ev_join[0], c->aux[0]));
