@@ -71,8 +71,8 @@ struct WalkArgs {
   int unc_cap;
   const int *gate;
   // Late level-1 moments (mixed walk): in the unshifted image's tasks, the
-  // far-field term of a root child (node < l1_end) of more than QV_L1_BIG
-  // points is not taken here; bit node - 1 of the task's byte in defer
+  // far-field term of a late root child (node < l1_end, qv_l1_late) is not
+  // taken here; bit node - 1 of the task's byte in defer
   // (NSPLIT x n_act, slot major like part) records it for k_walk_l1_fix.  The
   // periodic images' tasks, where those cells are far for most targets, run
   // once the payloads are in and take every term.  l1_end = 0: no deferral.
@@ -80,7 +80,7 @@ struct WalkArgs {
   unsigned char *defer;
   // Mixed walk, dynamic mode: the task counter next[ctr]; or (split != 0) the
   // two launches of a late level-1 build (walk32_body), with l1_ready the flag
-  // that the late payloads' pack sets.
+  // that k_l1_ready sets once the late payloads are packed.
   int ctr, split;
   const int *l1_ready;
 };
