@@ -328,8 +328,9 @@ int qv_get_links(qv_ctx *ctx, int *infront, int *behind);
  * their device times accumulate into ms[QV_NPHASES]. */
 /* ghosts, tree build, local term, non-local sum, update, search, wrap, two
  * parts of the tree build (the level-synchronous construction and the
- * moments), and the line operations (pinsert, premove) */
-#define QV_NPHASES 10
+ * moments), the line operations (pinsert, premove), and inside the non-local
+ * sum the mixed Barnes-Hut walk's kernel alone */
+#define QV_NPHASES 11
 int qv_profile(qv_ctx *ctx, int enable);
 int qv_phase_times(qv_ctx *ctx, double *ms, int reset);
 /* Kernel launches issued by this context so far, and the leaf / far-field

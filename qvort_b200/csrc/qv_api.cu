@@ -1215,6 +1215,7 @@ extern "C" int qv_profile(qv_ctx *c, int enable) {
   return QV_OK;
 }
 
+static_assert(PH_N == QV_NPHASES, "the phases qv_phase_times reports are qv.h's");
 extern "C" int qv_phase_times(qv_ctx *c, double *ms, int reset) {
   QV_CHECK_CTX(c);
   qv_phase_collect(c);

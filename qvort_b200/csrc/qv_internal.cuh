@@ -158,6 +158,7 @@ enum {
   PH_BUILD_LEVELS,   // inside PH_BUILD: init + the level-synchronous kernel
   PH_BUILD_MOMENTS,  // inside PH_BUILD: moment chains, root centroid join, packs
   PH_LINE,           // pinsert / premove
+  PH_WALK,           // inside PH_NONLOCAL: the mixed walk's kernel alone (its first launch)
   PH_N
 };
 

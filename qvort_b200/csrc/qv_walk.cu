@@ -1054,7 +1054,9 @@ int qv_launch_walk(qv_ctx *c) {
     a1.split = 1;
     a1.l1_ready = t.l1list + 15;
     QV_CUDA(c, cudaEventRecord(c->ev_fork, c->stream));
+    if (mixed) qv_phase_begin(c, PH_WALK);
     if ((rc = launch(a1, nb, c->stream))) return rc;
+    if (mixed) qv_phase_end_async(c, PH_WALK);
     WalkArgs a2 = a;
     a2.split = 2;
     cudaStream_t s3 = c->aux[3];
@@ -1062,8 +1064,10 @@ int qv_launch_walk(qv_ctx *c) {
     if ((rc = launch(a2, nb, s3))) return rc;
     QV_CUDA(c, cudaEventRecord(c->ev_l1, s3));
     // the finalize below joins ev_l1: the payloads and launch 2
-  } else if ((rc = launch(a, nb, c->stream))) {
-    return rc;
+  } else {
+    if (mixed) qv_phase_begin(c, PH_WALK);
+    if ((rc = launch(a, nb, c->stream))) return rc;
+    if (mixed) qv_phase_end_async(c, PH_WALK);
   }
   // joined now, long after they finished: the images' walk and the late
   // level-1 payloads, and the exact root centroid

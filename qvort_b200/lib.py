@@ -497,7 +497,7 @@ class Context:
 
     # ---- instrumentation
     PHASES = ("ghosts", "build", "local", "nonlocal", "update", "search", "wrap",
-              "build_levels", "build_moments", "line")
+              "build_levels", "build_moments", "line", "walk_kernel")
 
     def profile(self, enable: bool = True):
         self._check(_lib.qv_profile(self._h, int(enable)))
