@@ -652,6 +652,47 @@ def test_step_exchange_equals_set_step_get(delta):
     b.close()
 
 
+def test_step_exchange_equals_set_step_get_late_level1(L):
+    """The same equality on config 2's tangle with the root children's long
+    moment sums taken late (forced: the tangle is below the size that takes them
+    late by itself): the exchange step's copies of u and the AB history, taken
+    behind pinsert, hold the velocities with the deferred far-field terms in."""
+    w = W.tangle(0)
+    prm = dict(w.params, precision="mixed", line_ops=2)
+    n0 = w.n
+    cap = n0 + 8192
+
+    def host():
+        h = dict(x=np.zeros((cap, 3)), u=np.zeros((cap, 3)), u1=np.zeros((cap, 3)),
+                 u2=np.zeros((cap, 3)), u3=np.zeros((cap, 3)), infront=np.zeros(cap, np.int32),
+                 behind=np.zeros(cap, np.int32), closest=np.zeros(cap, np.int32),
+                 closestd=np.zeros(cap))
+        h["x"][:n0] = w.x
+        h["infront"][:n0] = w.infront
+        h["behind"][:n0] = w.behind
+        return h
+
+    ha, hb = host(), host()
+    ins = ("x", "infront", "behind", "u1", "u2", "u3", "closest")
+    L.test_late_level1(1)
+    try:
+        a = L.Context(L.default_params(**prm))
+        b = L.Context(L.default_params(**prm))
+        na = nb = n0
+        for it in range(1, 4):
+            na = a.step_exchange(it, na, cap, {k: ha[k] for k in ins}, ha)
+            b.set_state(nb, **{k: hb[k] for k in ins})
+            b.step(it)
+            nb = b.get_state(cap, **hb)
+            assert na == nb
+            for k in ha:
+                assert np.array_equal(ha[k][:na], hb[k][:nb]), (it, k)
+        a.close()
+        b.close()
+    finally:
+        L.test_late_level1(-1)
+
+
 @pytest.mark.parametrize("bc", ["open", "periodic", "openx", "openxy"])
 def test_field_velocity_direct_matches_oracle(L, bc):
     """biot_savart_general with the boundary's images (the BS arm of
